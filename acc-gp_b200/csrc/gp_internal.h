@@ -1,0 +1,17 @@
+// Internal declarations shared by the host and device translation units.
+#pragma once
+#include "../../include/gpart_b200.h"
+
+#include <cstdint>
+#include <string>
+
+namespace gp {
+
+constexpr int kMaxParts = 128;  // include/graph_types.hpp:4
+
+void set_error(const std::string& message);
+const char* last_error();
+gp_status capacity_of(uint64_t total, int k, double eps, uint64_t* out);
+gp_status validate_host_csr(const gp_csr* g, bool need_positive_vw);
+
+}  // namespace gp

@@ -1,0 +1,180 @@
+/*
+ * gpart_b200 — C ABI of the B200-native multilevel k-way graph partitioner.
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or framework types
+ * cross this boundary and no exception escapes it.  Host buffers belong to the
+ * caller.  Each function returns a gp_status; on failure gp_last_error()
+ * returns a thread-local message.
+ *
+ * Reference interfaces replaced (Acc-GPart, paths inside its source tree):
+ *   gp_partition            the pipeline that app/partition_main.cu:47-137 drives:
+ *                           load → partition_capacity → coarsen
+ *                           (include/coarsen.hpp:111) → initial_partition_metis
+ *                           (include/initial_partition.hpp:6) → uncoarsen
+ *                           (include/uncoarsen.hpp:19) → labels
+ *   gp_partition_device     the same pipeline on caller-owned device buffers
+ *                           (the reference's resident DeviceWeightedGraph path,
+ *                           include/graph.hpp:148-171)
+ *   gp_read_csr_int64       load_weighted_graph (include/graph.hpp:173, src/graph.cpp:47)
+ *   gp_write_csr_int64      the on-disk int64 CSR format that loader reads
+ *   gp_partition_capacity   partition_capacity (include/partition_capacity.hpp:14)
+ *   gp_verify               gpart_verify_csr (tools/verify_csr.cpp:37-110), extended
+ *                           with vertex/edge weights and a caller-chosen epsilon
+ *   gp_edge_cut             host_cut (src/graph.cpp:184)
+ */
+#ifndef GPART_B200_H
+#define GPART_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gp_status {
+    GP_OK = 0,
+    GP_INVALID_ARGUMENT = 1,    /* malformed CSR, k outside 2..128, bad epsilon ...   */
+    GP_CAPACITY_INFEASIBLE = 2, /* floor(total*eps/k) cannot hold the total weight    */
+    GP_OUT_OF_MEMORY = 3,       /* device or host allocation failed                   */
+    GP_DEVICE_TIMEOUT = 4,      /* a bounded device wait gave up                      */
+    GP_INTERNAL = 5,            /* an algorithm invariant failed (reference would throw) */
+    GP_CUDA_ERROR = 6,          /* a CUDA runtime call failed                         */
+    GP_NO_DEVICE = 7,           /* no usable CUDA device / extension not loaded       */
+    GP_IO_ERROR = 8             /* file could not be opened, read or written          */
+} gp_status;
+
+/* A graph in CSR form. offsets[n+1], neighbors[m] (int32), vertex_weights[n]
+ * and edge_weights[m] (uint32).  A NULL weight array means unit weights,
+ * exactly like the reference's implicit unit edge weights
+ * (include/detail/edge_weight.hpp:8).  The graph must be symmetric with equal
+ * reverse weights and strictly positive vertex weights. */
+typedef struct gp_csr {
+    int64_t n;
+    int64_t m;
+    const int32_t* offsets;
+    const int32_t* neighbors;
+    const uint32_t* vertex_weights;
+    const uint32_t* edge_weights;
+} gp_csr;
+
+/* Per-call statistics (all times in seconds, measured with CUDA events on
+ * the context stream where noted). */
+typedef struct gp_stats {
+    uint64_t edge_cut;            /* final undirected cut                            */
+    uint64_t max_part_weight;     /* heaviest part                                   */
+    uint64_t capacity;            /* floor(total*eps/k)                              */
+    uint64_t initial_cut;         /* cut of the METIS partition of the coarsest graph */
+    int32_t levels;               /* graphs in the hierarchy (input included)        */
+    int32_t coarsest_vertices;
+    double coarsen_seconds;       /* device time of coarsening                       */
+    double initial_seconds;       /* METIS step, including its copies                */
+    double uncoarsen_seconds;     /* projection + refinement                         */
+    double algorithm_seconds;     /* input resident → labels resident                */
+    double h2d_seconds;           /* host → device copy of the input (gp_partition)  */
+    double d2h_seconds;           /* device → host copy of the labels (gp_partition) */
+    uint64_t kernel_launches;     /* kernels this library launched during the call   */
+    uint64_t algorithmic_bytes;   /* compulsory HBM traffic model of the V-cycle     */
+} gp_stats;
+
+/* Flags for gp_partition / gp_partition_device. */
+#define GP_FLAG_VERIFY           0x1u /* the reference's --verify invariants, on host copies */
+#define GP_FLAG_KEEP_HIERARCHY   0x2u /* keep host copies of every level for gp_level_*     */
+#define GP_FLAG_NO_SEED_MATCHING 0x4u /* GPART_HEM_COARSEN=0 (app/partition_main.cu:57)    */
+#define GP_FLAG_QUIET            0x8u /* no per-level key=value log lines on stdout        */
+#define GP_FLAG_COARSEN_ONLY     0x10u /* stop after coarsening (levels kept, no labels)   */
+
+typedef struct gp_context gp_context;
+
+/* One context per host thread; contexts are independent of each other.  The
+ * context owns a device arena and a CUDA stream on `device`. */
+gp_status gp_context_create(int device, gp_context** out);
+void gp_context_destroy(gp_context* ctx);
+const char* gp_last_error(void);
+const char* gp_version(void);
+
+/* Partition a host CSR.  Copies the graph to the device, runs the V-cycle,
+ * copies int32 labels (length n, values in [0,k)) back to labels_out. */
+gp_status gp_partition(gp_context* ctx, const gp_csr* graph, int32_t k,
+                       double epsilon, uint32_t seed, uint32_t flags,
+                       int32_t* labels_out, gp_stats* stats);
+
+/* Same, with every pointer of `graph` and labels_out in device memory of the
+ * context's device.  `stream` is a cudaStream_t (NULL: the context stream);
+ * the call returns after the labels are written. */
+gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k,
+                              double epsilon, uint32_t seed, uint32_t flags,
+                              int32_t* labels_out_device, void* stream,
+                              gp_stats* stats);
+
+/* Hierarchy of the last call made with GP_FLAG_KEEP_HIERARCHY.  Level 0 is
+ * the input.  gp_level_copy fills any non-NULL array; `map` (length n of the
+ * level) maps this level's vertices to the next level and is absent for the
+ * last level.  metadata[4] = {maximum_degree bound, has_heavy_rows,
+ * incident_weight_bound, 0}. */
+gp_status gp_level_count(gp_context* ctx, int32_t* levels);
+gp_status gp_level_size(gp_context* ctx, int32_t level, int64_t* n, int64_t* m);
+gp_status gp_level_copy(gp_context* ctx, int32_t level, int32_t* offsets,
+                        int32_t* neighbors, uint32_t* edge_weights,
+                        uint32_t* vertex_weights, int32_t* map,
+                        uint64_t* metadata);
+/* METIS labels of the coarsest graph from the last call. */
+gp_status gp_initial_labels(gp_context* ctx, int32_t* labels, int64_t capacity);
+
+/* ---- host utilities (no device needed) ---- */
+
+/* floor(total*eps/k) in long double, with the reference's feasibility check. */
+gp_status gp_partition_capacity(uint64_t total, int32_t k, double epsilon,
+                                uint64_t* capacity);
+
+/* Read the reference's on-disk format: int64 indptr[n+1], int64 indices[m].
+ * Narrows to int32 with the same range checks.  Call with NULL outputs to
+ * get n and m, then again with buffers of that size. */
+gp_status gp_read_csr_int64(const char* indptr_path, const char* indices_path,
+                            int64_t* n, int64_t* m, int32_t* offsets,
+                            int32_t* neighbors);
+gp_status gp_write_csr_int64(const char* indptr_path, const char* indices_path,
+                             const gp_csr* graph);
+
+/* Exact undirected cut of `labels` (directed sum / 2; odd sum is an error). */
+gp_status gp_edge_cut(const gp_csr* graph, const int32_t* labels, uint64_t* cut);
+
+/* Independent verifier: cut, part loads (vertex weights), capacity
+ * floor(total*eps/k) and whether every load fits.  Writes one JSON line of at
+ * most json_capacity bytes.  Returns GP_OK even when capacity is violated;
+ * check *capacity_ok. */
+gp_status gp_verify(const gp_csr* graph, const int32_t* labels, int32_t k,
+                    double epsilon, int32_t check_symmetry, uint64_t* cut,
+                    uint64_t* loads /* k entries or NULL */,
+                    int32_t* capacity_ok, char* json, size_t json_capacity);
+
+/* ---- seeded synthetic inputs (counter-based, identical on every host) ---- */
+
+/* Generators write into caller buffers; call with NULL arrays first to learn
+ * n and m.  Weight arrays may be NULL. */
+gp_status gp_generate_grid2d(int32_t width, int32_t height, int64_t* n, int64_t* m,
+                             int32_t* offsets, int32_t* neighbors);
+/* 3D 7-point mesh, id = x + X*(y + Y*z).  With weighted != 0 vertex weights
+ * are uniform in [1,4] and edge weights uniform in [1,16], keyed by the
+ * unordered endpoint pair so the CSR stays symmetric. */
+gp_status gp_generate_mesh3d(int32_t x, int32_t y, int32_t z, int32_t weighted,
+                             uint64_t seed, int64_t* n, int64_t* m,
+                             int32_t* offsets, int32_t* neighbors,
+                             uint32_t* vertex_weights, uint32_t* edge_weights);
+/* R-MAT: edge_factor * 2^scale samples with probabilities (a,b,c,1-a-b-c),
+ * symmetrised, self loops and duplicates removed, rows sorted.  The graph is
+ * cached per (scale, edge_factor, a, b, c, seed) inside the library so the
+ * two-phase call generates once. */
+gp_status gp_generate_rmat(int32_t scale, int32_t edge_factor, double a,
+                           double b, double c, uint64_t seed, int64_t* n,
+                           int64_t* m, int32_t* offsets, int32_t* neighbors);
+/* Uniform random weights in [lo,hi] keyed by (seed, vertex) and by
+ * (seed, min(u,v), max(u,v)) for edges, so reverse edges agree. */
+gp_status gp_generate_weights(const gp_csr* graph, uint64_t seed, uint32_t vw_lo,
+                              uint32_t vw_hi, uint32_t ew_lo, uint32_t ew_hi,
+                              uint32_t* vertex_weights, uint32_t* edge_weights);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPART_B200_H */
