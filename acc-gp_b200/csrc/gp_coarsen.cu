@@ -1,0 +1,1373 @@
+// Coarsening on the B200: stable-receiver aggregation and exact coarse-CSR
+// contraction (Acc-GPart src/coarsen.cu, src/coarsening/*.cuh).
+//
+// Per level (aggregate_typed, src/coarsen.cu:467-1380):
+//   seed matching -> <=4 rounds of {frozen roles, exact per-cluster
+//   affinities, admission, commit} -> isolated packing -> two-hop pairing ->
+//   compaction; then contraction (src/coarsen.cu:1394-1673).
+// Every rule reproduces the reference exactly; the kernels differ: affinity
+// and proposal decoding are fused per degree class, admission sorts only the
+// requests of targets whose total demand overflows, and the coarse CSR is
+// built row-locally with one global radix sort reserved for the few huge rows.
+#include "gp_graph.h"
+#include "gp_primitives.cuh"
+
+#include <algorithm>
+#include <cstdio>
+
+namespace gp {
+
+thread_local u64 g_launches = 0;
+
+namespace {
+
+constexpr int kLowDegree = 8;       // SCLP_LOW_DEGREE
+constexpr int kMediumDegree = 256;  // SCLP_MEDIUM_DEGREE
+constexpr int kLargeDegree = 4096;  // rows above use a global-memory table
+constexpr int kMediumHash = 512;    // SCLP_MEDIUM_HASH_SIZE
+constexpr int kLargeHash = 8192;
+constexpr int kMediumWarps = 4;
+
+// ---------------------------------------------------------------- metadata
+
+// record_bound_kernel (src/coarsen.cu:51-99) plus the weight invariants of
+// aggregate_typed (:483-493).  Scalars: 0 max row bound, 1 unsorted,
+// 2 zero weight, 3 non-unit weight, 4 max raw degree, 5 total vertex
+// weight, 6 max vertex weight.
+template <int W>
+__global__ void k_level0_meta(i64 n, const int* off, const int* nbr, const u32* ew, const u32* vw, u64* bounds,
+                              u64* sc) {
+    __shared__ u64 s_max, s_raw, s_total, s_vmax;
+    __shared__ u32 s_flags;
+    if (threadIdx.x == 0) { s_max = s_raw = s_total = s_vmax = 0; s_flags = 0; }
+    __syncthreads();
+    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+    const int lane = threadIdx.x & (W - 1);
+    const bool valid = v < n;
+    u64 d = 0;
+    u32 flags = 0;
+    const i64 begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
+    for (i64 e = begin + lane; e < end; e += W) {
+        const u64 w = edge_w(ew, e);
+        d = ~0ULL - d < w ? ~0ULL : d + w;
+        if (e > begin && nbr[e] <= nbr[e - 1]) flags |= 1u;
+        if (!w) flags |= 2u;
+        if (w != 1) flags |= 4u;
+    }
+#pragma unroll
+    for (int s = W / 2; s; s >>= 1) {
+        const u64 o = __shfl_xor_sync(0xffffffffu, d, s, W);
+        d = ~0ULL - d < o ? ~0ULL : d + o;
+        flags |= __shfl_xor_sync(0xffffffffu, flags, s, W);
+    }
+    if (valid && lane == 0) {
+        bounds[v] = d;
+        atomicMax(&s_max, d);
+        atomicMax(&s_raw, static_cast<u64>(end - begin));
+        atomicAdd(&s_total, static_cast<u64>(vw[v]));
+        atomicMax(&s_vmax, static_cast<u64>(vw[v]));
+        if (flags) atomicOr(&s_flags, flags);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicMax(sc + 0, s_max);
+        if (s_flags & 1u) atomicOr(sc + 1, 1ULL);
+        if (s_flags & 2u) atomicOr(sc + 2, 1ULL);
+        if (s_flags & 4u) atomicOr(sc + 3, 1ULL);
+        atomicMax(sc + 4, s_raw);
+        atomicAdd(sc + 5, s_total);
+        atomicMax(sc + 6, s_vmax);
+    }
+}
+
+// Directed edge-weight sum (packed-weight decision, src/coarsen.cu:1839-1848).
+__global__ void k_weight_sum(i64 m, const u32* ew, u64* out) {
+    u64 s = 0;
+    for (i64 e = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += static_cast<i64>(gridDim.x) * blockDim.x)
+        s += ew[e];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+// Degree classes (sclp_compact_degree_classes, aggregation.cuh:5-71): exact
+// max degree, heavy flag and class lists.  Scalars: 0 max degree, 1 heavy,
+// 2..5 list sizes (low, medium, large, heavy), 6 heavy hash slots,
+// 7 isolated vertices.
+__global__ void k_degree_classes(i64 n, const int* off, int* low, int* medium, int* large, int* heavy, u64* sc) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = v < n;
+    const i64 deg = valid ? off[v + 1] - off[v] : 0;
+    const u32 dmax = __reduce_max_sync(0xffffffffu, static_cast<u32>(deg));
+    if (lane == 0 && dmax) atomicMax(sc + 0, static_cast<u64>(dmax));
+    if (__any_sync(0xffffffffu, valid && deg >= 4096) && lane == 0) atomicOr(sc + 1, 1ULL);
+    const int cls = !valid ? -1 : deg <= kLowDegree ? 0 : deg <= kMediumDegree ? 1 : deg <= kLargeDegree ? 2 : 3;
+    int* lists[4] = {low, medium, large, heavy};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const unsigned mask = __ballot_sync(0xffffffffu, cls == c);
+        if (!mask) continue;
+        u64 base = 0;
+        if (lane == 0) base = atomicAdd(sc + 2 + c, static_cast<u64>(__popc(mask)));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (cls == c) lists[c][base + __popc(mask & ((1u << lane) - 1u))] = static_cast<int>(v);
+    }
+    const unsigned iso = __ballot_sync(0xffffffffu, valid && deg == 0);
+    if (iso && lane == 0) atomicAdd(sc + 7, static_cast<u64>(__popc(iso)));
+}
+
+__host__ __device__ inline u64 heavy_slots(i64 deg) {
+    u64 s = kLargeHash;
+    while (s < 2 * static_cast<u64>(deg)) s <<= 1;
+    return s;
+}
+
+struct HeavySlots {
+    const int* rows;
+    const int* off;
+    __device__ u64 operator()(i64 i) const { return heavy_slots(off[rows[i] + 1] - off[rows[i]]); }
+};
+
+// ---------------------------------------------------------------- seed matching
+
+// matching_choose (seed_matching.cuh:12-71): heaviest capacity-feasible
+// neighbour; ties by the symmetric hash, then the larger id.
+template <int W>
+__global__ void k_match_choose(i64 n, const int* off, const int* nbr, const u32* ew, const u32* vw, u64 capacity,
+                               u32 salt, int* choice) {
+    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+    const int lane = threadIdx.x & (W - 1);
+    const bool valid = v < n;
+    int best = -1;
+    u32 bw = 0, bh = 0;
+    if (valid && off[v + 1] - off[v] <= 1024) {
+        const u64 weight = vw[v];
+        for (i64 e = off[v] + lane; e < off[v + 1]; e += W) {
+            const int u = nbr[e];
+            if (u == v || weight > capacity || static_cast<u64>(vw[u]) > capacity - weight) continue;
+            const int lo = min(static_cast<int>(v), u), hi = max(static_cast<int>(v), u);
+            const u32 h = mix32(static_cast<u32>(lo) ^ mix32(static_cast<u32>(hi) ^ salt));
+            const u32 w = edge_w(ew, e);
+            if (best < 0 || w > bw || (w == bw && (h > bh || (h == bh && u > best)))) { best = u; bw = w; bh = h; }
+        }
+    }
+#pragma unroll
+    for (int d = W / 2; d; d >>= 1) {
+        const int ob = __shfl_xor_sync(0xffffffffu, best, d, W);
+        const u32 ow = __shfl_xor_sync(0xffffffffu, bw, d, W);
+        const u32 oh = __shfl_xor_sync(0xffffffffu, bh, d, W);
+        if (ob >= 0 && (best < 0 || ow > bw || (ow == bw && (oh > bh || (oh == bh && ob > best))))) { best = ob; bw = ow; bh = oh; }
+    }
+    if (valid && lane == 0) choice[v] = best;
+}
+
+// matching_commit + matching_roots + residual_seed_weights.
+__global__ void k_match_roots(i64 n, const int* choice, int* clusters) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int u = choice[v];
+    int root = static_cast<int>(v);
+    if (u >= 0 && choice[u] == v) root = min(static_cast<int>(v), u);
+    clusters[v] = root;
+}
+
+__global__ void k_cluster_weights(i64 n, const int* clusters, const u32* vw, u64* cw) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n) atomicAdd(cw + clusters[v], static_cast<u64>(vw[v]));
+}
+
+__global__ void k_count_nonzero(i64 n, const u64* values, u64* out) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const unsigned b = __ballot_sync(0xffffffffu, i < n && values[i] != 0);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(out, static_cast<u64>(__popc(b)));
+}
+
+// ---------------------------------------------------------------- rounds
+
+struct RoundParams {
+    const int* off;
+    const int* nbr;
+    const u32* ew;
+    const u32* vw;
+    const int* clusters;
+    const u64* cw;
+    const unsigned char* roles;
+    u64 capacity;
+    u32 tie_salt;
+    bool filter_roles;  // receivers only, with admissibility
+    bool second_on;     // regret needed
+    int* proposals;
+    u64* gains;
+    u64* regret;
+    u32* ties;
+};
+
+// residual_freeze_roles (singleton_growth.cuh:27-40); also resets proposals.
+__global__ void k_roles(i64 n, const int* clusters, const u32* vw, const u64* cw, u32 salt, u32 threshold,
+                        bool all_singletons, unsigned char* roles, int* proposals) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    roles[v] = clusters[v] == v && cw[v] == static_cast<u64>(vw[v]) &&
+               (all_singletons || mix32(static_cast<u32>(v) ^ salt) < threshold);
+    proposals[v] = kInvalid;
+}
+
+// Candidate summary of one row: best (value, tie) with the reference's
+// zero-value rule, the runner-up value and the connection to the own cluster.
+struct Summary {
+    u64 current, best, tie, second;
+};
+
+__device__ __forceinline__ bool better(u64 a, u64 ta, u64 b, u64 tb) {  // sclp_better_candidate
+    return a > b || (a == b && a != 0 && ta > tb);
+}
+__device__ __forceinline__ void add_candidate(Summary& s, u64 value, u64 tie) {  // sclp_update_two
+    if (better(value, tie, s.best, s.tie)) {
+        s.second = max(s.second, s.best);
+        s.best = value;
+        s.tie = tie;
+    } else s.second = max(s.second, value);
+}
+__device__ __forceinline__ void merge(Summary& s, const Summary& o) {
+    s.current = max(s.current, o.current);
+    if (better(o.best, o.tie, s.best, s.tie)) {
+        s.second = max(max(s.second, o.second), s.best);
+        s.best = o.best;
+        s.tie = o.tie;
+    } else s.second = max(max(s.second, o.second), o.best);
+}
+template <int W>
+__device__ __forceinline__ void reduce_summary(Summary& s) {
+#pragma unroll
+    for (int d = W / 2; d; d >>= 1) {
+        Summary o;
+        o.current = __shfl_xor_sync(0xffffffffu, s.current, d, W);
+        o.best = __shfl_xor_sync(0xffffffffu, s.best, d, W);
+        o.tie = __shfl_xor_sync(0xffffffffu, s.tie, d, W);
+        o.second = __shfl_xor_sync(0xffffffffu, s.second, d, W);
+        merge(s, o);
+    }
+}
+
+// One distinct neighbour cluster `c` with connection `conn`.
+__device__ __forceinline__ void consider(const RoundParams& p, Summary& s, int v, int src, int c, u64 conn) {
+    if (c == src) { s.current = conn; return; }
+    if (p.filter_roles) {
+        if (p.roles[c]) return;
+        const u64 base = p.cw[c];
+        if (!(base != 0 && base <= p.capacity && p.cw[src] <= p.capacity - base)) return;
+    }
+    const u64 tie = (static_cast<u64>(mix32(static_cast<u32>(v) ^ mix32(static_cast<u32>(c)) ^ p.tie_salt)) << 32) |
+                    (0xffffffffULL - static_cast<u32>(c));
+    add_candidate(s, conn, tie);
+}
+
+// sclp_decode_gain_kernel (aggregation.cuh:513-557) for a mover row.
+__device__ __forceinline__ void decode(const RoundParams& p, int v, int src, const Summary& s) {
+    const u64 gain = s.best > s.current ? s.best - s.current : 0;
+    if (!gain) return;
+    const int target = static_cast<int>(0xffffffffULL - (s.tie & 0xffffffffULL));
+    if (target < 0 || target == src) return;
+    p.proposals[v] = target;
+    p.gains[v] = gain;
+    if (p.second_on) p.regret[v] = s.best - s.second;
+    p.ties[v] = static_cast<u32>(s.tie >> 32);
+}
+
+__device__ __forceinline__ bool is_mover(const RoundParams& p, int v, int& src) {
+    src = p.clusters[v];
+    return p.roles[src] != 0;
+}
+
+// Rows of degree <= 8: one 8-lane group per row; equal clusters are grouped
+// with match_any (sclp_affinity_low_match_kernel, aggregation.cuh:268-341).
+__global__ void k_affinity_low(i64 count, const int* rows, RoundParams p) {
+    const int lane = threadIdx.x & 31, sub = lane & 7;
+    const i64 index = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+    int v = -1, src = -1;
+    bool row = index < count;
+    if (row) {
+        v = rows ? rows[index] : static_cast<int>(index);
+        row = is_mover(p, v, src);
+    }
+    bool valid = false;
+    int c = kInvalid;
+    u64 w = 0;
+    if (row) {
+        const i64 begin = p.off[v], deg = p.off[v + 1] - begin;
+        if (sub < deg) {
+            const int u = p.nbr[begin + sub];
+            if (u != v) { valid = true; c = p.clusters[u]; w = edge_w(p.ew, begin + sub); }
+        }
+    }
+    // Group equal clusters only among this row's 8 lanes.
+    const unsigned active = __ballot_sync(0xffffffffu, valid) & (0xffu << (lane & 24));
+    Summary s{0, 0, 0, 0};
+    if (valid) {
+        const unsigned peers = __match_any_sync(active, c);
+        u64 conn = 0;
+        for (unsigned rem = peers; rem; rem &= rem - 1) conn += __shfl_sync(peers, w, __ffs(rem) - 1);
+        if (lane == __ffs(peers) - 1) consider(p, s, v, src, c, conn);
+    }
+    reduce_summary<8>(s);
+    if (row && sub == 0) decode(p, v, src, s);
+}
+
+// Rows of degree 9..256: one warp per row with a 512-slot shared hash
+// (sclp_affinity_medium_hash_kernel, aggregation.cuh:343-422).
+__global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count, const int* rows, RoundParams p) {
+    __shared__ int keys[kMediumWarps][kMediumHash];
+    __shared__ u64 vals[kMediumWarps][kMediumHash];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (i64 index = static_cast<i64>(blockIdx.x) * kMediumWarps + wib; index < count;
+         index += static_cast<i64>(gridDim.x) * kMediumWarps) {
+        const int v = rows[index];
+        int src;
+        if (!is_mover(p, v, src)) continue;
+        const i64 begin = p.off[v], end = p.off[v + 1];
+        int size = 32;
+        while (size < 2 * (end - begin)) size <<= 1;
+        for (int sl = lane; sl < size; sl += 32) { keys[wib][sl] = -1; vals[wib][sl] = 0; }
+        __syncwarp();
+        for (i64 e = begin + lane; e < end; e += 32) {
+            const int u = p.nbr[e];
+            if (u == v) continue;
+            const int c = p.clusters[u];
+            int sl = static_cast<int>(mix32(static_cast<u32>(c))) & (size - 1);
+            while (true) {
+                const int found = atomicCAS(&keys[wib][sl], -1, c);
+                if (found == -1 || found == c) { atomicAdd(&vals[wib][sl], static_cast<u64>(edge_w(p.ew, e))); break; }
+                sl = (sl + 1) & (size - 1);
+            }
+        }
+        __syncwarp();
+        Summary s{0, 0, 0, 0};
+        for (int sl = lane; sl < size; sl += 32) {
+            const int c = keys[wib][sl];
+            if (c >= 0) consider(p, s, v, src, c, vals[wib][sl]);
+        }
+        reduce_summary<32>(s);
+        if (lane == 0) decode(p, v, src, s);
+        __syncwarp();
+    }
+}
+
+// Rows of degree > 256: a 256-thread block per row with an open-addressing
+// table in shared memory (<= 4096 entries) or in a per-row global region.
+template <bool Global>
+__global__ void __launch_bounds__(256) k_affinity_large(i64 count, const int* rows, const u64* region_offsets,
+                                                        int* global_keys, u64* global_vals, RoundParams p) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ Summary warp_sum_s[8];
+    const int v = rows[blockIdx.x];
+    int src;
+    if (!is_mover(p, v, src)) return;
+    const i64 begin = p.off[v], end = p.off[v + 1];
+    int* keys;
+    u64* vals;
+    u64 size;
+    if (Global) {
+        keys = global_keys + region_offsets[blockIdx.x];
+        vals = global_vals + region_offsets[blockIdx.x];
+        size = heavy_slots(end - begin);
+    } else {
+        vals = reinterpret_cast<u64*>(smem_raw);
+        keys = reinterpret_cast<int*>(vals + kLargeHash);
+        size = 32;
+        while (size < 2 * static_cast<u64>(end - begin)) size <<= 1;
+    }
+    for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) { keys[sl] = -1; vals[sl] = 0; }
+    __syncthreads();
+    for (i64 e = begin + threadIdx.x; e < end; e += blockDim.x) {
+        const int u = p.nbr[e];
+        if (u == v) continue;
+        const int c = p.clusters[u];
+        u64 sl = mix32(static_cast<u32>(c)) & (size - 1);
+        while (true) {
+            const int found = atomicCAS(&keys[sl], -1, c);
+            if (found == -1 || found == c) { atomicAdd(&vals[sl], static_cast<u64>(edge_w(p.ew, e))); break; }
+            sl = (sl + 1) & (size - 1);
+        }
+    }
+    __syncthreads();
+    Summary s{0, 0, 0, 0};
+    for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) {
+        const int c = keys[sl];
+        if (c >= 0) consider(p, s, v, src, c, vals[sl]);
+    }
+    reduce_summary<32>(s);
+    if ((threadIdx.x & 31) == 0) warp_sum_s[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < 8 ? warp_sum_s[threadIdx.x] : Summary{0, 0, 0, 0};
+        reduce_summary<32>(s);
+        if (threadIdx.x == 0) decode(p, v, src, s);
+    }
+}
+
+// Admission (src/coarsen.cu:1015-1075).  Total demand per target first;
+// requests to a target whose whole demand fits are accepted without any
+// ordering, the rest are ordered by (target, regret desc, tie desc, vertex).
+__global__ void k_requests(i64 n, const int* proposals, const u32* vw, u64* demand) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n && proposals[v] != kInvalid) atomicAdd(demand + proposals[v], static_cast<u64>(vw[v]));
+}
+
+// accept: 0 reject, 1 accept, 2 needs the ordered prefix test.
+__global__ void k_classify(i64 n, const int* proposals, const u64* cw, const u64* demand, u64 capacity,
+                           unsigned char* accept) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int t = proposals[v];
+    if (t == kInvalid) { accept[v] = 0; return; }
+    const u64 base = cw[t];
+    accept[v] = base > capacity ? 0 : demand[t] <= capacity - base ? 1 : 2;
+}
+
+struct NeedsOrder {
+    const unsigned char* accept;
+    __device__ bool operator()(i64 v) const { return accept[v] == 2; }
+};
+struct HasValue {
+    const int* values;
+    __device__ bool operator()(i64 v) const { return values[v] != kInvalid; }
+};
+
+// Keys for the LSD passes over an ordered list of vertices.
+__global__ void k_key_tie(i64 count, const u32* items, const u32* ties, u64* keys) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) keys[i] = static_cast<u64>(~ties[items[i]]);
+}
+__global__ void k_key_gain(i64 count, const u32* items, const u64* gains, u64 mask, u64* keys) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) keys[i] = mask - (gains[items[i]] & mask);
+}
+__global__ void k_key_target(i64 count, const u32* items, const int* targets, u64* keys) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) keys[i] = static_cast<u64>(targets[items[i]]);
+}
+
+// Segment heads of an ordered list grouped by target.
+__global__ void k_segment_heads(i64 count, const u32* items, const int* targets, const u64* prefix, u64* segment_base,
+                                int* segment_first) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int t = targets[items[i]];
+    if (i == 0 || targets[items[i - 1]] != t) {
+        if (segment_base) segment_base[t] = prefix[i];
+        if (segment_first) segment_first[t] = static_cast<int>(i);
+    }
+}
+
+struct OrderedWeight {
+    const u32* items;
+    const u32* vw;
+    __device__ u64 operator()(i64 i) const { return vw[items[i]]; }
+};
+
+// sclp_commit_kernel's test (aggregation.cuh:641): base <= C and the
+// inclusive weight prefix within the target fits in C - base.
+__global__ void k_ordered_accept(i64 count, const u32* items, const int* targets, const u32* vw, const u64* prefix,
+                                 const u64* segment_base, const u64* cw, u64 capacity, unsigned char* accept) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = static_cast<int>(items[i]);
+    const int t = targets[v];
+    const u64 base = cw[t];
+    const u64 inclusive = prefix[i] + vw[v] - segment_base[t];
+    accept[v] = base <= capacity && inclusive <= capacity - base;
+}
+
+__global__ void k_commit(i64 n, const int* proposals, const unsigned char* accept, const u32* vw, int* clusters,
+                         u64* cw) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int t = proposals[v];
+    if (t == kInvalid || (accept && accept[v] != 1)) return;
+    const u64 w = vw[v];
+    atomicAdd(cw + clusters[v], 0ULL - w);
+    atomicAdd(cw + t, w);
+    clusters[v] = t;
+}
+
+// ---------------------------------------------------------------- isolated, two-hop
+
+struct IsolatedWeight {
+    const int* list;
+    const u32* vw;
+    __device__ u64 operator()(i64 i) const { return vw[list[i]]; }
+};
+struct IsIsolated {
+    const int* off;
+    __device__ bool operator()(i64 v) const { return off[v] == off[v + 1]; }
+};
+
+// isolated_representative_kernel / isolated_commit_kernel (aggregation.cuh:713-745);
+// `prefix` is exclusive here.
+__global__ void k_isolated_rep(i64 count, const int* list, const u64* prefix, const u32* vw, u64 capacity, int* reps) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = list[i];
+    const u64 incl = prefix[i] + vw[v];
+    const u64 fb = prefix[i] / capacity, lb = (incl - 1) / capacity;
+    if (fb == lb) atomicMin(reps + fb, v);
+}
+__global__ void k_isolated_commit(i64 count, const int* list, const u64* prefix, const u32* vw, u64 capacity,
+                                  const int* reps, int* clusters, u64* cw) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = list[i];
+    const u64 incl = prefix[i] + vw[v];
+    const u64 fb = prefix[i] / capacity, lb = (incl - 1) / capacity;
+    if (fb != lb) return;
+    const int t = reps[fb];
+    if (t == v) return;
+    clusters[v] = t;
+    cw[v] = 0;
+    atomicAdd(cw + t, static_cast<u64>(vw[v]));
+}
+
+// sclp_singleton_favorite_kernel (aggregation.cuh:654-664).
+__global__ void k_favorites(i64 n, const u32* vw, const u64* cw, const int* clusters, int* proposals) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n && cw[clusters[v]] != static_cast<u64>(vw[v])) proposals[v] = kInvalid;
+}
+
+// sclp_pair_flags_kernel (aggregation.cuh:666-676): even 1-based ranks inside
+// a favourite's group pair with their predecessor when both fit.
+__global__ void k_pair_flags(i64 count, const u32* items, const int* favorites, const int* segment_first,
+                             const u32* vw, u64 capacity, u32* flags) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = static_cast<int>(items[i]);
+    const i64 rank = i - segment_first[favorites[v]] + 1;
+    flags[i] = (rank % 2 == 0) && i > 0 && static_cast<u64>(vw[items[i - 1]]) <= capacity - vw[v];
+}
+struct LoadU32 {
+    const u32* p;
+    __device__ u32 operator()(i64 i) const { return p[i]; }
+};
+// sclp_two_hop_pair_commit_kernel (aggregation.cuh:678-696).
+__global__ void k_pair_commit(i64 count, const u32* items, const u32* flags, const u32* positions, u64 budget,
+                              const u32* vw, int* clusters, u64* cw) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count || !flags[i] || positions[i] >= budget) return;
+    const int v = static_cast<int>(items[i]);
+    const int s = clusters[v], t = clusters[items[i - 1]];
+    if (s == t) return;
+    const u64 w = vw[v];
+    atomicAdd(cw + s, 0ULL - w);
+    atomicAdd(cw + t, w);
+    clusters[v] = t;
+}
+
+// ---------------------------------------------------------------- compaction
+
+struct NonEmptyInt {
+    const u64* cw;
+    __device__ int operator()(i64 i) const { return cw[i] > 0 ? 1 : 0; }
+};
+__global__ void k_iota_clusters(i64 n, const u32* vw, int* clusters, u64* cw) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    clusters[v] = static_cast<int>(v);
+    cw[v] = vw[v];
+}
+__global__ void k_count_isolated(i64 n, const int* off, u64* out) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const unsigned b = __ballot_sync(0xffffffffu, v < n && off[v] == off[v + 1]);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(out, static_cast<u64>(__popc(b)));
+}
+__global__ void k_map(i64 n, const int* clusters, const int* ids, const u32* vw, int* map, u32* cvw) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int c = ids[clusters[v]];
+    map[v] = c;
+    atomicAdd(cvw + c, vw[v]);
+}
+__global__ void k_max_u32(i64 n, const u32* values, u64* out) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const u32 v = i < n ? values[i] : 0u;
+    const u32 m = __reduce_max_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, static_cast<u64>(m));
+}
+
+// ---------------------------------------------------------------- contraction
+
+// contract_record_bounds (src/coarsen.cu:101-120) plus raw row sizes and
+// member counts.
+__global__ void k_contract_bounds(i64 n, const int* map, const int* off, const u64* fine_bounds, u64* coarse_bounds,
+                                  int* raw, bool bounded) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int c = map[v];
+    atomicAdd(raw + c, off[v + 1] - off[v]);
+    const u64 a = fine_bounds[v];
+    if (bounded) { atomicAdd(coarse_bounds + c, a); return; }
+    u64 prev = atomicCAS(coarse_bounds + c, 0ULL, 0ULL);
+    while (true) {
+        const u64 sum = ~0ULL - prev < a ? ~0ULL : prev + a;
+        const u64 seen = atomicCAS(coarse_bounds + c, prev, sum);
+        if (seen == prev) break;
+        prev = seen;
+    }
+}
+__global__ void k_max_pair(i64 n, const u64* a, const int* b, u64* out) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const u64 x = i < n ? a[i] : 0, y = i < n ? static_cast<u64>(b[i]) : 0;
+    const u64 mx = warp_max(x), my = warp_max(y);
+    if ((threadIdx.x & 31) == 0) { if (mx) atomicMax(out, mx); if (my) atomicMax(out + 1, my); }
+}
+
+struct LoadInt {
+    const int* p;
+    __device__ int operator()(i64 i) const { return p[i]; }
+};
+
+// contraction_row_scatter (contraction_rows.cuh:18-38): every fine row is
+// copied into its coarse row's raw segment; intra-cluster entries -> INT_MAX.
+__global__ void k_scatter(i64 n, const int* off, const int* nbr, const u32* ew, const int* map, int* cursor,
+                          int* raw_t, u32* raw_w) {
+    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+    const int lane = threadIdx.x & 7;
+    if (v >= n) return;
+    const int c = map[v];
+    const int begin = off[v], end = off[v + 1];
+    int out = 0;
+    if (lane == 0) out = atomicAdd(cursor + c, end - begin);
+    out = __shfl_sync(0xffu << (threadIdx.x & 24), out, 0, 8);
+    for (int e = begin + lane; e < end; e += 8) {
+        const int t = map[nbr[e]];
+        raw_t[out + e - begin] = t == c ? INT_MAX : t;
+        raw_w[out + e - begin] = edge_w(ew, e);
+    }
+}
+
+// Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 larger.
+__global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u64* sc) {
+    const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int r = c < nc ? raw[c] : 0;
+    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kLargeDegree ? 2 : 3;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const unsigned mask = __ballot_sync(0xffffffffu, cls == k);
+        if (!mask) continue;
+        u64 base = 0;
+        if (lane == 0) base = atomicAdd(sc + k, static_cast<u64>(__popc(mask)));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (cls == k) lists[k * stride + base + __popc(mask & ((1u << lane) - 1u))] = static_cast<int>(c);
+    }
+    if (cls == 3) atomicAdd(sc + 4, static_cast<u64>(r));
+}
+
+// contraction_warp_sort / contraction_sort_row (contraction_rows.cuh:40-116):
+// striped bitonic network over Items*32 keys, then a segmented warp scan
+// that sums equal keys; writes the unique sorted run back at `begin`.
+template <int Items>
+__device__ void warp_sort_row(int begin, int degree, int* keys_io, u32* w_io, int lane, int* count_out) {
+    int keys[Items];
+    u32 vals[Items];
+#pragma unroll
+    for (int it = 0; it < Items; ++it) {
+        const int pos = lane + 32 * it;
+        keys[it] = pos < degree ? keys_io[begin + pos] : INT_MAX;
+        vals[it] = pos < degree ? w_io[begin + pos] : 0u;
+    }
+    for (int size = 2; size <= 32 * Items; size <<= 1) {
+        for (int dist = size >> 1; dist; dist >>= 1) {
+            int nk[Items];
+            u32 nv[Items];
+#pragma unroll
+            for (int it = 0; it < Items; ++it) {
+                const int index = it * 32 + lane;
+                int ok;
+                u32 ov;
+                if (dist >= 32) {
+                    ok = keys[it ^ (dist / 32)];
+                    ov = vals[it ^ (dist / 32)];
+                } else {
+                    ok = __shfl_xor_sync(0xffffffffu, keys[it], dist);
+                    ov = __shfl_xor_sync(0xffffffffu, vals[it], dist);
+                }
+                const bool lower = ((index & dist) == 0) == ((index & size) == 0);
+                const bool take = lower ? ok < keys[it] : ok > keys[it];
+                nk[it] = take ? ok : keys[it];
+                nv[it] = take ? ov : vals[it];
+            }
+#pragma unroll
+            for (int it = 0; it < Items; ++it) { keys[it] = nk[it]; vals[it] = nv[it]; }
+        }
+    }
+    int count = 0;
+    int carry_key = INT_MAX;
+    u32 carry_sum = 0;
+#pragma unroll
+    for (int it = 0; it < Items; ++it) {
+        const int key = keys[it];
+        u32 sum = vals[it];
+        if (!lane && key == carry_key) sum += carry_sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int ok = __shfl_up_sync(0xffffffffu, key, d);
+            const u32 os = __shfl_up_sync(0xffffffffu, sum, d);
+            if (lane >= d && key == ok) sum += os;
+        }
+        const int next_stripe = it + 1 < Items ? keys[it + 1] : INT_MAX;
+        const int following = __shfl_down_sync(0xffffffffu, key, 1);
+        const int following_stripe = __shfl_sync(0xffffffffu, next_stripe, 0);
+        const int next_key = lane < 31 ? following : following_stripe;
+        const bool emit = key != INT_MAX && key != next_key;
+        const unsigned mask = __ballot_sync(0xffffffffu, emit);
+        if (emit) {
+            const int out = begin + count + __popc(mask & ((1u << lane) - 1u));
+            keys_io[out] = key;
+            w_io[out] = sum;
+        }
+        count += __popc(mask);
+        carry_key = __shfl_sync(0xffffffffu, key, 31);
+        carry_sum = __shfl_sync(0xffffffffu, sum, 31);
+    }
+    *count_out = count;
+}
+
+template <bool Long>
+__global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off, int* raw_t, u32* raw_w, int* ucount) {
+    const i64 index = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (index >= count) return;
+    const int c = rows[index];
+    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+    int out = 0;
+    if (Long) {
+        if (degree <= 256) warp_sort_row<8>(begin, degree, raw_t, raw_w, lane, &out);
+        else warp_sort_row<16>(begin, degree, raw_t, raw_w, lane, &out);
+    } else {
+        if (degree <= 32) warp_sort_row<1>(begin, degree, raw_t, raw_w, lane, &out);
+        else if (degree <= 64) warp_sort_row<2>(begin, degree, raw_t, raw_w, lane, &out);
+        else warp_sort_row<4>(begin, degree, raw_t, raw_w, lane, &out);
+    }
+    if (lane == 0) ucount[c] = out;
+}
+
+// Rows of 513..4096 raw entries: bitonic sort in shared memory, then one
+// thread per run of equal keys sums it.
+__global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
+                                                         int* ucount) {
+    __shared__ int keys[kLargeDegree];
+    __shared__ u32 vals[kLargeDegree];
+    __shared__ unsigned char heads[kLargeDegree];
+    __shared__ int scan_smem[9];
+    const int c = rows[blockIdx.x];
+    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+    int size = 1;
+    while (size < degree) size <<= 1;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        keys[i] = i < degree ? raw_t[begin + i] : INT_MAX;
+        vals[i] = i < degree ? raw_w[begin + i] : 0u;
+    }
+    __syncthreads();
+    for (int k = 2; k <= size; k <<= 1)
+        for (int j = k >> 1; j; j >>= 1) {
+            for (int i = threadIdx.x; i < size; i += blockDim.x) {
+                const int x = i ^ j;
+                if (x > i) {
+                    const bool up = (i & k) == 0;
+                    if ((keys[i] > keys[x]) == up) {
+                        const int tk = keys[i]; keys[i] = keys[x]; keys[x] = tk;
+                        const u32 tv = vals[i]; vals[i] = vals[x]; vals[x] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // Head flags and their exclusive scan (16 items per thread).
+    const int per = (size + blockDim.x - 1) / blockDim.x;
+    int local = 0;
+    for (int q = 0; q < per; ++q) {
+        const int i = threadIdx.x * per + q;
+        if (i < size) {
+            const bool h = keys[i] != INT_MAX && (i == 0 || keys[i] != keys[i - 1]);
+            heads[i] = h;
+            local += h;
+        }
+    }
+    int total;
+    int run = block_exclusive_scan<int>(local, total, scan_smem);
+    for (int q = 0; q < per; ++q) {
+        const int i = threadIdx.x * per + q;
+        if (i < size && heads[i]) {
+            u64 sum = 0;
+            for (int j = i; j < size && keys[j] == keys[i]; ++j) sum += vals[j];
+            raw_t[begin + run] = keys[i];
+            raw_w[begin + run] = static_cast<u32>(sum);
+            ++run;
+        }
+    }
+    if (threadIdx.x == 0) ucount[c] = total;
+}
+
+// Rows above 4096 raw entries: records (row rank, target) -> global radix sort.
+__global__ void k_large_records(i64 count, const int* rows, const int* raw_off, const int* rec_off, const int* raw_t,
+                                const u32* raw_w, int tbits, u64* keys, u32* vals) {
+    const int j = blockIdx.x;
+    const int c = rows[j];
+    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+    const int out = rec_off[j];
+    const u64 sentinel = (1ULL << tbits) - 1;
+    for (int i = threadIdx.x; i < degree; i += blockDim.x) {
+        const int t = raw_t[begin + i];
+        keys[out + i] = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
+        vals[out + i] = raw_w[begin + i];
+    }
+}
+struct LargeRowSize {
+    const int* rows;
+    const int* raw_off;
+    __device__ int operator()(i64 i) const { return raw_off[rows[i] + 1] - raw_off[rows[i]]; }
+};
+struct UniqueCount {
+    const int* ucount;
+    i64 nc;
+    __device__ int operator()(i64 i) const { return i < nc ? ucount[i] : 0; }
+};
+struct RecordHead {
+    const u64* keys;
+    u64 sentinel_mask;
+    __device__ u32 operator()(i64 i) const {
+        const u64 k = keys[i];
+        if ((k & sentinel_mask) == sentinel_mask) return 0;
+        return (i == 0 || keys[i - 1] != k) ? 1u : 0u;
+    }
+};
+__global__ void k_large_write(i64 records, const u64* keys, const u32* vals, const u32* hpos, int tbits,
+                              const int* rows, const int* rec_off, const int* raw_off, int* raw_t, u32* raw_w) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= records) return;
+    const u64 k = keys[i];
+    const u64 tmask = (1ULL << tbits) - 1;
+    if ((k & tmask) == tmask || (i > 0 && keys[i - 1] == k)) return;
+    const int j = static_cast<int>(k >> tbits);
+    u64 sum = 0;
+    for (i64 r = i; r < records && keys[r] == k; ++r) sum += vals[r];
+    const int c = rows[j];
+    const int pos = raw_off[c] + static_cast<int>(hpos[i] - hpos[rec_off[j]]);
+    raw_t[pos] = static_cast<int>(k & tmask);
+    raw_w[pos] = static_cast<u32>(sum);
+}
+__global__ void k_large_counts(i64 count, const int* rows, const int* rec_off, const u32* hpos, const u32* total,
+                               i64 records, int* ucount) {
+    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const u32 first = hpos[rec_off[j]];
+    const u32 last = j + 1 < count ? hpos[rec_off[j + 1]] : *total;
+    ucount[rows[j]] = static_cast<int>(last - first);
+}
+
+// contraction_copy_rows (contraction_rows.cuh:140-154).
+__global__ void k_copy_rows(i64 nc, const int* raw_off, const int* raw_t, const u32* raw_w, const int* off, int* nbr,
+                            u32* ew) {
+    const i64 c = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+    const int lane = threadIdx.x & 7;
+    if (c >= nc) return;
+    const int begin = off[c], end = off[c + 1], raw = raw_off[c];
+    for (int e = begin + lane; e < end; e += 8) {
+        nbr[e] = raw_t[raw + e - begin];
+        ew[e] = raw_w[raw + e - begin];
+    }
+}
+
+// ---------------------------------------------------------------- host orchestration
+
+struct Workspace {  // SclpWorkspace::Impl state (src/coarsen.cu:299-396)
+    bool positive = false, unit = false, sorted_unique = false, invariants_known = false;
+    bool packed_weights = false;
+    i64 original_vertices = 0;
+    u64 maximum_row_weight = 0, total_vw = 0, max_vw = 0;
+    u64* row_bounds = nullptr;  // device, current level
+};
+
+struct AggregateOut {
+    int* map = nullptr;
+    u32* cvw = nullptr;
+    i64 nc = 0;
+    u64 max_w = 0, capacity = 0, stats_max_degree = 0;
+    bool stats_heavy = false;
+};
+
+constexpr int kThreads = 256;
+
+// Orders `items` (vertex ids, `count` of them, ascending on entry) by
+// (target asc, key desc, tie desc): three stable LSD stages.
+void order_by_target(Context& ctx, i64 count, u32*& items, u32*& items_alt, const int* targets, const u64* key_values,
+                     int key_bits, const u32* ties, int target_bits) {
+    Arena& A = ctx.scratch;
+    ArenaScope scope(A);
+    u64* keys = A.alloc<u64>(static_cast<size_t>(count));
+    u64* keys_alt = A.alloc<u64>(static_cast<size_t>(count));
+    const int blocks = blocks_for(count, kThreads);
+    launch(k_key_tie, blocks, kThreads, 0, ctx.stream, count, items, ties, keys);
+    radix_sort_pairs(A, ctx.stream, count, keys, items, keys_alt, items_alt, 0, 32);
+    if (key_bits > 0) {
+        const u64 mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
+        launch(k_key_gain, blocks, kThreads, 0, ctx.stream, count, items, key_values, mask, keys);
+        radix_sort_pairs(A, ctx.stream, count, keys, items, keys_alt, items_alt, 0, key_bits);
+    }
+    launch(k_key_target, blocks, kThreads, 0, ctx.stream, count, items, targets, keys);
+    radix_sort_pairs(A, ctx.stream, count, keys, items, keys_alt, items_alt, 0, target_bits);
+}
+
+struct WriteU32Index {
+    u32* dst;
+    __device__ void operator()(u32 slot, i64 i) const { dst[slot] = static_cast<u32>(i); }
+};
+
+class Aggregator {
+public:
+    Aggregator(Context& c, const DGraph& g, Workspace& ws, const CoarsenOptions& o, int level, int factor, u32 seed,
+               bool matching)
+        : ctx(c), g(g), ws(ws), o(o), level(level), factor(factor), seed(seed), matching(matching) {}
+
+    AggregateOut run();
+
+private:
+    Context& ctx;
+    const DGraph& g;
+    Workspace& ws;
+    const CoarsenOptions& o;
+    int level, factor;
+    u32 seed;
+    bool matching;
+
+    int* clusters = nullptr;
+    u64* cw = nullptr;
+    unsigned char* roles = nullptr;
+    int* proposals = nullptr;
+    u64* gains = nullptr;
+    u64* regret = nullptr;
+    u32* ties = nullptr;
+    int* lists[4] = {};
+    i64 list_size[4] = {};
+    u64* heavy_offsets = nullptr;
+    int* heavy_keys = nullptr;
+    u64* heavy_vals = nullptr;
+    int gain_bits = 64, target_bits = 32;
+
+    u64 count_clusters() {
+        ctx.clear_scalars(1);
+        launch(k_count_nonzero, blocks_for(g.n, kThreads), kThreads, 0, ctx.stream, g.n, cw, ctx.dev_scalars);
+        return ctx.read_scalars(1)[0];
+    }
+    void form_proposals(u64 capacity, int round, bool filter_roles, u32 threshold, bool need_regret);
+};
+
+void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 threshold, bool need_regret) {
+    const u32 role_salt = seed ^ (static_cast<u32>(level) * 0x9e3779b9U) ^ (static_cast<u32>(round) * 0x85ebca6bU) ^ 0x27d4eb2dU;
+    const u32 tie_salt = seed ^ (static_cast<u32>(level) * 0xc2b2ae35U) ^ (static_cast<u32>(round) * 0x165667b1U) ^ 0xd3a2646cU;
+    const i64 n = g.n;
+    launch(k_roles, blocks_for(n, kThreads), kThreads, 0, ctx.stream, n, clusters, g.vw, cw, role_salt, threshold,
+                                                                         !filter_roles, roles, proposals);
+    RoundParams p{g.off, g.nbr, g.ew, g.vw, clusters, cw, roles, capacity, tie_salt, filter_roles,
+                  filter_roles && need_regret, proposals, gains, regret, ties};
+    if (list_size[0])
+        launch(k_affinity_low, blocks_for(list_size[0] * 8, kThreads), kThreads, 0, ctx.stream, list_size[0], lists[0], p);
+    if (list_size[1]) {
+        const int blocks = static_cast<int>(std::min<i64>(blocks_for(list_size[1], kMediumWarps), 148 * 64));
+        launch(k_affinity_medium, blocks, kMediumWarps * 32, 0, ctx.stream, list_size[1], lists[1], p);
+    }
+    if (list_size[2]) {
+        const size_t smem = kLargeHash * (sizeof(u64) + sizeof(int));
+        static bool configured = false;
+        if (!configured) {
+            GP_CUDA(cudaFuncSetAttribute(k_affinity_large<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+            configured = true;
+        }
+        launch(k_affinity_large<false>, static_cast<int>(list_size[2]), 256, smem, ctx.stream, 
+            list_size[2], lists[2], static_cast<const u64*>(nullptr), static_cast<int*>(nullptr), static_cast<u64*>(nullptr), p);
+    }
+    if (list_size[3])
+        launch(k_affinity_large<true>, static_cast<int>(list_size[3]), 256, 0, ctx.stream, 
+            list_size[3], lists[3], heavy_offsets, heavy_keys, heavy_vals, p);
+}
+
+AggregateOut Aggregator::run() {
+    Arena& A = ctx.scratch;
+    cudaStream_t s = ctx.stream;
+    const i64 n = g.n;
+    const int vb = blocks_for(n, kThreads);
+    AggregateOut out;
+    const u64 total = ws.total_vw, maxv = ws.max_vw;
+    const u64 denom = static_cast<u64>(factor) * static_cast<u64>(o.parts);
+    out.capacity = std::max(maxv, total / denom + (total % denom != 0));
+    const u64 C = out.capacity;
+
+    clusters = A.alloc<int>(n);
+    cw = A.alloc<u64>(n);
+    roles = A.alloc<unsigned char>(n);
+    proposals = A.alloc<int>(n);
+    gains = A.alloc<u64>(n);
+    regret = A.alloc<u64>(n);
+    ties = A.alloc<u32>(n);
+    i64 cluster_count = n;
+    if (matching) {  // src/coarsen.cu:505-535
+        int* choice = proposals;
+        const u32 salt = seed ^ (static_cast<u32>(level) * 0x9e3779b9U);
+        if (g.m / n < 8)
+            launch(k_match_choose<1>, vb, kThreads, 0, s, n, g.off, g.nbr, g.ew, g.vw, C, salt, choice);
+        else
+            launch(k_match_choose<32>, blocks_for(n * 32, kThreads), kThreads, 0, s, n, g.off, g.nbr, g.ew, g.vw, C, salt, choice);
+        launch(k_match_roots, vb, kThreads, 0, s, n, choice, clusters);
+        GP_CUDA(cudaMemsetAsync(cw, 0, sizeof(u64) * n, s));
+        launch(k_cluster_weights, vb, kThreads, 0, s, n, clusters, g.vw, cw);
+        cluster_count = static_cast<i64>(count_clusters());
+    } else {
+        launch(k_iota_clusters, vb, kThreads, 0, s, n, g.vw, clusters, cw);
+    }
+    // Degree classes, once per level.
+    i64 isolated = 0;
+    {
+        for (int c = 0; c < 4; ++c) lists[c] = nullptr;
+        if (g.maximum_degree <= kLowDegree) {
+            out.stats_max_degree = g.maximum_degree;
+            out.stats_heavy = false;
+            list_size[0] = n;
+            list_size[1] = list_size[2] = list_size[3] = 0;
+            ctx.clear_scalars(1);
+            launch(k_count_isolated, vb, kThreads, 0, s, n, g.off, ctx.dev_scalars);
+            isolated = static_cast<i64>(ctx.read_scalars(1)[0]);
+        } else {
+            int* storage = A.alloc<int>(static_cast<size_t>(n) * 4);
+            for (int c = 0; c < 4; ++c) lists[c] = storage + static_cast<size_t>(n) * c;
+            ctx.clear_scalars(8);
+            launch(k_degree_classes, vb, kThreads, 0, s, n, g.off, lists[0], lists[1], lists[2], lists[3], ctx.dev_scalars);
+            const u64* sc = ctx.read_scalars(8);
+            out.stats_max_degree = sc[0];
+            out.stats_heavy = sc[1] != 0;
+            for (int c = 0; c < 4; ++c) list_size[c] = static_cast<i64>(sc[2 + c]);
+            isolated = static_cast<i64>(sc[7]);
+            if (list_size[3]) {
+                heavy_offsets = A.alloc<u64>(static_cast<size_t>(list_size[3]));
+                u64* slot_total = ctx.dev_scalars;
+                exclusive_scan<u64>(A, s, list_size[3], HeavySlots{lists[3], g.off}, heavy_offsets, slot_total);
+                const u64 slots = ctx.read_scalars(1)[0];
+                heavy_keys = A.alloc<int>(slots);
+                heavy_vals = A.alloc<u64>(slots);
+            }
+        }
+    }
+    // row_gain_bits (src/coarsen.cu:649-656) and target_bits.
+    target_bits = std::max(1, bit_length(static_cast<u64>(n - 1)));
+    gain_bits = std::max(1, std::min(ws.packed_weights ? 32 : 64, bit_length(ws.maximum_row_weight)));
+
+    const i64 desired = (n + 1) / 2;
+    u64 bound = matching ? (maxv > C / 2 ? C : 2 * maxv) : maxv;
+    unsigned char* accept = A.alloc<unsigned char>(n);
+    u64* demand = A.alloc<u64>(n);
+    for (int round = 0; round < 4; ++round) {  // src/coarsen.cu:982-1128
+        if (static_cast<double>(cluster_count) <= 0.60 * n) break;
+        const i64 removable = std::max<i64>(0, cluster_count - desired);
+        const double fraction = std::min(0.50, static_cast<double>(removable) / static_cast<double>(cluster_count));
+        const auto threshold = static_cast<u32>(fraction * 4294967296.0);
+        const u64 room = C - bound;
+        const u64 degree = out.stats_max_degree;
+        const bool all_fit = o.fast_path && (degree == 0 || bound <= room / maxv / degree);
+        const u64 next_bound = all_fit ? bound + bound * degree * maxv : C;
+        form_proposals(C, round, true, threshold, !all_fit);
+        if (all_fit) {
+            launch(k_commit, vb, kThreads, 0, s, n, proposals, static_cast<const unsigned char*>(nullptr), g.vw, clusters, cw);
+        } else {
+            GP_CUDA(cudaMemsetAsync(demand, 0, sizeof(u64) * n, s));
+            launch(k_requests, vb, kThreads, 0, s, n, proposals, g.vw, demand);
+            launch(k_classify, vb, kThreads, 0, s, n, proposals, cw, demand, C, accept);
+            ArenaScope rs(A);
+            u32* items = A.alloc<u32>(n);
+            u32* count_dev = reinterpret_cast<u32*>(ctx.dev_scalars);
+            select_if(A, s, n, NeedsOrder{accept}, WriteU32Index{items}, count_dev);
+            const i64 count = static_cast<i64>(static_cast<u32>(ctx.read_scalars(1)[0] & 0xffffffffULL));
+            if (count > 0) {
+                u32* items_alt = A.alloc<u32>(count);
+                order_by_target(ctx, count, items, items_alt, proposals, regret, gain_bits, ties, target_bits);
+                u64* prefix = A.alloc<u64>(count);
+                exclusive_scan<u64>(A, s, count, OrderedWeight{items, g.vw}, prefix, static_cast<u64*>(nullptr));
+                const int cb = blocks_for(count, kThreads);
+                launch(k_segment_heads, cb, kThreads, 0, s, count, items, proposals, prefix, demand, static_cast<int*>(nullptr));
+                launch(k_ordered_accept, cb, kThreads, 0, s, count, items, proposals, g.vw, prefix, demand, cw, C, accept);
+            }
+            launch(k_commit, vb, kThreads, 0, s, n, proposals, accept, g.vw, clusters, cw);
+        }
+        const i64 before = cluster_count;
+        cluster_count = static_cast<i64>(count_clusters());
+        if (cluster_count > before) fail(GP_INTERNAL, "residual singleton merge accounting failed");
+        bound = next_bound;
+        if (o.log)
+            std::printf("ml_residual_round level=%d round=%d regret_elided=%d clusters=%lld\n", level, round,
+                        all_fit ? 1 : 0, static_cast<long long>(cluster_count));
+        if (static_cast<double>(cluster_count) <= 0.60 * n) break;
+    }
+    if (o.pack_isolated && isolated > 1) {  // src/coarsen.cu:1130-1161
+        ArenaScope is(A);
+        int* list = A.alloc<int>(isolated);
+        u64* prefix = A.alloc<u64>(isolated);
+        select_if(A, s, n, IsIsolated{g.off}, WriteIndex{list}, static_cast<u32*>(nullptr));
+        u64* total_dev = ctx.dev_scalars;
+        exclusive_scan<u64>(A, s, isolated, IsolatedWeight{list, g.vw}, prefix, total_dev);
+        const u64 iso_total = ctx.read_scalars(1)[0];
+        const i64 bins = static_cast<i64>(iso_total / C + (iso_total % C != 0));
+        int* reps = A.alloc<int>(bins);
+        fill<int>(s, reps, bins, INT_MAX);
+        const int ib = blocks_for(isolated, kThreads);
+        launch(k_isolated_rep, ib, kThreads, 0, s, isolated, list, prefix, g.vw, C, reps);
+        launch(k_isolated_commit, ib, kThreads, 0, s, isolated, list, prefix, g.vw, C, reps, clusters, cw);
+        cluster_count = static_cast<i64>(count_clusters());
+    }
+    if (static_cast<double>(cluster_count) > 0.60 * n) {  // two-hop, src/coarsen.cu:1166-1259
+        form_proposals(C, 4, false, 0, false);
+        launch(k_favorites, vb, kThreads, 0, s, n, g.vw, cw, clusters, proposals);
+        ArenaScope ts(A);
+        u32* items = A.alloc<u32>(n);
+        select_if(A, s, n, HasValue{proposals}, WriteU32Index{items}, reinterpret_cast<u32*>(ctx.dev_scalars));
+        const i64 count = static_cast<i64>(static_cast<u32>(ctx.read_scalars(1)[0] & 0xffffffffULL));
+        const u64 budget = static_cast<u64>(std::max<i64>(0, cluster_count - desired));
+        if (count > 0 && budget > 0) {
+            u32* items_alt = A.alloc<u32>(count);
+            order_by_target(ctx, count, items, items_alt, proposals, gains, gain_bits, ties, target_bits);
+            int* first = A.alloc<int>(n);  // first position of every favourite's group
+            const int cb = blocks_for(count, kThreads);
+            launch(k_segment_heads, cb, kThreads, 0, s, count, items, proposals, static_cast<const u64*>(nullptr),
+                                                            static_cast<u64*>(nullptr), first);
+            u32* flags = A.alloc<u32>(count);
+            u32* positions = A.alloc<u32>(count);
+            launch(k_pair_flags, cb, kThreads, 0, s, count, items, proposals, first, g.vw, C, flags);
+            exclusive_scan<u32>(A, s, count, LoadU32{flags}, positions, static_cast<u32*>(nullptr));
+            launch(k_pair_commit, cb, kThreads, 0, s, count, items, flags, positions, budget, g.vw, clusters, cw);
+        }
+        cluster_count = static_cast<i64>(count_clusters());
+    }
+    // Compaction (src/coarsen.cu:1261-1298).
+    {
+        ArenaScope cs(A);
+        int* ids = A.alloc<int>(n);
+        u64* nc_dev = ctx.dev_scalars;
+        GP_CUDA(cudaMemsetAsync(nc_dev, 0, sizeof(u64), s));
+        exclusive_scan<int>(A, s, n, NonEmptyInt{cw}, ids, reinterpret_cast<int*>(nc_dev));
+        out.nc = static_cast<i64>(static_cast<int>(ctx.read_scalars(1)[0] & 0xffffffffULL));
+        out.map = ctx.persist.alloc<int>(n);
+        out.cvw = ctx.persist.alloc<u32>(out.nc);
+        GP_CUDA(cudaMemsetAsync(out.cvw, 0, sizeof(u32) * out.nc, s));
+        launch(k_map, vb, kThreads, 0, s, n, clusters, ids, g.vw, out.map, out.cvw);
+        ctx.clear_scalars(1);
+        launch(k_max_u32, blocks_for(out.nc, kThreads), kThreads, 0, s, out.nc, out.cvw, ctx.dev_scalars);
+        out.max_w = ctx.read_scalars(1)[0];
+    }
+    ws.max_vw = out.max_w;
+    if (out.max_w > C) fail(GP_INTERNAL, "SCLP coarsening exceeded cluster capacity");
+    return out;
+}
+
+
+// contract_typed / contract_short_rows (src/coarsen.cu:1394-1673): the exact
+// coarse CSR plus the carried row bounds and degree metadata.
+DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& ws) {
+    Arena& A = ctx.scratch;
+    cudaStream_t s = ctx.stream;
+    const i64 n = fine.n, nc = agg.nc;
+    const int vb = blocks_for(n, kThreads);
+    u64* next_bounds = ctx.persist.alloc<u64>(nc);
+    ArenaScope scope(A);
+    int* raw = A.alloc<int>(nc + 1);
+    GP_CUDA(cudaMemsetAsync(next_bounds, 0, sizeof(u64) * nc, s));
+    GP_CUDA(cudaMemsetAsync(raw, 0, sizeof(int) * (nc + 1), s));
+    const bool bounded = n > 0 && ws.maximum_row_weight <= ~0ULL / static_cast<u64>(n);
+    launch(k_contract_bounds, vb, kThreads, 0, s, n, agg.map, fine.off, ws.row_bounds, next_bounds, raw, bounded);
+    ctx.clear_scalars(2);
+    launch(k_max_pair, blocks_for(nc, kThreads), kThreads, 0, s, nc, next_bounds, raw, ctx.dev_scalars);
+    const u64* sc = ctx.read_scalars(2);
+    const u64 row_bound = sc[0], raw_max = sc[1];
+    const bool count_raw = ws.positive && n >= 65536 && fine.maximum_degree <= 512;
+    const u64 raw_bound = count_raw ? raw_max : ~0ULL;
+    const u64 degree_bound = count_raw && fine.maximum_degree <= 128 ? raw_bound : row_bound;
+    const bool short_rows = count_raw && raw_bound <= 512;
+
+    // Raw segments of every coarse row, filled by one scatter of the fine CSR.
+    int* raw_off = A.alloc<int>(nc + 1);
+    exclusive_scan<int>(A, s, nc + 1, LoadInt{raw}, raw_off, static_cast<int*>(nullptr));
+    int* cursor = A.alloc<int>(nc);
+    GP_CUDA(cudaMemcpyAsync(cursor, raw_off, sizeof(int) * nc, cudaMemcpyDeviceToDevice, s));
+    int* raw_t = A.alloc<int>(fine.m);
+    u32* raw_w = A.alloc<u32>(fine.m);
+    launch(k_scatter, blocks_for(n * 8, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map, cursor,
+                                                                     raw_t, raw_w);
+    // Row classes by raw size.
+    int* lists = A.alloc<int>(static_cast<size_t>(nc) * 4);
+    ctx.clear_scalars(5);
+    launch(k_row_classes, blocks_for(nc, kThreads), kThreads, 0, s, nc, raw, lists, nc, ctx.dev_scalars);
+    const u64* cls = ctx.read_scalars(5);
+    const i64 count[4] = {static_cast<i64>(cls[0]), static_cast<i64>(cls[1]), static_cast<i64>(cls[2]),
+                          static_cast<i64>(cls[3])};
+    const i64 large_records = static_cast<i64>(cls[4]);
+    int* ucount = raw;  // raw sizes are no longer needed once the classes exist
+    if (count[0])
+        launch(k_sort_rows_warp<false>, blocks_for(count[0] * 32, kThreads), kThreads, 0, s, 
+            count[0], lists, raw_off, raw_t, raw_w, ucount);
+    if (count[1])
+        launch(k_sort_rows_warp<true>, blocks_for(count[1] * 32, kThreads), kThreads, 0, s, 
+            count[1], lists + nc, raw_off, raw_t, raw_w, ucount);
+    if (count[2])
+        launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
+                                                                            ucount);
+    if (count[3]) {
+        ArenaScope ls(A);
+        const int* large = lists + 3 * nc;
+        int* rec_off = A.alloc<int>(count[3]);
+        exclusive_scan<int>(A, s, count[3], LargeRowSize{large, raw_off}, rec_off,
+                            static_cast<int*>(nullptr));
+        const int tbits = bit_length(static_cast<u64>(nc));
+        const int jbits = std::max(1, bit_length(static_cast<u64>(count[3] - 1)));
+        u64* keys = A.alloc<u64>(large_records);
+        u64* keys_alt = A.alloc<u64>(large_records);
+        u32* vals = A.alloc<u32>(large_records);
+        u32* vals_alt = A.alloc<u32>(large_records);
+        launch(k_large_records, static_cast<int>(count[3]), 256, 0, s, count[3], large, raw_off, rec_off, raw_t,
+                                                                         raw_w, tbits, keys, vals);
+        radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, 0, tbits + jbits);
+        u32* hpos = A.alloc<u32>(large_records);
+        u32* heads_total = reinterpret_cast<u32*>(ctx.dev_scalars);
+        exclusive_scan<u32>(A, s, large_records, RecordHead{keys, (1ULL << tbits) - 1}, hpos, heads_total);
+        launch(k_large_write, blocks_for(large_records, kThreads), kThreads, 0, s, 
+            large_records, keys, vals, hpos, tbits, large, rec_off, raw_off, raw_t, raw_w);
+        launch(k_large_counts, blocks_for(count[3], kThreads), kThreads, 0, s, count[3], large, rec_off, hpos,
+                                                                                 heads_total, large_records, ucount);
+    }
+    // Final offsets, then the compact copy into the level's own storage.
+    DGraph coarse;
+    coarse.n = nc;
+    coarse.off = ctx.persist.alloc<int>(nc + 1);
+    u64* m_dev = ctx.dev_scalars + 8;
+    GP_CUDA(cudaMemsetAsync(m_dev, 0, sizeof(u64), s));
+    exclusive_scan<int>(A, s, nc + 1, UniqueCount{ucount, nc}, coarse.off, static_cast<int*>(nullptr));
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, coarse.off + nc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    coarse.m = *reinterpret_cast<const int*>(ctx.host_scalars);
+    coarse.nbr = ctx.persist.alloc<int>(coarse.m);
+    coarse.ew = ctx.persist.alloc<u32>(coarse.m);
+    launch(k_copy_rows, blocks_for(nc * 8, kThreads), kThreads, 0, s, nc, raw_off, raw_t, raw_w, coarse.off,
+                                                                       coarse.nbr, coarse.ew);
+    coarse.vw = agg.cvw;
+    coarse.implicit_unit = false;
+    coarse.incident_bound = row_bound;
+    if (short_rows || ws.positive) {
+        coarse.maximum_degree = degree_bound;
+        coarse.has_heavy_rows = degree_bound >= 4096;
+    }
+    ws.maximum_row_weight = row_bound;
+    ws.row_bounds = next_bounds;
+    return coarse;
+}
+
+}  // namespace
+
+// coarsen_impl (src/coarsen.cu:1762-2060).
+Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
+    cudaStream_t s = ctx.stream;
+    Hierarchy h;
+    Workspace ws;
+    DGraph current = input;
+    if (current.n > 0) {
+        ws.row_bounds = ctx.persist.alloc<u64>(current.n);
+        ctx.clear_scalars(7);
+        if (current.m / current.n < 8)
+            launch(k_level0_meta<8>, blocks_for(current.n * 8, kThreads), kThreads, 0, s, 
+                current.n, current.off, current.nbr, current.ew, current.vw, ws.row_bounds, ctx.dev_scalars);
+        else
+            launch(k_level0_meta<32>, blocks_for(current.n * 32, kThreads), kThreads, 0, s, 
+                current.n, current.off, current.nbr, current.ew, current.vw, ws.row_bounds, ctx.dev_scalars);
+        const u64* sc = ctx.read_scalars(7);
+        ws.original_vertices = current.n;
+        ws.maximum_row_weight = sc[0];
+        current.incident_bound = sc[0];
+        ws.sorted_unique = sc[1] == 0;
+        ws.positive = sc[2] == 0;
+        ws.unit = sc[3] == 0;
+        current.maximum_degree = sc[4];
+        current.has_heavy_rows = sc[4] >= 4096;
+        ws.total_vw = sc[5];
+        ws.max_vw = sc[6];
+        ws.invariants_known = true;
+        if (ws.unit) {
+            ws.packed_weights = static_cast<u64>(current.m) <= 0xffffffffULL;
+        } else {
+            ctx.clear_scalars(1);
+            launch(k_weight_sum, std::min(blocks_for(current.m, kThreads), 148 * 8), kThreads, 0, s, 
+                current.m, current.ew, ctx.dev_scalars);
+            ws.packed_weights = ctx.read_scalars(1)[0] <= 0xffffffffULL;
+        }
+    }
+    const i64 cutoff = std::max<i64>(32, static_cast<i64>(o.cluster_size_factor) * o.parts);
+    for (int level = 0; level < o.max_levels && current.n > cutoff; ++level) {
+        const u32 level_seed = o.seed + static_cast<u32>(level);
+        int factor = o.cluster_size_factor;
+        if (o.progressive) {
+            const i64 fine = std::max(o.fine_factor, (512 + o.parts - 1) / o.parts);
+            const i64 denom = static_cast<i64>(o.growth) * o.parts;
+            const i64 remaining = (current.n + denom - 1) / denom;
+            factor = static_cast<int>(std::max<i64>(factor, std::min<i64>(fine, remaining)));
+        }
+        const i64 avg = current.m / current.n;
+        const bool matching = o.seed_matching && current.n >= 65536 && !current.has_heavy_rows &&
+                              (avg < 8 || current.maximum_degree <= 256) && avg < o.heavy_limit && ws.sorted_unique &&
+                              ws.positive;
+        const Arena::Mark mark = ctx.scratch.mark();
+        Aggregator aggregator(ctx, current, ws, o, level, factor, level_seed, matching);
+        AggregateOut agg = aggregator.run();
+        current.has_heavy_rows = agg.stats_heavy;
+        current.maximum_degree = agg.stats_max_degree;
+        const double ratio = static_cast<double>(agg.nc) / static_cast<double>(current.n);
+        if (o.log)
+            std::printf("ml_coarsen_map level=%d vertices=%lld coarse_vertices=%lld ratio=%g capacity=%llu\n", level,
+                        static_cast<long long>(current.n), static_cast<long long>(agg.nc), ratio,
+                        static_cast<unsigned long long>(agg.capacity));
+        ctx.scratch.release(mark);
+        if (agg.nc >= current.n || ratio > o.stop_ratio) {
+            if (o.log) std::printf("ml_coarsen_stop reason=insufficient_contraction\n");
+            break;
+        }
+        DGraph coarse = contract(ctx, current, agg, ws);
+        ctx.scratch.release(mark);
+        h.levels.push_back(current);
+        h.maps.push_back(agg.map);
+        current = coarse;
+        ws.sorted_unique = true;
+    }
+    h.levels.push_back(current);
+    return h;
+}
+
+void keep_levels(Context& ctx, const Hierarchy& h) {
+    ctx.kept.clear();
+    for (size_t i = 0; i < h.levels.size(); ++i) {
+        const DGraph& g = h.levels[i];
+        Context::HostLevel lv;
+        lv.n = g.n;
+        lv.m = g.m;
+        lv.off.resize(g.n + 1);
+        lv.nbr.resize(g.m);
+        lv.ew.resize(g.m);
+        lv.vw.resize(g.n);
+        GP_CUDA(cudaMemcpy(lv.off.data(), g.off, sizeof(int) * (g.n + 1), cudaMemcpyDeviceToHost));
+        if (g.m) GP_CUDA(cudaMemcpy(lv.nbr.data(), g.nbr, sizeof(int) * g.m, cudaMemcpyDeviceToHost));
+        if (g.ew) { if (g.m) GP_CUDA(cudaMemcpy(lv.ew.data(), g.ew, sizeof(u32) * g.m, cudaMemcpyDeviceToHost)); }
+        else std::fill(lv.ew.begin(), lv.ew.end(), 1u);
+        GP_CUDA(cudaMemcpy(lv.vw.data(), g.vw, sizeof(u32) * g.n, cudaMemcpyDeviceToHost));
+        if (i < h.maps.size()) {
+            lv.map.resize(g.n);
+            GP_CUDA(cudaMemcpy(lv.map.data(), h.maps[i], sizeof(int) * g.n, cudaMemcpyDeviceToHost));
+        }
+        lv.meta[0] = g.maximum_degree;
+        lv.meta[1] = g.has_heavy_rows;
+        lv.meta[2] = g.incident_bound;
+        ctx.kept.push_back(std::move(lv));
+    }
+}
+
+}  // namespace gp

@@ -1,0 +1,138 @@
+// Device-side foundations shared by every kernel file: error handling,
+// the stack arena, launch accounting and small warp/block helpers.
+#pragma once
+#include "gp_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace gp {
+
+using u64 = unsigned long long;
+using i64 = long long;
+using u32 = unsigned int;
+
+// Errors travel as exceptions inside the library and become a gp_status at
+// the C ABI (gp_partition.cu).  No exception crosses that boundary.
+struct Failure : std::runtime_error {
+    gp_status status;
+    Failure(gp_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+[[noreturn]] inline void fail(gp_status s, const std::string& m) { throw Failure(s, m); }
+
+#define GP_CUDA(call)                                                                          \
+    do {                                                                                       \
+        const cudaError_t gp_err__ = (call);                                                   \
+        if (gp_err__ != cudaSuccess)                                                           \
+            ::gp::fail(gp_err__ == cudaErrorMemoryAllocation ? GP_OUT_OF_MEMORY : GP_CUDA_ERROR, \
+                       std::string(#call) + ": " + cudaGetErrorString(gp_err__));             \
+    } while (0)
+
+// Number of kernels this library launched; every launch goes through launch().
+extern thread_local u64 g_launches;
+template <class... Params, class... Args>
+inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                   Args&&... args) {
+    ++g_launches;
+    kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
+}
+
+inline int blocks_for(i64 items, int per_block) {
+    const i64 b = (items + per_block - 1) / per_block;
+    return static_cast<int>(b < 1 ? 1 : b);
+}
+
+// Grow-only chunked stack allocator.  Allocation is a bump inside the current
+// chunk; release() pops back to a mark.  Chunks stay allocated for the next
+// call, so a repeated workload performs no cudaMalloc after its first run.
+class Arena {
+public:
+    struct Mark { size_t chunk, offset; };
+    ~Arena() { reset_device(); }
+    void reset_device() {
+        for (auto& c : chunks_) cudaFree(c.base);
+        chunks_.clear();
+        current_ = 0;
+    }
+    Mark mark() const { return {current_, chunks_.empty() ? 0 : chunks_[current_].top}; }
+    void release(Mark m) {
+        if (chunks_.empty()) return;
+        for (size_t c = m.chunk + 1; c < chunks_.size(); ++c) chunks_[c].top = 0;
+        current_ = m.chunk;
+        chunks_[current_].top = m.offset;
+    }
+    template <class T>
+    T* alloc(size_t count) {
+        return static_cast<T*>(raw(count * sizeof(T)));
+    }
+    void* raw(size_t bytes) {
+        bytes = (bytes + 255) & ~size_t{255};
+        if (bytes == 0) bytes = 256;
+        while (current_ < chunks_.size()) {
+            Chunk& c = chunks_[current_];
+            if (c.top + bytes <= c.size) {
+                void* p = c.base + c.top;
+                c.top += bytes;
+                return p;
+            }
+            if (current_ + 1 < chunks_.size()) { ++current_; chunks_[current_].top = 0; continue; }
+            break;
+        }
+        Chunk c;
+        c.size = bytes > chunk_bytes_ ? bytes : chunk_bytes_;
+        GP_CUDA(cudaMalloc(&c.base, c.size));
+        c.top = bytes;
+        chunks_.push_back(c);
+        current_ = chunks_.size() - 1;
+        return c.base;
+    }
+    void set_chunk_bytes(size_t b) { chunk_bytes_ = b; }
+    size_t reserved() const { size_t s = 0; for (auto& c : chunks_) s += c.size; return s; }
+
+private:
+    struct Chunk { char* base = nullptr; size_t size = 0, top = 0; };
+    std::vector<Chunk> chunks_;
+    size_t current_ = 0;
+    size_t chunk_bytes_ = size_t{256} << 20;
+};
+
+// Scoped release of an arena region.
+struct ArenaScope {
+    Arena& arena;
+    Arena::Mark mark;
+    explicit ArenaScope(Arena& a) : arena(a), mark(a.mark()) {}
+    ~ArenaScope() { arena.release(mark); }
+};
+
+// ---------------------------------------------------------------- device helpers
+
+// mix32 (src/coarsen.cu:173-179, seed_matching.cuh:7, refine.cu:50).
+__host__ __device__ __forceinline__ u32 mix32(u32 x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    return x ^ (x >> 16);
+}
+
+// Order key of the deterministic repair (shared with the oracle).
+__host__ __device__ __forceinline__ u32 repair_hash(int v) { return mix32(static_cast<u32>(v) ^ 0x85ebca6bU); }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v, unsigned mask = 0xffffffffu) {
+    for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(mask, v, d);
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+    for (int d = 16; d; d >>= 1) { const T o = __shfl_xor_sync(0xffffffffu, v, d); v = o > v ? o : v; }
+    return v;
+}
+
+__device__ __forceinline__ u32 edge_w(const u32* w, i64 e) { return w ? w[e] : 1u; }
+
+}  // namespace gp

@@ -1,0 +1,96 @@
+// Device graph, hierarchy and per-call context shared by the pipeline files.
+#pragma once
+#include "gp_device.cuh"
+
+#include <vector>
+
+namespace gp {
+
+constexpr int kInvalid = 0x7fffffff;  // SCLP_INVALID (src/coarsen.cu:292)
+
+// A CSR level on the device (DeviceWeightedGraph, include/graph.hpp:148-171).
+// ew == nullptr means unit edge weights.  The three metadata fields follow
+// the reference's meaning exactly: maximum_degree is a bound (exact after an
+// aggregation pass), incident_bound bounds every row's weight sum.
+struct DGraph {
+    i64 n = 0, m = 0;
+    int* off = nullptr;
+    int* nbr = nullptr;
+    u32* ew = nullptr;
+    u32* vw = nullptr;
+    bool implicit_unit = false;
+    u64 maximum_degree = ~0ULL;
+    bool has_heavy_rows = true;
+    u64 incident_bound = ~0ULL;
+};
+
+struct Hierarchy {
+    std::vector<DGraph> levels;  // level 0 is the input
+    std::vector<int*> maps;      // maps[i]: level i -> level i+1
+};
+
+// Coarsening options, app/partition_main.cu:52-87 with no environment overrides.
+struct CoarsenOptions {
+    int parts = 4;
+    u32 seed = 0;
+    double stop_ratio = 0.90;
+    int max_levels = 24;
+    int cluster_size_factor = 256;
+    bool pack_isolated = true;
+    bool progressive = false;
+    int fine_factor = 64, growth = 8;
+    bool seed_matching = true, fast_path = true;
+    int heavy_limit = 64;
+    bool log = true;
+};
+
+// Device-resident scalars read back in batches through pinned memory.
+constexpr int kScalars = 64;
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Arena persist;  // hierarchy storage for one call
+    Arena scratch;  // stack-disciplined temporaries
+    u64* dev_scalars = nullptr;
+    u64* host_scalars = nullptr;  // pinned
+    cudaEvent_t ev[8] = {};
+    // Kept host copies (GP_FLAG_KEEP_HIERARCHY).
+    struct HostLevel {
+        i64 n = 0, m = 0;
+        std::vector<int> off, nbr, map;
+        std::vector<u32> ew, vw;
+        u64 meta[4] = {0, 0, 0, 0};
+    };
+    std::vector<HostLevel> kept;
+    std::vector<int> initial_labels;
+
+    // Copy `count` device scalars to the host and wait for them.
+    const u64* read_scalars(int count) {
+        GP_CUDA(cudaMemcpyAsync(host_scalars, dev_scalars, sizeof(u64) * count, cudaMemcpyDeviceToHost, stream));
+        GP_CUDA(cudaStreamSynchronize(stream));
+        return host_scalars;
+    }
+    void clear_scalars(int count) {
+        GP_CUDA(cudaMemsetAsync(dev_scalars, 0, sizeof(u64) * count, stream));
+    }
+};
+
+// Entry points of the pipeline stages.
+Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o);
+void keep_levels(Context& ctx, const Hierarchy& h);
+
+struct RefineOutcome {
+    u64 cut = 0;
+    u64 max_load = 0;
+    int levels_refined = 0;
+};
+// Refines from the coarsest level down to level 0 (refine_hierarchy_impl,
+// src/refine.cu:483-730); `labels` (device, level-0 sized) receives the result.
+RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
+                        int* labels, bool log);
+
+// Device edge cut of labels (directed sum / 2); throws on an odd sum.
+u64 device_cut(Context& ctx, const DGraph& g, const int* labels);
+
+}  // namespace gp

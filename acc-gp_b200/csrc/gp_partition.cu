@@ -1,0 +1,358 @@
+// C ABI and pipeline driver: upload -> coarsen -> METIS -> uncoarsen -> labels
+// (the sequence app/partition_main.cu:99-137 runs), on one CUDA stream.
+#include "gp_graph.h"
+#include "gp_metis.h"
+#include "gp_primitives.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+
+struct gp_context {
+    gp::Context ctx;
+    gp::CoarsenOptions defaults;  // overridable per context, see gp_set_option
+    bool seed_matching = true, fast_path = true;
+    int cluster_size_factor = 0, fine_factor = 64, growth = 8, heavy_limit = 64;
+};
+
+namespace gp {
+namespace {
+
+__global__ void k_fill_ones(i64 n, u32* p) {
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        p[i] = 1u;
+}
+
+// Shape and range checks of a device CSR (validate_weighted_shape,
+// src/graph.cpp:118-155).  Scalars: 0 bad offsets, 1 bad neighbour,
+// 2 zero vertex weight, 3 total vertex weight, 4 odd-weight probe (directed
+// edge-weight sum).
+__global__ void k_validate(i64 n, i64 m, const int* off, const int* nbr, const u32* vw, const u32* ew, u64* sc) {
+    u64 total = 0, directed = 0;
+    u32 bad_off = 0, bad_nbr = 0, zero = 0;
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int b = off[v], e = off[v + 1];
+        if (b > e || b < 0 || e > m) { bad_off = 1; continue; }
+        const u32 w = vw ? vw[v] : 1u;
+        zero |= w == 0;
+        total += w;
+        for (int i = b; i < e; ++i) {
+            const int u = nbr[i];
+            bad_nbr |= u < 0 || u >= n;
+            directed += ew ? ew[i] : 1u;
+        }
+    }
+    total = warp_sum(total);
+    directed = warp_sum(directed);
+    bad_off = __any_sync(0xffffffffu, bad_off);
+    bad_nbr = __any_sync(0xffffffffu, bad_nbr);
+    zero = __any_sync(0xffffffffu, zero);
+    if ((threadIdx.x & 31) == 0) {
+        if (bad_off) atomicOr(sc + 0, 1ULL);
+        if (bad_nbr) atomicOr(sc + 1, 1ULL);
+        if (zero) atomicOr(sc + 2, 1ULL);
+        if (total) atomicAdd(sc + 3, total);
+        if (directed) atomicAdd(sc + 4, directed);
+    }
+}
+
+HostCsr download(Context& ctx, const DGraph& g) {
+    HostCsr h;
+    h.n = g.n;
+    h.off.resize(g.n + 1);
+    h.nbr.resize(g.m);
+    h.ew.resize(g.m);
+    h.vw.resize(g.n);
+    cudaStream_t s = ctx.stream;
+    GP_CUDA(cudaMemcpyAsync(h.off.data(), g.off, sizeof(int) * (g.n + 1), cudaMemcpyDeviceToHost, s));
+    if (g.m) GP_CUDA(cudaMemcpyAsync(h.nbr.data(), g.nbr, sizeof(int) * g.m, cudaMemcpyDeviceToHost, s));
+    if (g.ew && g.m) GP_CUDA(cudaMemcpyAsync(h.ew.data(), g.ew, sizeof(u32) * g.m, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaMemcpyAsync(h.vw.data(), g.vw, sizeof(u32) * g.n, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    if (!g.ew) std::fill(h.ew.begin(), h.ew.end(), 1u);
+    return h;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    GP_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+// Compulsory HBM traffic of the V-cycle (the roofline model): per coarsened
+// level 2 CSR sweeps + writing the next level; per refined level one sweep
+// plus the projection.
+u64 algorithmic_bytes(const Hierarchy& h) {
+    u64 bytes = 0;
+    for (size_t i = 0; i < h.levels.size(); ++i) {
+        const DGraph& g = h.levels[i];
+        const u64 n = static_cast<u64>(g.n), m = static_cast<u64>(g.m);
+        const u64 sweep = 4 * (n + 1) + 4 * m + (g.ew ? 4 * m : 0) + 4 * m + 4 * n;
+        if (i + 1 < h.levels.size()) {
+            const DGraph& c = h.levels[i + 1];
+            bytes += 2 * sweep + 4 * (static_cast<u64>(c.n) + 1) + 8 * static_cast<u64>(c.m) + 4 * static_cast<u64>(c.n) + 4 * n;
+        }
+        bytes += sweep + 12 * n;
+    }
+    return bytes;
+}
+
+gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, double eps, uint32_t seed,
+              uint32_t flags, int* labels_out, void* user_stream, gp_stats* stats) {
+    Context& ctx = handle->ctx;
+    if (!in || !labels_out) fail(GP_INVALID_ARGUMENT, "graph and labels must not be NULL");
+    if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(GP_INVALID_ARGUMENT, "invalid partition capacity options");
+    if (in->n <= 0) fail(GP_INVALID_ARGUMENT, "empty CSR indptr");
+    if (in->n > std::numeric_limits<int>::max() || in->m > std::numeric_limits<int>::max() || in->m < 0)
+        fail(GP_INVALID_ARGUMENT, "graph exceeds supported 32-bit CSR limits; dataset excluded");
+    if (!device_input) {
+        if (gp_status s = validate_host_csr(in, true); s != GP_OK) fail(s, last_error());
+    }
+    GP_CUDA(cudaSetDevice(ctx.device));
+    cudaStream_t s = ctx.stream;
+    cudaStream_t caller = static_cast<cudaStream_t>(user_stream);
+    if (caller) {  // order after the caller's producers
+        GP_CUDA(cudaEventRecord(ctx.ev[7], caller));
+        GP_CUDA(cudaStreamWaitEvent(s, ctx.ev[7], 0));
+    }
+    const u64 launches0 = g_launches;
+    ctx.persist.release({0, 0});
+    ctx.scratch.release({0, 0});
+    const i64 n = in->n, m = in->m;
+    DGraph g;
+    g.n = n;
+    g.m = m;
+    GP_CUDA(cudaEventRecord(ctx.ev[0], s));
+    if (device_input) {
+        g.off = const_cast<int*>(in->offsets);
+        g.nbr = const_cast<int*>(in->neighbors);
+        g.ew = const_cast<u32*>(in->edge_weights);
+        g.vw = const_cast<u32*>(in->vertex_weights);
+    } else {
+        g.off = ctx.persist.alloc<int>(n + 1);
+        g.nbr = ctx.persist.alloc<int>(m);
+        GP_CUDA(cudaMemcpyAsync(g.off, in->offsets, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+        if (m) GP_CUDA(cudaMemcpyAsync(g.nbr, in->neighbors, sizeof(int) * m, cudaMemcpyHostToDevice, s));
+        if (in->edge_weights) {
+            g.ew = ctx.persist.alloc<u32>(m);
+            if (m) GP_CUDA(cudaMemcpyAsync(g.ew, in->edge_weights, sizeof(u32) * m, cudaMemcpyHostToDevice, s));
+        }
+        if (in->vertex_weights) {
+            g.vw = ctx.persist.alloc<u32>(n);
+            GP_CUDA(cudaMemcpyAsync(g.vw, in->vertex_weights, sizeof(u32) * n, cudaMemcpyHostToDevice, s));
+        }
+    }
+    if (!g.vw) {
+        g.vw = ctx.persist.alloc<u32>(n);
+        launch(k_fill_ones, std::min(blocks_for(n, 256), 148 * 8), 256, 0, s, n, g.vw);
+    }
+    g.implicit_unit = g.ew == nullptr;
+    GP_CUDA(cudaEventRecord(ctx.ev[1], s));
+    // Device-side validation: it also yields the total weight and the
+    // directed edge-weight sum the reference checks at the end.
+    ctx.clear_scalars(5);
+    launch(k_validate, std::min(blocks_for(n, 256), 148 * 16), 256, 0, s, n, m, g.off, g.nbr, g.vw, g.ew,
+           ctx.dev_scalars);
+    const u64* vs = ctx.read_scalars(5);
+    if (vs[0]) fail(GP_INVALID_ARGUMENT, "weighted CSR offsets are not monotone");
+    if (vs[1]) fail(GP_INVALID_ARGUMENT, "weighted CSR contains an invalid neighbor");
+    if (vs[2]) fail(GP_INVALID_ARGUMENT, "vertex weights must be positive");
+    const u64 total = vs[3], directed = vs[4];
+    uint64_t capacity = 0;
+    if (gp_status st = capacity_of(total, k, eps, &capacity); st != GP_OK) fail(st, last_error());
+
+    CoarsenOptions o;
+    o.parts = k;
+    o.seed = seed;
+    o.cluster_size_factor = handle->cluster_size_factor
+        ? handle->cluster_size_factor
+        : (k <= 8 ? std::max(64, (512 + k - 1) / k) : std::max(2, (32 + k - 1) / k));
+    o.pack_isolated = true;
+    o.progressive = k >= 16;
+    o.fine_factor = handle->fine_factor;
+    o.growth = handle->growth;
+    o.heavy_limit = handle->heavy_limit;
+    o.seed_matching = handle->seed_matching && !(flags & GP_FLAG_NO_SEED_MATCHING);
+    o.fast_path = handle->fast_path;
+    o.log = !(flags & GP_FLAG_QUIET);
+    Hierarchy h = coarsen(ctx, g, o);
+    GP_CUDA(cudaEventRecord(ctx.ev[2], s));
+    if (flags & GP_FLAG_KEEP_HIERARCHY) keep_levels(ctx, h);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (flags & GP_FLAG_COARSEN_ONLY) {
+        GP_CUDA(cudaStreamSynchronize(s));
+        if (stats) {
+            stats->levels = static_cast<int32_t>(h.levels.size());
+            stats->coarsest_vertices = static_cast<int32_t>(h.levels.back().n);
+            stats->coarsen_seconds = elapsed(ctx.ev[1], ctx.ev[2]) * 1e-3;
+            stats->kernel_launches = g_launches - launches0;
+        }
+        return GP_OK;
+    }
+    const auto t_init = std::chrono::steady_clock::now();
+    HostCsr coarsest = download(ctx, h.levels.back());
+    std::vector<int> coarse_labels;
+    std::string error;
+    if (gp_status st = metis_initial_partition(coarsest, k, eps, seed, coarse_labels, error); st != GP_OK) fail(st, error);
+    const double init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_init).count();
+    ctx.initial_labels = coarse_labels;
+    GP_CUDA(cudaEventRecord(ctx.ev[3], s));
+    int* labels_dev = device_input ? labels_out : ctx.persist.alloc<int>(n);
+    RefineOutcome r = uncoarsen(ctx, h, coarse_labels, k, eps, labels_dev, o.log);
+    GP_CUDA(cudaEventRecord(ctx.ev[4], s));
+    if (directed & 1ULL) fail(GP_INTERNAL, "symmetric graph has odd directed edge weight");
+    if (!device_input)
+        GP_CUDA(cudaMemcpyAsync(labels_out, labels_dev, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaEventRecord(ctx.ev[5], s));
+    GP_CUDA(cudaEventSynchronize(ctx.ev[5]));
+    if (caller) {
+        GP_CUDA(cudaEventRecord(ctx.ev[6], s));
+        GP_CUDA(cudaStreamWaitEvent(caller, ctx.ev[6], 0));
+    }
+    if (stats) {
+        stats->edge_cut = r.cut;
+        stats->max_part_weight = r.max_load;
+        stats->capacity = capacity;
+        stats->levels = static_cast<int32_t>(h.levels.size());
+        stats->coarsest_vertices = static_cast<int32_t>(h.levels.back().n);
+        stats->coarsen_seconds = elapsed(ctx.ev[1], ctx.ev[2]) * 1e-3;
+        stats->initial_seconds = init_seconds;
+        stats->uncoarsen_seconds = elapsed(ctx.ev[3], ctx.ev[4]) * 1e-3;
+        stats->algorithm_seconds = elapsed(ctx.ev[1], ctx.ev[4]) * 1e-3;
+        stats->h2d_seconds = device_input ? 0.0 : elapsed(ctx.ev[0], ctx.ev[1]) * 1e-3;
+        stats->d2h_seconds = device_input ? 0.0 : elapsed(ctx.ev[4], ctx.ev[5]) * 1e-3;
+        stats->kernel_launches = g_launches - launches0;
+        stats->algorithmic_bytes = algorithmic_bytes(h);
+    }
+    return GP_OK;
+}
+
+template <class F>
+gp_status guarded(F&& f) {
+    try {
+        return f();
+    } catch (const Failure& e) {
+        set_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return GP_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return GP_INTERNAL;
+    }
+}
+
+}  // namespace
+}  // namespace gp
+
+using namespace gp;
+
+extern "C" {
+
+gp_status gp_context_create(int device, gp_context** out) {
+    return guarded([&]() -> gp_status {
+        if (!out) fail(GP_INVALID_ARGUMENT, "out is NULL");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            fail(GP_NO_DEVICE, "no CUDA device is available");
+        }
+        if (device < 0 || device >= count) fail(GP_INVALID_ARGUMENT, "device ordinal out of range");
+        GP_CUDA(cudaSetDevice(device));
+        auto* h = new gp_context;
+        Context& c = h->ctx;
+        c.device = device;
+        try {
+            GP_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            GP_CUDA(cudaMalloc(&c.dev_scalars, sizeof(u64) * kScalars));
+            GP_CUDA(cudaMallocHost(&c.host_scalars, sizeof(u64) * kScalars));
+            for (auto& e : c.ev) GP_CUDA(cudaEventCreate(&e));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return GP_OK;
+    });
+}
+
+void gp_context_destroy(gp_context* h) {
+    if (!h) return;
+    Context& c = h->ctx;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    c.persist.reset_device();
+    c.scratch.reset_device();
+    if (c.dev_scalars) cudaFree(c.dev_scalars);
+    if (c.host_scalars) cudaFreeHost(c.host_scalars);
+    for (auto& e : c.ev) if (e) cudaEventDestroy(e);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete h;
+}
+
+gp_status gp_partition(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon, uint32_t seed,
+                       uint32_t flags, int32_t* labels_out, gp_stats* stats) {
+    if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
+    return guarded([&] { return run(ctx, graph, false, k, epsilon, seed, flags, labels_out, nullptr, stats); });
+}
+
+gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon, uint32_t seed,
+                              uint32_t flags, int32_t* labels_out_device, void* stream, gp_stats* stats) {
+    if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
+    return guarded([&] { return run(ctx, graph, true, k, epsilon, seed, flags, labels_out_device, stream, stats); });
+}
+
+gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
+    if (!ctx || !name) { set_error("context/name is NULL"); return GP_INVALID_ARGUMENT; }
+    const std::string key(name);
+    if (key == "seed_matching") ctx->seed_matching = value != 0;
+    else if (key == "capacity_safe_fast_path") ctx->fast_path = value != 0;
+    else if (key == "cluster_size_factor" && (value == 0 || (value >= 2 && value <= 256))) ctx->cluster_size_factor = static_cast<int>(value);
+    else if (key == "progressive_fine_factor" && value >= 2 && value <= (1 << 20)) ctx->fine_factor = static_cast<int>(value);
+    else if (key == "progressive_capacity_growth" && value >= 2 && value <= 16) ctx->growth = static_cast<int>(value);
+    else if (key == "heavy_edge_degree_limit" && value >= 2 && value <= 256) ctx->heavy_limit = static_cast<int>(value);
+    else { set_error("unknown option or value out of range: " + key); return GP_INVALID_ARGUMENT; }
+    return GP_OK;
+}
+
+gp_status gp_level_count(gp_context* ctx, int32_t* levels) {
+    if (!ctx || !levels) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    *levels = static_cast<int32_t>(ctx->ctx.kept.size());
+    return GP_OK;
+}
+
+gp_status gp_level_size(gp_context* ctx, int32_t level, int64_t* n, int64_t* m) {
+    if (!ctx || level < 0 || level >= static_cast<int32_t>(ctx->ctx.kept.size())) { set_error("no such level"); return GP_INVALID_ARGUMENT; }
+    if (n) *n = ctx->ctx.kept[level].n;
+    if (m) *m = ctx->ctx.kept[level].m;
+    return GP_OK;
+}
+
+gp_status gp_level_copy(gp_context* ctx, int32_t level, int32_t* offsets, int32_t* neighbors, uint32_t* edge_weights,
+                        uint32_t* vertex_weights, int32_t* map, uint64_t* metadata) {
+    if (!ctx || level < 0 || level >= static_cast<int32_t>(ctx->ctx.kept.size())) { set_error("no such level"); return GP_INVALID_ARGUMENT; }
+    const auto& L = ctx->ctx.kept[level];
+    if (offsets) std::copy(L.off.begin(), L.off.end(), offsets);
+    if (neighbors) std::copy(L.nbr.begin(), L.nbr.end(), neighbors);
+    if (edge_weights) std::copy(L.ew.begin(), L.ew.end(), edge_weights);
+    if (vertex_weights) std::copy(L.vw.begin(), L.vw.end(), vertex_weights);
+    if (map && !L.map.empty()) std::copy(L.map.begin(), L.map.end(), map);
+    if (metadata) std::copy(L.meta, L.meta + 4, metadata);
+    return GP_OK;
+}
+
+gp_status gp_initial_labels(gp_context* ctx, int32_t* labels, int64_t capacity) {
+    if (!ctx || !labels) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    const auto& v = ctx->ctx.initial_labels;
+    if (static_cast<int64_t>(v.size()) > capacity) { set_error("buffer too small"); return GP_INVALID_ARGUMENT; }
+    std::copy(v.begin(), v.end(), labels);
+    return GP_OK;
+}
+
+}  // extern "C"

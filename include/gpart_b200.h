@@ -93,6 +93,14 @@ void gp_context_destroy(gp_context* ctx);
 const char* gp_last_error(void);
 const char* gp_version(void);
 
+/* Coarsening knobs of the reference CLI's environment variables
+ * (app/partition_main.cu:55-87): "seed_matching" (GPART_HEM_COARSEN),
+ * "capacity_safe_fast_path" (GPART_REGRET_FORCE_FULL), "cluster_size_factor"
+ * (GPART_COARSE_BETA, 0 = default rule), "progressive_fine_factor"
+ * (GPART_FINE_FACTOR), "progressive_capacity_growth" (GPART_CAPACITY_GROWTH),
+ * "heavy_edge_degree_limit" (GPART_HEM_DEGREE_LIMIT). */
+gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value);
+
 /* Partition a host CSR.  Copies the graph to the device, runs the V-cycle,
  * copies int32 labels (length n, values in [0,k)) back to labels_out. */
 gp_status gp_partition(gp_context* ctx, const gp_csr* graph, int32_t k,
