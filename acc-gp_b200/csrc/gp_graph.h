@@ -45,7 +45,7 @@ struct CoarsenOptions {
 };
 
 // Device-resident scalars read back in batches through pinned memory.
-constexpr int kScalars = 64;
+constexpr int kScalars = 512;  // >= 2 * kMaxParts + headroom
 
 struct Context {
     int device = 0;

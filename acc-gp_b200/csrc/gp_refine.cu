@@ -1,46 +1,1458 @@
-// Projection and refinement (temporary: projection only).
+// Projection and refinement on the B200 (Acc-GPart src/refine.cu,
+// src/refinement/*.cuh): dense affinity cache, label propagation with the
+// priority filter, exact cut/cache updates, capacity repair and the
+// capacity-complementary exchange.  One host loop per level with one small
+// read-back per LP round; every decision is a pure function of the state, so
+// the result does not depend on thread scheduling.  The repair ranks donors
+// and receiver tickets in the deterministic (bucket, repair hash, id) order.
 #include "gp_graph.h"
 #include "gp_primitives.cuh"
 
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cstdio>
+
 namespace gp {
 namespace {
+
+constexpr int kBalanceWidth = 800;  // kBalanceBuckets * kBalanceSections
+constexpr int kThreads = 256;
+
+struct Sample {
+    long long loss;
+    u64 weight;
+};
+
+// ---------------------------------------------------------------- small kernels
+
 __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, u64* out) {
+    const int lane = threadIdx.x & 31;
     u64 local = 0;
-    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
+    for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
+         v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int p = labels[v];
-        for (int e = off[v]; e < off[v + 1]; ++e) if (labels[nbr[e]] != p) local += edge_w(ew, e);
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32)
+            if (labels[nbr[e]] != p) local += edge_w(ew, e);
     }
     local = warp_sum(local);
-    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+    if (lane == 0 && local) atomicAdd(out, local);
 }
+
 __global__ void k_project(i64 n, const int* map, const int* coarse, int* fine) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (v < n) fine[v] = coarse[map[v]];
 }
+
+__global__ void k_loads(i64 n, int k, const int* labels, const u32* vw, u64* loads) {
+    extern __shared__ u64 part[];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) part[p] = 0;
+    __syncthreads();
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x)
+        atomicAdd(part + labels[v], static_cast<u64>(vw[v]));
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (part[p]) atomicAdd(loads + p, part[p]);
+}
+
+__global__ void k_max_load(int k, const u64* loads, u64* out) {
+    u64 m = 0;
+    for (int p = threadIdx.x; p < k; p += 32) m = max(m, loads[p]);
+    m = warp_max(m);
+    if (threadIdx.x == 0) *out = m;
+}
+
+__global__ void k_max_edge(i64 m, const u32* ew, u64* out) {
+    u32 mx = 0;
+    for (i64 e = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += static_cast<i64>(gridDim.x) * blockDim.x)
+        mx = max(mx, ew[e]);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, static_cast<u64>(mx));
+}
+
+// publish_repair_prices (incremental.cuh:161-164).
+__global__ void k_prices(int k, const Sample* samples, double* prices) {
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (samples[p].weight)
+            prices[p] = samples[p].loss > 0 ? static_cast<double>(samples[p].loss) / static_cast<double>(samples[p].weight) : 0.0;
+}
+
+// Warp-aggregated append of `v` when `active` (append_warp, incremental.cuh:201-208).
+__device__ __forceinline__ void append(int v, bool active, int* queue, u64* count) {
+    const int lane = threadIdx.x & 31;
+    const unsigned mask = __ballot_sync(0xffffffffu, active);
+    u64 base = 0;
+    if (lane == 0 && mask) base = atomicAdd(count, static_cast<u64>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (active) queue[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+// estimated_repair_cost (incremental.cuh:156-160).  Products and sums use
+// explicit round-to-nearest intrinsics so no multiply-add is contracted.
+__device__ __forceinline__ double repair_cost(int part, u64 weight, const u64* loads, u64 capacity, const double* prices) {
+    const u64 slack = capacity - loads[part];
+    return weight > slack ? __dmul_rn(prices[part], static_cast<double>(weight - slack)) : 0.0;
+}
+
+// ---------------------------------------------------------------- affinity cache
+
+// incremental_build_affinity (incremental.cuh:61-140), dense layout: one warp
+// per row accumulates a k-wide histogram in shared memory.
+template <class C>
+__global__ void k_build(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, int k, C* A,
+                        C* totals) {
+    extern __shared__ unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C* row = reinterpret_cast<C*>(smem_raw) + warp * k;
+    for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
+         v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        for (int p = lane; p < k; p += 32) row[p] = 0;
+        __syncwarp();
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+            const int u = nbr[e];
+            if (u != v) atomicAdd(row + labels[u], static_cast<C>(edge_w(ew, e)));
+        }
+        __syncwarp();
+        C total = 0;
+        for (int p = lane; p < k; p += 32) {
+            const C x = row[p];
+            A[static_cast<i64>(v) * k + p] = x;
+            total += x;
+        }
+        total = warp_sum(total);
+        if (lane == 0) totals[v] = total;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- label propagation
+
+struct LpParams {
+    i64 n;
+    int k;
+    u64 capacity;
+    double filter;
+    const int* off;
+    const int* nbr;
+    const u32* ew;
+    const u32* vw;
+    int* labels;
+    u64* loads;
+    const double* prices;  // nullptr: unpriced
+    int* targets;
+    long long* gains;
+    unsigned char* locks;
+    int* flags;
+    int* cand;
+    int* movers;
+    u64* counters;  // 0 candidates, 1 movers, 2 delta (signed), 3 max load
+};
+
+// incremental_lp_proposal (incremental.cuh:166-198) with the warp layout of
+// incremental_warp_lp_proposals (:229-289): W lanes per vertex scan its k
+// affinities; ties keep the lowest part id.
+template <class C, int W>
+__global__ void k_proposals(LpParams q, const C* A, const C* totals) {
+    const int sub = threadIdx.x & (W - 1);
+    const i64 groups = (static_cast<i64>(gridDim.x) * blockDim.x) / W;
+    const i64 rounds = (q.n + groups - 1) / groups;
+    for (i64 r = 0; r < rounds; ++r) {
+        const i64 v = r * groups + (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+        const bool valid = v < q.n;
+        // The group leader resets the slot, consumes the lock and decides
+        // whether the row is a boundary row; the group follows its decision.
+        int act = 0, src = 0;
+        u64 current = 0;
+        if (valid && sub == 0) {
+            q.targets[v] = -1;
+            q.gains[v] = LLONG_MIN;
+            if (q.locks[v]) {
+                q.locks[v] = 0;
+            } else {
+                src = q.labels[v];
+                current = A[v * q.k + src];
+                act = current != static_cast<u64>(totals[v]);
+            }
+        }
+        const bool active = __shfl_sync(0xffffffffu, act, 0, W) != 0;
+        src = __shfl_sync(0xffffffffu, src, 0, W);
+        current = __shfl_sync(0xffffffffu, current, 0, W);
+        int target = -1;
+        u64 best = 0;
+        double best_score = -DBL_MAX;
+        if (active) {
+            const u64 weight = q.vw[v];
+            for (int p = sub; p < q.k; p += W) {
+                const u64 conn = A[v * q.k + p];
+                if (p == src || !conn) continue;
+                if (q.prices) {
+                    const double score = __dsub_rn(static_cast<double>(conn), repair_cost(p, weight, q.loads, q.capacity, q.prices));
+                    if (target < 0 || score > best_score) { target = p; best = conn; best_score = score; }
+                } else if (target < 0 || conn > best) {
+                    target = p;
+                    best = conn;
+                }
+            }
+        }
+#pragma unroll
+        for (int d = W / 2; d; d >>= 1) {
+            const int ot = __shfl_xor_sync(0xffffffffu, target, d, W);
+            const u64 ob = __shfl_xor_sync(0xffffffffu, best, d, W);
+            const double os = __shfl_xor_sync(0xffffffffu, best_score, d, W);
+            if (ot >= 0) {
+                const bool greater = q.prices ? os > best_score : ob > best;
+                const bool equal = q.prices ? os == best_score : ob == best;
+                if (target < 0 || greater || (equal && ot < target)) { target = ot; best = ob; best_score = os; }
+            }
+        }
+        bool propose = false;
+        if (active && sub == 0 && target >= 0 &&
+            (best >= current || current - best < static_cast<u64>(q.filter * static_cast<double>(current)))) {
+            q.targets[v] = target;
+            q.gains[v] = best >= current ? static_cast<long long>(best - current) : -static_cast<long long>(current - best);
+            propose = true;
+        }
+        append(static_cast<int>(v), propose, q.cand, q.counters + 0);
+    }
+}
+
+// incremental_priority_filter (incremental.cuh:361-393): one warp per
+// candidate; a vertex keeps its move when its gain corrected by the intended
+// moves of higher-priority neighbours stays non-negative.
+__global__ void k_filter(LpParams q) {
+    const int lane = threadIdx.x & 31;
+    const i64 count = static_cast<i64>(q.counters[0]);
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        const int v = q.cand[i];
+        const int s = q.labels[v], t = q.targets[v];
+        const long long gain = q.gains[v];
+        long long corr = 0;
+        for (int e = q.off[v] + lane; e < q.off[v + 1]; e += 32) {
+            const int u = q.nbr[e];
+            if (u == v) continue;
+            const int tu = q.targets[u];
+            if (tu < 0) continue;
+            const long long gu = q.gains[u];
+            if (!(gu > gain || (gu == gain && u < v))) continue;
+            const int lu = q.labels[u];
+            corr += static_cast<long long>(edge_w(q.ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+        }
+        corr = warp_sum(corr);
+        if (lane == 0) {
+            bool keep;
+            if (q.prices) {
+                const u64 w = q.vw[v];
+                const double adj = __dsub_rn(repair_cost(s, w, q.loads, q.capacity, q.prices),
+                                             repair_cost(t, w, q.loads, q.capacity, q.prices));
+                keep = __dadd_rn(static_cast<double>(gain + corr), adj) >= 0;
+            } else keep = gain + corr >= 0;
+            q.flags[v] = keep;
+        }
+    }
+}
+
+// Candidates with a kept move -> mover list (incremental_compact_candidates).
+__global__ void k_compact_movers(LpParams q) {
+    const i64 count = static_cast<i64>(q.counters[0]);
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < count; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 i = base + threadIdx.x;
+        const int v = i < count ? q.cand[i] : 0;
+        append(v, i < count && q.flags[v], q.movers, q.counters + 1);
+    }
+}
+
+// incremental_update_cache_and_cut (incremental.cuh:440-506): exact cut delta
+// (an edge whose both ends move is counted by its larger endpoint's partner
+// rule) and dense cache updates; optional repair samples per source part.
+template <class C>
+__global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
+                         const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
+                         C* A, long long* delta, Sample* samples) {
+    const int lane = threadIdx.x & 31;
+    if (live_count) count = static_cast<i64>(*live_count);
+    long long total = 0;
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        const int v = movers[i];
+        const int s = labels[v], t = targets[v];
+        long long gain = 0;
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+            const int u = nbr[e];
+            if (u == v) continue;
+            const int old = labels[u];
+            const bool moves = flags[u] != 0;
+            const int nw = moves ? targets[u] : old;
+            const u32 w = edge_w(ew, e);
+            atomicAdd(A + static_cast<i64>(u) * k + s, static_cast<C>(0) - static_cast<C>(w));
+            atomicAdd(A + static_cast<i64>(u) * k + t, static_cast<C>(w));
+            if (!moves || u > v) gain += static_cast<long long>(w) * ((s != old) - (t != nw));
+        }
+        gain = warp_sum(gain);
+        total += gain;
+        if (samples && lane == 0) {
+            atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
+            atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
+        }
+    }
+    if (lane == 0 && total) atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(total));
+}
+
+// incremental_commit (incremental.cuh:532-547) with per-block aggregation of
+// the part-load changes.
+__global__ void k_commit(i64 count, const int* movers, const u64* live_count, int* labels, const int* targets,
+                         const u32* vw, int k, u64* loads, unsigned char* locks, int* flags) {
+    extern __shared__ long long diff[];
+    if (live_count) count = static_cast<i64>(*live_count);
+    for (int p = threadIdx.x; p < k; p += blockDim.x) diff[p] = 0;
+    __syncthreads();
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = movers[i];
+        const int s = labels[v], t = targets[v];
+        const long long w = vw[v];
+        atomicAdd(reinterpret_cast<u64*>(diff + s), static_cast<u64>(-w));
+        atomicAdd(reinterpret_cast<u64*>(diff + t), static_cast<u64>(w));
+        labels[v] = t;
+        if (locks) locks[v] = 1;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (diff[p]) atomicAdd(loads + p, static_cast<u64>(diff[p]));
+    (void)flags;
+}
+
+__global__ void k_clear_flags(i64 count, const int* movers, const u64* live_count, int* flags) {
+    if (live_count) count = static_cast<i64>(*live_count);
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        flags[movers[i]] = 0;
+}
+
+// ---------------------------------------------------------------- repair
+
+// Deterministic gain bucket: smallest j with 1.5^j >= (current-best)/relief,
+// evaluated exactly (balance_gain_bucket, incremental.cuh:553-557, computes
+// the same ceil(log(x)/log(1.5)) in floating point).
+__device__ int gain_bucket(u64 best, u64 current, u64 relief) {
+    if (best > current) return 0;
+    if (best == current) return 1;
+    const unsigned __int128 G = current - best, R = relief;
+    unsigned __int128 p3 = 1, p2 = 1;  // 3^a, 2^a
+    // j < 0: 2^-j R >= 3^-j G ; check j = -23 .. -1 in increasing order.
+    for (int j = -23; j <= 24; ++j) {
+        unsigned __int128 lhs = R, rhs = G;
+        const int a = j < 0 ? -j : j;
+        p3 = 1;
+        p2 = 1;
+        for (int i = 0; i < a; ++i) { p3 *= 3; p2 *= 2; }
+        if (j >= 0) { lhs *= p3; rhs *= p2; } else { lhs *= p2; rhs *= p3; }
+        if (lhs >= rhs) return max(2, min(49, 25 + j));
+    }
+    return 49;
+}
+
+// initialize_receiver_slack (rebalance_select.cuh:79-104) by one thread.
+__global__ void k_slack(int k, const u64* loads, u64 capacity, u64* slack, u64* requests, u64* cdf) {
+    if (threadIdx.x) return;
+    u64 carry = 0, minimum = ~0ULL;
+    for (int p = 0; p < k; ++p) {
+        const u64 room = loads[p] < capacity ? capacity - loads[p] : 0;
+        slack[p] = room;
+        requests[p] = 0;
+        if (room) minimum = min(minimum, room);
+        carry = ~0ULL - carry < room ? ~0ULL : carry + room;
+        cdf[p] = carry;
+    }
+    cdf[k] = minimum;
+}
+
+struct IsDonor {
+    const u32* order;
+    const int* labels;
+    const u64* loads;
+    u64 capacity;
+    __device__ bool operator()(i64 i) const { return loads[labels[order[i]]] > capacity; }
+};
+struct WriteOrdered {
+    const u32* order;
+    u32* out;
+    __device__ void operator()(u32 slot, i64 i) const { out[slot] = order[i]; }
+};
+
+// enumerate_repair_destination (rebalance_select.cuh:9-75), dense layout, plus
+// the bucket of incremental_rebalance_proposals (incremental.cuh:559-622).
+// One warp per donor.
+template <class C>
+__global__ void k_repair_dest(i64 count, const u32* donors, const C* A, const C* totals, const int* labels,
+                              const u32* vw, int k, const u64* loads, u64 capacity, const u64* cdf, int* targets,
+                              u64* bucket_keys) {
+    const int lane = threadIdx.x & 31;
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        const int v = static_cast<int>(donors[i]);
+        const int src = labels[v];
+        const u64 w = vw[v];
+        const u64 current = A[static_cast<i64>(v) * k + src];
+        int part = -1;
+        u64 conn = 0, best_slack = 0;
+        if (current != static_cast<u64>(totals[v])) {
+            for (int p = lane; p < k; p += 32) {
+                if (p == src || loads[p] >= capacity || w > capacity - loads[p]) continue;
+                const u64 value = A[static_cast<i64>(v) * k + p], slack = capacity - loads[p];
+                if (part < 0 || value > conn || (value == conn && slack > best_slack)) { part = p; conn = value; best_slack = slack; }
+            }
+            for (int d = 16; d; d >>= 1) {
+                const int op = __shfl_xor_sync(0xffffffffu, part, d);
+                const u64 oc = __shfl_xor_sync(0xffffffffu, conn, d);
+                const u64 os = __shfl_xor_sync(0xffffffffu, best_slack, d);
+                if (op >= 0 && (part < 0 || oc > conn || (oc == conn && (os > best_slack || (os == best_slack && op < part))))) {
+                    part = op; conn = oc; best_slack = os;
+                }
+            }
+            if (!conn) part = -1;
+        }
+        if (lane == 0) {
+            if (part < 0) {
+                conn = 0;
+                const u32 hash = mix32(static_cast<u32>(v));
+                if (loads[src] >= capacity && w <= cdf[k]) {
+                    const u64 total = cdf[k - 1];
+                    if (total) {
+                        const u64 ticket = static_cast<u64>(hash) % total;
+                        int lo = 0, hi = k;
+                        while (lo < hi) { const int mid = (lo + hi) / 2; if (cdf[mid] <= ticket) lo = mid + 1; else hi = mid; }
+                        part = lo;
+                    }
+                } else {
+                    u64 total = 0;
+                    for (int p = 0; p < k; ++p)
+                        if (p != src && loads[p] < capacity && w <= capacity - loads[p]) {
+                            const u64 s = capacity - loads[p];
+                            total = ~0ULL - total < s ? ~0ULL : total + s;
+                        }
+                    if (total) {
+                        u64 ticket = static_cast<u64>(hash) % total;
+                        for (int p = 0; p < k; ++p)
+                            if (p != src && loads[p] < capacity && w <= capacity - loads[p]) {
+                                const u64 s = capacity - loads[p];
+                                if (ticket < s) { part = p; break; }
+                                ticket -= s;
+                            }
+                    }
+                }
+            }
+            targets[v] = part;
+            u64 key = ~0ULL;
+            if (part >= 0) {
+                const u64 excess = loads[src] - capacity;
+                const u64 relief = w < excess ? w : excess;
+                key = static_cast<u64>(src) * kBalanceWidth + gain_bucket(conn, current, relief) * 16 +
+                      mix32(static_cast<u32>(v)) % 16;
+            }
+            bucket_keys[i] = key;
+        }
+    }
+}
+
+constexpr u64 kNoBucket = 0xffffffULL;  // donors without a destination sort last
+
+__global__ void k_clamp_keys(i64 count, u64* keys) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count && keys[i] > kNoBucket) keys[i] = kNoBucket;
+}
+__global__ void k_repair_keys(i64 n, u64* keys, u32* order) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    keys[v] = repair_hash(static_cast<int>(v));
+    order[v] = static_cast<u32>(v);
+}
+
+struct SortedWeight {
+    const u32* items;
+    const u32* vw;
+    __device__ u64 operator()(i64 i) const { return vw[items[i]]; }
+};
+
+// Segment base per source part over the bucket-sorted donors.
+__global__ void k_part_heads(i64 count, const u64* keys, const u64* prefix, u64* part_base) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count || keys[i] == kNoBucket) return;
+    const u64 part = keys[i] / kBalanceWidth;
+    if (i == 0 || keys[i - 1] / kBalanceWidth != part) part_base[part] = prefix[i];
+}
+// reserve_receiver_prefixes' donor test (rebalance_graph.cuh:104-107).
+__global__ void k_donor_test(i64 count, const u64* keys, const u32* items, const u64* prefix, const u64* part_base,
+                             const u64* loads, u64 capacity, unsigned char* active) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = static_cast<int>(items[i]);
+    if (keys[i] == kNoBucket) { active[v] = 0; return; }
+    const u64 part = keys[i] / kBalanceWidth;
+    active[v] = prefix[i] - part_base[part] < loads[part] - capacity;
+}
+struct IsActive {
+    const u32* donors;
+    const unsigned char* active;
+    __device__ bool operator()(i64 i) const { return active[donors[i]] != 0; }
+};
+struct WriteFrom {
+    const u32* src;
+    u32* out;
+    __device__ void operator()(u32 slot, i64 i) const { out[slot] = src[i]; }
+};
+
+// One attempt of the receiver reservation: choose a part for every active,
+// unplaced donor (attempt 0: its proposal; later: best affinity among parts
+// not yet tried whose remaining virtual room holds it).
+template <class C>
+__global__ void k_choose(i64 count, const u32* active, int attempt, const C* A, const int* labels, const u32* vw,
+                         int k, const int* proposal, const u64* slack, const u64* requests, u64* tried,
+                         unsigned char* state, int* want, u64* requesters) {
+    const int lane = threadIdx.x & 31;
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        if (state[i]) {  // placed or out of options
+            if (lane == 0) want[i] = -1;
+            continue;
+        }
+        const int v = static_cast<int>(active[i]);
+        const u64 w = vw[v];
+        int target = -1;
+        if (attempt == 0) {
+            target = proposal[v];
+        } else {
+            u64 best = 0, room = 0;
+            for (int p = lane; p < k; p += 32) {
+                if (p == labels[v] || ((tried[2 * i + (p >> 6)] >> (p & 63)) & 1)) continue;
+                const u64 avail = requests[p] < slack[p] ? slack[p] - requests[p] : 0;
+                if (avail < w) continue;
+                const u64 c = A[static_cast<i64>(v) * k + p];
+                if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+            }
+            for (int d = 16; d; d >>= 1) {
+                const int ot = __shfl_xor_sync(0xffffffffu, target, d);
+                const u64 ob = __shfl_xor_sync(0xffffffffu, best, d);
+                const u64 orr = __shfl_xor_sync(0xffffffffu, room, d);
+                if (ot >= 0 && (target < 0 || ob > best || (ob == best && (orr > room || (orr == room && ot < target))))) {
+                    target = ot; best = ob; room = orr;
+                }
+            }
+        }
+        if (lane == 0) {
+            want[i] = target;
+            if (target < 0) state[i] = 2;
+            else atomicAdd(requesters, 1ULL);
+        }
+    }
+}
+
+struct WantsPart {
+    const int* want;
+    __device__ bool operator()(i64 i) const { return want[i] >= 0; }
+};
+struct WriteIdx {
+    u32* out;
+    __device__ void operator()(u32 slot, i64 i) const { out[slot] = static_cast<u32>(i); }
+};
+__global__ void k_want_keys(i64 count, const u32* reqs, const int* want, u64* keys) {
+    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j < count) keys[j] = static_cast<u64>(want[reqs[j]]);
+}
+struct ReqWeight {
+    const u32* reqs;
+    const u32* active;
+    const u32* vw;
+    __device__ u64 operator()(i64 j) const { return vw[active[reqs[j]]]; }
+};
+__global__ void k_req_heads(i64 count, const u64* keys, const u64* prefix, u64* base) {
+    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j < count && (j == 0 || keys[j - 1] != keys[j])) base[keys[j]] = prefix[j];
+}
+// reserve_receiver_prefixes' ticket rule (rebalance_graph.cuh:127-153) in
+// (part, repair order) order: a donor is admitted when its whole weighted
+// range [begin, begin+w) lies inside the part's immutable room.
+__global__ void k_admit(i64 count, const u32* reqs, const u64* keys, const u32* active, const u64* prefix,
+                        const u64* base, const u32* vw, const u64* slack, const u64* requests, u64* added,
+                        u64* tried, unsigned char* state, int* targets, int* flags) {
+    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const u32 i = reqs[j];
+    const int t = static_cast<int>(keys[j]);
+    const int v = static_cast<int>(active[i]);
+    const u64 w = vw[v];
+    tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
+    const u64 begin = requests[t] + prefix[j] - base[t];
+    atomicAdd(added + t, w);
+    if (begin <= slack[t] && w <= slack[t] - begin) {
+        targets[v] = t;
+        flags[v] = 1;
+        state[i] = 1;
+    }
+}
+__global__ void k_merge_requests(int k, u64* requests, u64* added) {
+    for (int p = threadIdx.x; p < k; p += blockDim.x) { requests[p] += added[p]; added[p] = 0; }
+}
+struct IsPlaced {
+    const unsigned char* state;
+    __device__ bool operator()(i64 i) const { return state[i] == 1; }
+};
+struct WriteActiveVertex {
+    const u32* active;
+    int* out;
+    __device__ void operator()(u32 slot, i64 i) const { out[slot] = static_cast<int>(active[i]); }
+};
+
+// ---------------------------------------------------------------- exchange
+
+constexpr int kJointSeeds = 128, kJointSide = 4, kJointArchive = 4;
+
+struct JointMove {  // exchange.cuh:9-13
+    int vertices[2 * kJointSide];
+    int size, a, b, id;
+    long long gain, net;
+};
+
+__host__ __device__ inline JointMove empty_move() {
+    JointMove m;
+    for (int j = 0; j < 8; ++j) m.vertices[j] = -1;
+    m.size = 0; m.a = -1; m.b = -1; m.id = 0; m.gain = 0; m.net = 0;
+    return m;
+}
+__device__ __forceinline__ long long joint_gap(long long net, long long lo, long long hi) {
+    return net < lo ? lo - net : net > hi ? net - hi : 0;
+}
+__device__ bool joint_same(const JointMove& x, const JointMove& y) {  // joint_same_move
+    if (!x.size || x.size != y.size || x.a != y.a || x.b != y.b || x.gain != y.gain || x.net != y.net) return false;
+    for (int j = 0; j < x.size; ++j) {
+        bool found = false;
+        for (int t = 0; t < y.size; ++t) found |= x.vertices[j] == y.vertices[t];
+        if (!found) return false;
+    }
+    return true;
+}
+struct NetOrder {  // JointNetOrder (complementary_moves.cuh:5-14)
+    __device__ bool operator()(const JointMove& x, const JointMove& y) const {
+        if (x.a != y.a) return x.a < y.a;
+        if (x.net != y.net) return x.net < y.net;
+        if (x.gain != y.gain) return x.gain > y.gain;
+        if (x.size != y.size) return x.size < y.size;
+        for (int j = 0; j < x.size; ++j) if (x.vertices[j] != y.vertices[j]) return x.vertices[j] < y.vertices[j];
+        return x.id < y.id;
+    }
+};
+struct MoveOrder {  // JointOrder (exchange.cuh:29-36)
+    __device__ bool operator()(const JointMove& x, const JointMove& y) const {
+        if ((x.size != 0) != (y.size != 0)) return x.size != 0;
+        if (x.a != y.a) return x.a < y.a;
+        if (x.gain != y.gain) return x.gain > y.gain;
+        return x.id < y.id;
+    }
+};
+
+// One bitonic stage over an index permutation padded to a power of two.
+template <class Cmp>
+__global__ void k_bitonic(int size, int count, const JointMove* moves, int* idx, int kk, int jj, Cmp cmp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= size) return;
+    const int x = i ^ jj;
+    if (x <= i) return;
+    const int a = idx[i], b = idx[x];
+    // Padding (index >= count) sorts after every real entry.
+    bool greater;
+    if (a >= count) greater = b < count;
+    else if (b >= count) greater = false;
+    else greater = cmp(moves[b], moves[a]);
+    const bool up = (i & kk) == 0;
+    if (greater == up) { idx[i] = b; idx[x] = a; }
+}
+__global__ void k_iota(int n, int* idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) idx[i] = i;
+}
+__global__ void k_gather_moves(int count, const int* idx, const JointMove* in, JointMove* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = in[idx[i]];
+}
+
+// joint_quotient (exchange.cuh:41-54).
+template <class C>
+__global__ void k_quotient(i64 n, const int* labels, const C* A, int k, u64* quotient) {
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int a = labels[v];
+        for (int b = a + 1; b < k; ++b) {
+            const C w = A[v * k + b];
+            if (w) atomicAdd(quotient + a * k + b, static_cast<u64>(w));
+        }
+    }
+}
+// joint_match (exchange.cuh:55-82): rounds of mutual best choices.
+__global__ void k_match_parts(int k, const u64* quotient, int* partner, int* visits) {
+    __shared__ int choice[128], progress;
+    const int p = threadIdx.x;
+    if (p < k) partner[p] = -1;
+    __syncthreads();
+    for (int round = 0; round < k / 2; ++round) {
+        if (!p) progress = 0;
+        int best = -1;
+        double score = -1;
+        if (p < k && partner[p] < 0)
+            for (int q = 0; q < k; ++q)
+                if (q != p && partner[q] < 0) {
+                    const int pair = min(p, q) * k + max(p, q);
+                    if (!quotient[pair]) continue;
+                    const double penalty = 1.0 + visits[pair];
+                    const double value = __ddiv_rn(static_cast<double>(quotient[pair]), __dmul_rn(penalty, penalty));
+                    if (value > score || (value == score && q < best)) { score = value; best = q; }
+                }
+        if (p < k) choice[p] = best;
+        __syncthreads();
+        if (p < k && best >= 0 && choice[best] == p) {
+            partner[p] = best;
+            if (p < best) { ++visits[p * k + best]; atomicAdd(&progress, 1); }
+        }
+        __syncthreads();
+        const int gained = progress;
+        __syncthreads();
+        if (!gained) break;
+    }
+}
+// joint_seeds (exchange.cuh:83-93).
+template <class C>
+__global__ void k_seeds(i64 n, const int* labels, const C* A, int k, const int* partner, u64* seeds, int sw, int pass) {
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int p = labels[v], q = partner[p];
+        if (q < 0 || !A[v * k + q]) continue;
+        const u32 h = mix32(static_cast<u32>(v) ^ mix32(static_cast<u32>(pass + 17)));
+        atomicMin(seeds + static_cast<i64>(p) * sw + (h % sw), (static_cast<u64>(h) << 32) | static_cast<u32>(v));
+    }
+}
+
+// joint_grow (exchange.cuh:95-204): one warp per (seed, policy) slot.
+template <class C>
+__global__ void k_grow(int slots, int sw, const u64* seeds, const int* partner, const int* off, const int* nbr,
+                       const u32* ew, const u32* masses, const int* labels, const C* A, int k, const u64* loads,
+                       u64 capacity, JointMove* moves, JointMove* archive) {
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (slot >= slots) return;
+    const int policy = slot % 2;
+    JointMove best = empty_move();
+    best.id = slot;
+    if (!lane) {
+        moves[slot] = best;
+        for (int j = 0; j < kJointArchive; ++j) archive[slot * kJointArchive + j] = empty_move();
+    }
+    const u64 enc = seeds[slot / 2];
+    if (enc == ~0ULL) return;
+    const int root = static_cast<int>(static_cast<u32>(enc)), source = labels[root], target = partner[source];
+    if (target < 0) return;
+    auto aff = [&](int u, int p) -> long long { return static_cast<long long>(A[static_cast<i64>(u) * k + p]); };
+    int members[8] = {root, -1, -1, -1, -1, -1, -1, -1};
+    int size = 1, counts[2] = {1, 0};
+    long long net = masses[root];
+    const long long lo = static_cast<long long>(loads[source]) - static_cast<long long>(capacity);
+    const long long hi = static_cast<long long>(capacity) - static_cast<long long>(loads[target]);
+    long long gain = aff(root, target) - aff(root, source);
+    for (int step = 0; step < 8; ++step) {
+        if (!lane && gain > 0 && size <= kJointArchive) {
+            JointMove st = empty_move();
+            st.size = size; st.a = min(source, target); st.b = max(source, target);
+            st.gain = gain; st.net = source == st.a ? net : -net; st.id = slot * kJointArchive + step;
+            for (int j = 0; j < size; ++j) {
+                int pos = j;
+                while (pos && st.vertices[pos - 1] > members[j]) { st.vertices[pos] = st.vertices[pos - 1]; --pos; }
+                st.vertices[pos] = members[j];
+            }
+            archive[slot * kJointArchive + step] = st;
+        }
+        if (gain > best.gain && !joint_gap(net, lo, hi)) {
+            best.size = size; best.a = min(source, target); best.b = max(source, target);
+            best.gain = gain; best.net = source == best.a ? net : -net;
+            for (int j = 0; j < size; ++j) best.vertices[j] = members[j];
+        }
+        if (size == 8) break;
+        const bool gap_first = policy == 0 && joint_gap(net, lo, hi);
+        long long cg = LLONG_MIN, cgap = LLONG_MAX;
+        int chosen = INT_MAX;
+        for (int origin = -1; origin < size; ++origin) {
+            const bool reverse = origin < 0;
+            if (reverse && counts[1]) continue;
+            const int m = reverse ? -1 : members[origin];
+            const int begin = reverse ? 0 : off[m];
+            const int end = reverse ? sw : min(off[m + 1], begin + 128);
+            for (int e = begin + lane; e < end; e += 32) {
+                int u;
+                if (reverse) {
+                    const u64 value = seeds[static_cast<i64>(target) * sw + e];
+                    if (value == ~0ULL) continue;
+                    u = static_cast<int>(static_cast<u32>(value));
+                } else u = nbr[e];
+                const int p = labels[u];
+                if (p != source && p != target) continue;
+                const int side = p == source ? 0 : 1;
+                if (counts[side] >= kJointSide) continue;
+                if (!reverse && p != labels[m]) continue;
+                bool dup = false;
+                for (int j = 0; j < size; ++j) dup |= u == members[j];
+                if (dup || off[u + 1] - off[u] > 1024) continue;
+                const long long cnet = net + (side ? -static_cast<long long>(masses[u]) : static_cast<long long>(masses[u]));
+                const long long gp = joint_gap(cnet, lo, hi);
+                if (net > hi && !side) continue;
+                if (net < lo && side) continue;
+                long long marginal = aff(u, side ? source : target) - aff(u, p);
+                if (!reverse) marginal += 2LL * edge_w(ew, e);
+                const bool better = gap_first
+                    ? (gp < cgap || (gp == cgap && (marginal > cg || (marginal == cg && u < chosen))))
+                    : (marginal > cg || (marginal == cg && (gp < cgap || (gp == cgap && u < chosen))));
+                if (better) { chosen = u; cg = marginal; cgap = gp; }
+            }
+        }
+        for (int d = 16; d; d >>= 1) {
+            const int u = __shfl_down_sync(0xffffffffu, chosen, d);
+            const long long g = __shfl_down_sync(0xffffffffu, cg, d);
+            const long long gp = __shfl_down_sync(0xffffffffu, cgap, d);
+            const bool better = gap_first ? (gp < cgap || (gp == cgap && (g > cg || (g == cg && u < chosen))))
+                                          : (g > cg || (g == cg && (gp < cgap || (gp == cgap && u < chosen))));
+            if (lane + d < 32 && better) { chosen = u; cg = g; cgap = gp; }
+        }
+        chosen = __shfl_sync(0xffffffffu, chosen, 0);
+        if (chosen == INT_MAX) break;
+        const int side = labels[chosen] == source ? 0 : 1;
+        long long correction = 0;
+        for (int e = off[chosen] + lane; e < off[chosen + 1]; e += 32)
+            for (int j = 0; j < size; ++j)
+                if (nbr[e] == members[j]) correction += (labels[members[j]] == labels[chosen] ? 2LL : -2LL) * edge_w(ew, e);
+        correction = warp_sum(correction);
+        const long long cgain = aff(chosen, side ? source : target) - aff(chosen, labels[chosen]) + correction;
+        members[size++] = chosen;
+        ++counts[side];
+        gain += cgain;
+        net += side ? -static_cast<long long>(masses[chosen]) : static_cast<long long>(masses[chosen]);
+    }
+    if (!lane) moves[slot] = best;
+}
+
+struct NonEmptyMove {
+    const JointMove* moves;
+    __device__ bool operator()(i64 i) const { return moves[i].size != 0; }
+};
+struct CopyMove {
+    const JointMove* in;
+    JointMove* out;
+    __device__ void operator()(u32 slot, i64 i) const { out[slot] = in[i]; }
+};
+struct UniqueHead {
+    const JointMove* moves;
+    __device__ bool operator()(i64 i) const { return i == 0 || !joint_same(moves[i - 1], moves[i]); }
+};
+
+// joint_combine (complementary_moves.cuh:31-75): one warp per fragment.
+__global__ void k_combine(int count, const JointMove* archive, const int* off, const int* nbr, const u32* ew,
+                          const int* labels, const u64* loads, u64 capacity, int id_base, JointMove* out) {
+    const int lane = threadIdx.x & 31, i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= count) return;
+    const JointMove x = archive[i];
+    const long long lo = static_cast<long long>(loads[x.a]) - static_cast<long long>(capacity);
+    const long long hi = static_cast<long long>(capacity) - static_cast<long long>(loads[x.b]);
+    if (!lane) {
+        JointMove y = x;
+        y.id = id_base + i;
+        if (joint_gap(x.net, lo, hi)) y.size = 0;
+        out[i] = y;
+        out[count + i] = empty_move();
+    }
+    auto bound = [&](long long net, bool upper) {
+        int l = 0, h = count;
+        while (l < h) {
+            const int mid = (l + h) / 2;
+            const JointMove& y = archive[mid];
+            if (y.a < x.a || (y.a == x.a && (y.net < net || (upper && y.net == net)))) l = mid + 1;
+            else h = mid;
+        }
+        return l;
+    };
+    const int begin = bound(lo - x.net, false), end = bound(hi - x.net, true);
+    long long best_gain = 0;
+    int best = -1, previous = -1;
+    for (int r = 0; r < 4 && begin < end; ++r) {
+        const int j = begin + static_cast<int>((static_cast<long long>(end - begin - 1) * r) / 3);
+        if (j == previous) continue;
+        previous = j;
+        if (j == i) continue;
+        const JointMove y = archive[j];
+        if (y.a != x.a || y.b != x.b || x.size + y.size > 8) continue;
+        bool overlap = false;
+        for (int u = 0; u < x.size; ++u) for (int w = 0; w < y.size; ++w) overlap |= x.vertices[u] == y.vertices[w];
+        if (overlap) continue;
+        long long correction = 0;
+        for (int u = 0; u < x.size; ++u) {
+            const int v = x.vertices[u];
+            for (int e = off[v] + lane; e < off[v + 1]; e += 32)
+                for (int t = 0; t < y.size; ++t)
+                    if (nbr[e] == y.vertices[t]) correction += (labels[v] == labels[nbr[e]] ? 2LL : -2LL) * edge_w(ew, e);
+        }
+        correction = warp_sum(correction);
+        const long long gain = x.gain + y.gain + correction;
+        if (gain > best_gain || (gain == best_gain && gain > 0 && j < best)) { best_gain = gain; best = j; }
+    }
+    if (!lane && best >= 0) {
+        JointMove r = x;
+        const JointMove y = archive[best];
+        for (int j = 0; j < y.size; ++j) r.vertices[r.size++] = y.vertices[j];
+        r.gain = best_gain;
+        r.net += y.net;
+        r.id = id_base + count + i;
+        out[count + i] = r;
+    }
+}
+__global__ void k_claim(int count, const JointMove* moves, int* owners) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count && moves[i].size)
+        for (int j = 0; j < moves[i].size; ++j) atomicMin(owners + moves[i].vertices[j], i);
+}
+__global__ void k_resolve(int count, JointMove* moves, const int* owners) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    for (int j = 0; j < moves[i].size; ++j)
+        if (owners[moves[i].vertices[j]] != i) { moves[i].size = 0; break; }
+}
+__global__ void k_mark(int count, const JointMove* moves, const int* labels, int* owners, int* targets) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count)
+        for (int j = 0; j < moves[i].size; ++j) {
+            const int v = moves[i].vertices[j];
+            owners[v] = i;
+            targets[v] = labels[v] == moves[i].a ? moves[i].b : moves[i].a;
+        }
+}
+// joint_events (exchange.cuh:227-262).
+__global__ void k_events(int count, const JointMove* moves, const int* owners, const int* targets, const int* labels,
+                         const int* off, const int* nbr, const u32* ew, u64* events) {
+    const int lane = threadIdx.x & 31, i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= count || !moves[i].size) return;
+    u64 own = 0;
+    for (int j = 0; j < moves[i].size; ++j) {
+        const int v = moves[i].vertices[j];
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+            const int u = nbr[e], other = owners[u];
+            if (u == v || (other != INT_MAX && v > u)) continue;
+            if (other != INT_MAX && labels[u] != moves[i].a && labels[u] != moves[i].b) continue;
+            const long long w = edge_w(ew, e);
+            const int before = labels[v] != labels[u];
+            if (other == i || other == INT_MAX) {
+                const int after = targets[v] != (other == i ? targets[u] : labels[u]);
+                own += static_cast<u64>((before - after) * w);
+            } else {
+                const int middle = i < other ? targets[v] != labels[u] : labels[v] != targets[u];
+                const int after = targets[v] != targets[u];
+                const u64 first = static_cast<u64>((before - middle) * w), last = static_cast<u64>((middle - after) * w);
+                own += i < other ? first : last;
+                atomicAdd(events + other, i < other ? last : first);
+            }
+        }
+    }
+    own = warp_sum(own);
+    if (!lane && own) atomicAdd(events + i, own);
+}
+// joint_prefix (exchange.cuh:263-284).
+__global__ void k_prefix(int count, int k, const JointMove* moves, const u64* events, const u64* loads, u64 capacity,
+                         int* stops) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= k) return;
+    long long gain = 0, net = 0, best = 0;
+    int stop = -1;
+    int low = 0, high = count;
+    while (low < high) { const int mid = (low + high) / 2; if (moves[mid].a < a) low = mid + 1; else high = mid; }
+    for (int i = low; i < count && moves[i].a == a; ++i)
+        if (moves[i].size) {
+            gain += static_cast<long long>(events[i]);
+            net += moves[i].net;
+            const int b = moves[i].b;
+            const long long lo = static_cast<long long>(loads[a]) - static_cast<long long>(capacity);
+            const long long hi = static_cast<long long>(capacity) - static_cast<long long>(loads[b]);
+            if (!joint_gap(net, lo, hi) && gain > best) { best = gain; stop = i; }
+        }
+    stops[a] = stop;
+}
+__global__ void k_accept(int count, const JointMove* moves, const int* stops, int* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count && moves[i].size && i <= stops[moves[i].a])
+        for (int j = 0; j < moves[i].size; ++j) flags[moves[i].vertices[j]] = 1;
+}
+struct Flagged {
+    const int* flags;
+    __device__ bool operator()(i64 v) const { return flags[v] != 0; }
+};
+
+// ---------------------------------------------------------------- host side
+
+struct LevelResult {
+    u64 cut = 0;
+    bool refined = false, repair_failed = false;
+};
+
+template <class T>
+class LevelRefiner {
+public:
+    LevelRefiner(Context& c, const DGraph& g, int k, double eps, int* labels, u64* loads, u64 total, bool log)
+        : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log) {}
+
+    LevelResult run(bool has_known, u64 known);
+
+private:
+    Context& ctx;
+    const DGraph& g;
+    int k;
+    double eps;
+    int* labels;
+    u64* loads;
+    u64 total;
+    bool log;
+
+    u64 C = 0;
+    i64 n = 0;
+    T* A = nullptr;
+    T* totals = nullptr;
+    int* targets = nullptr;
+    long long* gains = nullptr;
+    unsigned char* locks = nullptr;
+    int* flags = nullptr;
+    int* cand = nullptr;
+    int* movers = nullptr;
+    double* prices = nullptr;
+    Sample* samples = nullptr;
+    u32* rorder = nullptr;
+    u64* counters = nullptr;  // device: 0 cand, 1 movers, 2 delta, 3 max load, 4.. scratch
+    u64 cut = 0, revision = 0;
+    u64 max_load_host = 0;
+
+    cudaStream_t s() const { return ctx.stream; }
+    int grid_for(i64 items, int per_block) const { return static_cast<int>(std::min<i64>(blocks_for(items, per_block), 148 * 32)); }
+
+    void build() {
+        const size_t smem = 8 * k * sizeof(T);
+        launch(k_build<T>, grid_for(n * 32, kThreads), kThreads, smem, s(), n, g.off, g.nbr, g.ew, labels, k, A, totals);
+    }
+    // Applies the movers listed in `list` (count on device at `live`):
+    // cache/cut update, commit, flag reset.  Returns the cut decrease.
+    void apply(const int* list, const u64* live, i64 host_count, bool lp, bool sample) {
+        GP_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(u64), s()));
+        launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
+               g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
+               sample ? samples : static_cast<Sample*>(nullptr));
+        launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
+               labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
+        launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
+        launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
+    }
+    void account(long long delta) {
+        if (delta >= 0) {
+            if (static_cast<u64>(delta) > cut) fail(GP_INTERNAL, "incremental cut underflow");
+            cut -= static_cast<u64>(delta);
+        } else cut += static_cast<u64>(-delta);
+    }
+    i64 lp_round(double filter);
+    bool repair();
+    void exchange(u64& best);
+};
+
+template <class T>
+i64 LevelRefiner<T>::lp_round(double filter) {
+    GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
+    LpParams q{n, k, C, filter, g.off, g.nbr, g.ew, g.vw, labels, loads, prices, targets, gains, locks, flags, cand, movers, counters};
+    const int W = k <= 8 ? 8 : k <= 16 ? 16 : 32;
+    const int grid = grid_for(n * W, kThreads);
+    if (W == 8) launch(k_proposals<T, 8>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
+    else if (W == 16) launch(k_proposals<T, 16>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
+    else launch(k_proposals<T, 32>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
+    launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
+    launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q);
+    apply(movers, counters + 1, n, true, false);
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters, 4 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+    GP_CUDA(cudaStreamSynchronize(s()));
+    const i64 count = static_cast<i64>(ctx.host_scalars[1]);
+    const long long delta = static_cast<long long>(ctx.host_scalars[2]);
+    max_load_host = ctx.host_scalars[3];
+    if (count) {
+        account(delta);
+        ++revision;
+    }
+    return count;
+}
+
+// One capacity repair (RebalanceGraph, rebalance_graph.cuh:160-280) in the
+// deterministic order.  Returns feasibility.
+template <class T>
+bool LevelRefiner<T>::repair() {
+    if (max_load_host <= C) return true;
+    Arena& A_ = ctx.scratch;
+    ArenaScope scope(A_);
+    u64* slack = A_.alloc<u64>(k);
+    u64* requests = A_.alloc<u64>(k);
+    u64* added = A_.alloc<u64>(k);
+    u64* cdf = A_.alloc<u64>(k + 1);
+    u64* part_base = A_.alloc<u64>(k);
+    u64* base_t = A_.alloc<u64>(k);
+    GP_CUDA(cudaMemsetAsync(added, 0, sizeof(u64) * k, s()));
+    u32* donors = A_.alloc<u32>(n);
+    u32* donor_count = reinterpret_cast<u32*>(counters + 4);
+    unsigned char* active_flag = A_.alloc<unsigned char>(n);
+    int iterations = 0;
+    while (true) {
+        ArenaScope it(A_);
+        launch(k_slack, 1, 32, 0, s(), k, loads, C, slack, requests, cdf);
+        select_if(A_, s(), n, IsDonor{rorder, labels, loads, C}, WriteOrdered{rorder, donors}, donor_count);
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        const i64 dcount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+        i64 placed = 0;
+        long long delta = 0;
+        if (dcount > 0) {
+            u64* keys = A_.alloc<u64>(dcount);
+            u64* keys_alt = A_.alloc<u64>(dcount);
+            u32* items = A_.alloc<u32>(dcount);
+            u32* items_alt = A_.alloc<u32>(dcount);
+            launch(k_repair_dest<T>, grid_for(dcount * 32, kThreads), kThreads, 0, s(), dcount, donors,
+                   static_cast<const T*>(A), static_cast<const T*>(totals), labels, g.vw, k, loads, C, cdf, targets, keys);
+            GP_CUDA(cudaMemcpyAsync(items, donors, sizeof(u32) * dcount, cudaMemcpyDeviceToDevice, s()));
+            // Stable sort by bucket keeps the repair order inside a bucket;
+            // bucket keys are below k*800 < 2^17, the sentinel sorts last.
+            launch(k_clamp_keys, blocks_for(dcount, kThreads), kThreads, 0, s(), dcount, keys);
+            radix_sort_pairs(A_, s(), dcount, keys, items, keys_alt, items_alt, 0, 24);
+            u64* prefix = A_.alloc<u64>(dcount);
+            exclusive_scan<u64>(A_, s(), dcount, SortedWeight{items, g.vw}, prefix, static_cast<u64*>(nullptr));
+            launch(k_part_heads, blocks_for(dcount, kThreads), kThreads, 0, s(), dcount, keys, prefix, part_base);
+            launch(k_donor_test, blocks_for(dcount, kThreads), kThreads, 0, s(), dcount, keys, items, prefix, part_base,
+                   loads, C, active_flag);
+            // Active donors, back in repair order.
+            u32* active = A_.alloc<u32>(dcount);
+            select_if(A_, s(), dcount, IsActive{donors, active_flag}, WriteFrom{donors, active}, donor_count);
+            GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+            GP_CUDA(cudaStreamSynchronize(s()));
+            const i64 acount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+            if (acount > 0) {
+                u64* tried = A_.alloc<u64>(2 * acount);
+                unsigned char* state = A_.alloc<unsigned char>(acount);
+                int* want = A_.alloc<int>(acount);
+                GP_CUDA(cudaMemsetAsync(tried, 0, sizeof(u64) * 2 * acount, s()));
+                GP_CUDA(cudaMemsetAsync(state, 0, acount, s()));
+                u32* reqs = A_.alloc<u32>(acount);
+                u32* reqs_alt = A_.alloc<u32>(acount);
+                u64* rkeys = A_.alloc<u64>(acount);
+                u64* rkeys_alt = A_.alloc<u64>(acount);
+                u64* rprefix = A_.alloc<u64>(acount);
+                for (int attempt = 0; attempt < k; ++attempt) {
+                    GP_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(u64), s()));
+                    launch(k_choose<T>, grid_for(acount * 32, kThreads), kThreads, 0, s(), acount, active, attempt,
+                           static_cast<const T*>(A), labels, g.vw, k, targets, slack, requests, tried, state, want,
+                           counters + 5);
+                    select_if(A_, s(), acount, WantsPart{want}, WriteIdx{reqs}, donor_count);
+                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                    GP_CUDA(cudaStreamSynchronize(s()));
+                    const i64 rcount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+                    if (!rcount) break;
+                    u32* r = reqs;
+                    u32* ra = reqs_alt;
+                    u64* kk = rkeys;
+                    u64* ka = rkeys_alt;
+                    launch(k_want_keys, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, want, kk);
+                    radix_sort_pairs(A_, s(), rcount, kk, r, ka, ra, 0, 8);
+                    exclusive_scan<u64>(A_, s(), rcount, ReqWeight{r, active, g.vw}, rprefix, static_cast<u64*>(nullptr));
+                    launch(k_req_heads, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, kk, rprefix, base_t);
+                    launch(k_admit, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, kk, active, rprefix, base_t,
+                           g.vw, slack, requests, added, tried, state, targets, flags);
+                    launch(k_merge_requests, 1, 128, 0, s(), k, requests, added);
+                }
+                // Movers = placed donors, in repair order.
+                select_if(A_, s(), acount, IsPlaced{state}, WriteActiveVertex{active, movers}, donor_count);
+                GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                GP_CUDA(cudaStreamSynchronize(s()));
+                placed = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+                if (placed) {
+                    apply(movers, nullptr, placed, false, samples != nullptr);
+                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                    GP_CUDA(cudaStreamSynchronize(s()));
+                    delta = static_cast<long long>(ctx.host_scalars[0]);
+                    max_load_host = ctx.host_scalars[1];
+                    account(delta);
+                    ++revision;
+                }
+            }
+        }
+        ++iterations;
+        const bool feasible = max_load_host <= C;
+        if (feasible || placed == 0 || iterations >= 2 * k + 4) return feasible;
+    }
+}
+
+template <class T>
+void LevelRefiner<T>::exchange(u64& best_cut) {
+    Arena& A_ = ctx.scratch;
+    ArenaScope scope(A_);
+    const int sw = std::min(kJointSeeds, std::max(32, 4096 / k));
+    const int slots = k * sw * 2;
+    u64* quotient = A_.alloc<u64>(static_cast<size_t>(k) * k);
+    int* visits = A_.alloc<int>(static_cast<size_t>(k) * k);
+    int* partner = A_.alloc<int>(k);
+    u64* seeds = A_.alloc<u64>(static_cast<size_t>(k) * sw);
+    JointMove* moves = A_.alloc<JointMove>(slots);
+    JointMove* archive = A_.alloc<JointMove>(static_cast<size_t>(slots) * kJointArchive);
+    JointMove* frag = A_.alloc<JointMove>(static_cast<size_t>(slots) * kJointArchive);
+    JointMove* frag_sorted = A_.alloc<JointMove>(static_cast<size_t>(slots) * kJointArchive);
+    const size_t pool_cap = static_cast<size_t>(slots) + 2 * static_cast<size_t>(slots) * kJointArchive;
+    JointMove* pool = A_.alloc<JointMove>(pool_cap);
+    JointMove* act = A_.alloc<JointMove>(pool_cap);
+    JointMove* act_sorted = A_.alloc<JointMove>(pool_cap);
+    int* idx = A_.alloc<int>(2 * pool_cap);
+    int* owners = A_.alloc<int>(n);
+    u64* events = A_.alloc<u64>(pool_cap);
+    int* stops = A_.alloc<int>(k);
+    u32* cnt = reinterpret_cast<u32*>(counters + 4);
+    GP_CUDA(cudaMemsetAsync(quotient, 0, sizeof(u64) * k * k, s()));
+    GP_CUDA(cudaMemsetAsync(visits, 0, sizeof(int) * k * k, s()));
+    launch(k_quotient<T>, grid_for(n, kThreads), kThreads, 0, s(), n, labels, static_cast<const T*>(A), k, quotient);
+    auto read_count = [&]() -> i64 {
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        return static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+    };
+    auto sort_moves = [&](JointMove* in, JointMove* out, int count, auto cmp) {
+        int size = 1;
+        while (size < count) size <<= 1;
+        launch(k_iota, blocks_for(size, kThreads), kThreads, 0, s(), size, idx);
+        for (int kk = 2; kk <= size; kk <<= 1)
+            for (int jj = kk >> 1; jj; jj >>= 1)
+                launch(k_bitonic<decltype(cmp)>, blocks_for(size, kThreads), kThreads, 0, s(), size, count,
+                       static_cast<const JointMove*>(in), idx, kk, jj, cmp);
+        launch(k_gather_moves, blocks_for(count, kThreads), kThreads, 0, s(), count, static_cast<const int*>(idx),
+               static_cast<const JointMove*>(in), out);
+    };
+    int empty = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        launch(k_match_parts, 1, 128, 0, s(), k, quotient, partner, visits);
+        GP_CUDA(cudaMemsetAsync(seeds, 0xff, sizeof(u64) * k * sw, s()));
+        launch(k_seeds<T>, grid_for(n, kThreads), kThreads, 0, s(), n, labels, static_cast<const T*>(A), k, partner,
+               seeds, sw, pass);
+        launch(k_grow<T>, blocks_for(slots, 8), kThreads, 0, s(), slots, sw, seeds, partner, g.off, g.nbr, g.ew, g.vw,
+               labels, static_cast<const T*>(A), k, loads, C, moves, archive);
+        select_if(A_, s(), static_cast<i64>(slots) * kJointArchive, NonEmptyMove{archive}, CopyMove{archive, frag}, cnt);
+        int fragments = static_cast<int>(read_count());
+        if (fragments) {
+            sort_moves(frag, frag_sorted, fragments, NetOrder{});
+            select_if(A_, s(), fragments, UniqueHead{frag_sorted}, CopyMove{frag_sorted, frag}, cnt);
+            fragments = static_cast<int>(read_count());
+        }
+        const int pool_size = slots + 2 * fragments;
+        GP_CUDA(cudaMemcpyAsync(pool, moves, sizeof(JointMove) * slots, cudaMemcpyDeviceToDevice, s()));
+        if (fragments)
+            launch(k_combine, blocks_for(fragments, 8), kThreads, 0, s(), fragments, static_cast<const JointMove*>(frag),
+                   g.off, g.nbr, g.ew, labels, loads, C, slots, pool + slots);
+        select_if(A_, s(), pool_size, NonEmptyMove{pool}, CopyMove{pool, act}, cnt);
+        const int active = static_cast<int>(read_count());
+        if (!active) { if (++empty >= 2) break; continue; }
+        sort_moves(act, act_sorted, active, MoveOrder{});
+        fill<int>(s(), owners, n, INT_MAX);
+        launch(k_claim, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted), owners);
+        launch(k_resolve, blocks_for(active, kThreads), kThreads, 0, s(), active, act_sorted, static_cast<const int*>(owners));
+        fill<int>(s(), owners, n, INT_MAX);
+        launch(k_mark, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
+               static_cast<const int*>(labels), owners, targets);
+        GP_CUDA(cudaMemsetAsync(events, 0, sizeof(u64) * active, s()));
+        launch(k_events, blocks_for(active, 8), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
+               static_cast<const int*>(owners), static_cast<const int*>(targets), static_cast<const int*>(labels), g.off,
+               g.nbr, g.ew, events);
+        launch(k_prefix, blocks_for(k, 128), 128, 0, s(), active, k, static_cast<const JointMove*>(act_sorted),
+               static_cast<const u64*>(events), static_cast<const u64*>(loads), C, stops);
+        launch(k_accept, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
+               static_cast<const int*>(stops), flags);
+        select_if(A_, s(), n, Flagged{flags}, WriteIndex{movers}, cnt);
+        const i64 count = read_count();
+        if (!count) { if (++empty >= 2) break; continue; }
+        empty = 0;
+        apply(movers, nullptr, count, false, false);
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        const long long delta = static_cast<long long>(ctx.host_scalars[0]);
+        max_load_host = ctx.host_scalars[1];
+        account(delta);
+        ++revision;
+        if (delta <= 0) fail(GP_INTERNAL, "non-improving boundary group batch");
+        if (max_load_host > C || cut >= best_cut) fail(GP_INTERNAL, "capacity exchange violated cut/capacity");
+        best_cut = cut;
+    }
+}
+
+// run_incremental_refinement_typed (incremental.cuh:660-1051).
+template <class T>
+LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
+    Arena& A_ = ctx.scratch;
+    ArenaScope scope(A_);
+    n = g.n;
+    uint64_t cap = 0;
+    if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
+    C = cap;
+    const bool priced = total > static_cast<u64>(n);
+    A = A_.alloc<T>(static_cast<size_t>(n) * k);
+    totals = A_.alloc<T>(n);
+    targets = A_.alloc<int>(n);
+    gains = A_.alloc<long long>(n);
+    locks = A_.alloc<unsigned char>(n);
+    flags = A_.alloc<int>(n);
+    cand = A_.alloc<int>(n);
+    movers = A_.alloc<int>(n);
+    counters = A_.alloc<u64>(8);
+    int* saved_labels = A_.alloc<int>(n);
+    u64* saved_loads = A_.alloc<u64>(k);
+    GP_CUDA(cudaMemsetAsync(locks, 0, n, s()));
+    GP_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * n, s()));
+    fill<int>(s(), targets, n, -1);
+    if (priced) {
+        prices = A_.alloc<double>(k);
+        samples = A_.alloc<Sample>(k);
+        GP_CUDA(cudaMemsetAsync(prices, 0, sizeof(double) * k, s()));
+        GP_CUDA(cudaMemsetAsync(samples, 0, sizeof(Sample) * k, s()));
+    }
+    {  // repair order: ascending (repair hash, id)
+        rorder = A_.alloc<u32>(n);
+        u32* rorder_alt = A_.alloc<u32>(n);
+        u64* keys = A_.alloc<u64>(n);
+        u64* keys_alt = A_.alloc<u64>(n);
+        launch(k_repair_keys, blocks_for(n, kThreads), kThreads, 0, s(), n, keys, rorder);
+        radix_sort_pairs(A_, s(), n, keys, rorder, keys_alt, rorder_alt, 0, 32);
+    }
+    build();
+    cut = has_known ? known : device_cut(ctx, g, labels);
+    launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+    GP_CUDA(cudaStreamSynchronize(s()));
+    max_load_host = ctx.host_scalars[0];
+    LevelResult res;
+    if (max_load_host > C) {
+        if (!repair()) {
+            res.cut = cut;
+            res.repair_failed = true;
+            return res;
+        }
+    }
+    const u64 feasible_start = cut;
+    u64 best = cut;
+    GP_CUDA(cudaMemcpyAsync(saved_labels, labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
+    GP_CUDA(cudaMemcpyAsync(saved_loads, loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
+    u64 best_revision = revision;
+    double filter = 0.25;
+    if (g.ew) {
+        ctx.clear_scalars(1);
+        launch(k_max_edge, std::min(blocks_for(g.m, kThreads), 148 * 8), kThreads, 0, s(), g.m, g.ew, ctx.dev_scalars);
+        filter = ctx.read_scalars(1)[0] <= 1 ? 0.25 : 0.75;
+    }
+    int stale = 0, empty = 0, rounds = 0;
+    for (int phase = 0; phase < 32 && stale < 3; ++phase) {
+        ++rounds;
+        if (samples) GP_CUDA(cudaMemsetAsync(samples, 0, sizeof(Sample) * k, s()));
+        const i64 count = lp_round(filter);
+        if (!count) { if (++empty >= 2) break; ++stale; continue; }
+        empty = 0;
+        if (!repair()) break;
+        if (prices) launch(k_prices, 1, 128, 0, s(), k, static_cast<const Sample*>(samples), prices);
+        ++stale;
+        if (cut < best) {
+            if (best - cut > best / 1000) stale = 0;
+            best = cut;
+            GP_CUDA(cudaMemcpyAsync(saved_labels, labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
+            GP_CUDA(cudaMemcpyAsync(saved_loads, loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
+            best_revision = revision;
+        }
+    }
+    const bool restored = revision != best_revision;
+    if (restored) {
+        GP_CUDA(cudaMemcpyAsync(labels, saved_labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
+        GP_CUDA(cudaMemcpyAsync(loads, saved_loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
+        launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        max_load_host = ctx.host_scalars[0];
+    }
+    cut = best;
+    if (n <= 65536) {
+        if (restored) build();
+        exchange(best);
+    }
+    if (cut != best || cut > feasible_start || max_load_host > C) fail(GP_INTERNAL, "incremental refinement postcondition failed");
+    if (log)
+        std::printf("refine_level vertices=%lld initial_cut=%llu final_cut=%llu rounds=%d\n", static_cast<long long>(n),
+                    static_cast<unsigned long long>(feasible_start), static_cast<unsigned long long>(cut), rounds);
+    res.cut = cut;
+    res.refined = true;
+    return res;
+}
+
 }  // namespace
 
 u64 device_cut(Context& ctx, const DGraph& g, const int* labels) {
     ctx.clear_scalars(1);
-    launch(k_cut, std::min(blocks_for(g.n, 256), 148 * 16), 256, 0, ctx.stream, g.n, g.off, g.nbr, g.ew, labels, ctx.dev_scalars);
+    launch(k_cut, std::min(blocks_for(g.n * 32, 256), 148 * 32), 256, 0, ctx.stream, g.n, g.off, g.nbr, g.ew, labels,
+           ctx.dev_scalars);
     const u64 d = ctx.read_scalars(1)[0];
     if (d & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
     return d / 2;
 }
 
+// refine_hierarchy_impl (src/refine.cu:483-730).
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
                         int* labels, bool log) {
+    cudaStream_t s = ctx.stream;
     const size_t L = h.levels.size();
-    int* cur = ctx.scratch.alloc<int>(h.levels.back().n);
-    GP_CUDA(cudaMemcpyAsync(cur, coarse_labels.data(), sizeof(int) * coarse_labels.size(), cudaMemcpyHostToDevice, ctx.stream));
+    std::vector<int*> level_labels(L);
+    level_labels[0] = labels;
+    for (size_t i = 1; i < L; ++i) level_labels[i] = ctx.persist.alloc<int>(h.levels[i].n);
+    u64* loads = ctx.persist.alloc<u64>(k);
+    const DGraph& coarsest = h.levels.back();
+    GP_CUDA(cudaMemcpyAsync(level_labels[L - 1], coarse_labels.data(), sizeof(int) * coarsest.n, cudaMemcpyHostToDevice, s));
+    GP_CUDA(cudaMemsetAsync(loads, 0, sizeof(u64) * k, s));
+    launch(k_loads, std::min(blocks_for(coarsest.n, 256), 148 * 4), 256, sizeof(u64) * k, s, coarsest.n, k,
+           level_labels[L - 1], coarsest.vw, loads);
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    u64 total = 0, maxload = 0;
+    for (int p = 0; p < k; ++p) { total += ctx.host_scalars[p]; maxload = std::max<u64>(maxload, ctx.host_scalars[p]); }
+    auto refine = [&](const DGraph& g, int* lab, bool has_known, u64 known) {
+        if (g.incident_bound <= 0xffffffffULL)
+            return LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log).run(has_known, known);
+        return LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log).run(has_known, known);
+    };
+    LevelResult res = refine(coarsest, level_labels[L - 1], false, 0);
+    u64 last_cut = res.cut;
+    i64 last_refined = coarsest.n;
+    RefineOutcome out;
+    out.levels_refined = res.refined;
+    uint64_t cap = 0;
+    if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
     for (size_t c = L - 1; c > 0; --c) {
-        const DGraph& f = h.levels[c - 1];
-        int* next = c - 1 == 0 ? labels : ctx.scratch.alloc<int>(f.n);
-        launch(k_project, blocks_for(f.n, 256), 256, 0, ctx.stream, f.n, h.maps[c - 1], cur, next);
-        cur = next;
+        const size_t f = c - 1;
+        const DGraph& fg = h.levels[f];
+        launch(k_project, blocks_for(fg.n, 256), 256, 0, s, fg.n, h.maps[f], level_labels[c], level_labels[f]);
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+        GP_CUDA(cudaStreamSynchronize(s));
+        maxload = 0;
+        for (int p = 0; p < k; ++p) maxload = std::max<u64>(maxload, ctx.host_scalars[p]);
+        const bool refine_here = f == 0 || maxload > cap || static_cast<double>(fg.n) >= 2.0 * static_cast<double>(last_refined);
+        LevelResult lr;
+        if (refine_here) {
+            lr = refine(fg, level_labels[f], true, last_cut);
+            if (!lr.repair_failed) last_refined = fg.n;
+            out.levels_refined += lr.refined;
+        } else {
+            lr.cut = last_cut;
+        }
+        last_cut = lr.cut;
     }
-    if (L == 1) GP_CUDA(cudaMemcpyAsync(labels, cur, sizeof(int) * h.levels[0].n, cudaMemcpyDeviceToDevice, ctx.stream));
-    RefineOutcome r;
-    r.cut = device_cut(ctx, h.levels[0], labels);
-    return r;
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    maxload = 0;
+    for (int p = 0; p < k; ++p) maxload = std::max<u64>(maxload, ctx.host_scalars[p]);
+    if (maxload > cap) fail(GP_INTERNAL, "final original partition violates capacity");
+    out.cut = last_cut;
+    out.max_load = maxload;
+    return out;
 }
+
 }  // namespace gp
