@@ -286,6 +286,29 @@ class Context:
                                              _C.c_void_p(stream_ptr) if stream_ptr else None, _C.byref(stats)))
         return Stats._from(stats)
 
+    def partition_host_ptrs(self, offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
+                            edge_weights_ptr, k: int, epsilon: float, seed: int, labels_ptr: int,
+                            flags: int = FLAG_QUIET) -> Stats:
+        """gp_partition on raw host pointers (e.g. pinned buffers)."""
+        stats = _Stats()
+        g = _Csr(n, m, offsets_ptr, neighbors_ptr, vertex_weights_ptr, edge_weights_ptr)
+        _check(self._lib.gp_partition(self._handle, _C.byref(g), _C.c_int32(k), _C.c_double(epsilon),
+                                      _C.c_uint32(seed), _C.c_uint32(flags), _C.c_void_p(labels_ptr), _C.byref(stats)))
+        return Stats._from(stats)
+
+    def profile_begin(self, kernel_substring: str) -> None:
+        """Time every launch of kernels whose name contains the substring."""
+        _check(self._lib.gp_profile_begin(self._handle, kernel_substring.encode()))
+
+    def profile_end(self) -> tuple[int, float]:
+        """(launches, total device milliseconds) since profile_begin."""
+        launches, ms = _C.c_uint64(), _C.c_double()
+        _check(self._lib.gp_profile_end(self._handle, _C.byref(launches), _C.byref(ms)))
+        return launches.value, ms.value
+
+    def set_option(self, name: str, value: int) -> None:
+        _check(self._lib.gp_set_option(self._handle, name.encode(), _C.c_int64(value)))
+
     def levels(self) -> list[dict]:
         """Host copies of the hierarchy kept by FLAG_KEEP_HIERARCHY."""
         lib = self._lib

@@ -23,9 +23,11 @@ namespace {
 
 constexpr int kLowDegree = 8;       // SCLP_LOW_DEGREE
 constexpr int kMediumDegree = 256;  // SCLP_MEDIUM_DEGREE
-constexpr int kLargeDegree = 4096;  // rows above use a global-memory table
-constexpr int kMediumHash = 512;    // SCLP_MEDIUM_HASH_SIZE
-constexpr int kLargeHash = 8192;
+constexpr int kLargeDegree = kHeavyRow;   // rows above use a chunked global table
+constexpr int kMediumHash = 512;          // SCLP_MEDIUM_HASH_SIZE
+constexpr int kLargeHash = 2 * kHeavyRow; // shared-memory table of the large class
+constexpr int kSegment = 4096;            // table slots summarised per block
+constexpr int kBlockSortRow = 4096;       // contraction: block bitonic sort limit
 constexpr int kMediumWarps = 4;
 
 // ---------------------------------------------------------------- metadata
@@ -47,7 +49,8 @@ __global__ void k_level0_meta(i64 n, const int* off, const int* nbr, const u32* 
     u64 d = 0;
     u32 flags = 0;
     const i64 begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
-    for (i64 e = begin + lane; e < end; e += W) {
+    const bool heavy = end - begin > kHeavyRow;  // summed by k_level0_meta_chunks
+    for (i64 e = begin + lane; !heavy && e < end; e += W) {
         const u64 w = edge_w(ew, e);
         d = ~0ULL - d < w ? ~0ULL : d + w;
         if (e > begin && nbr[e] <= nbr[e - 1]) flags |= 1u;
@@ -78,6 +81,33 @@ __global__ void k_level0_meta(i64 n, const int* off, const int* nbr, const u32* 
         atomicAdd(sc + 5, s_total);
         atomicMax(sc + 6, s_vmax);
     }
+}
+
+// Heavy rows of record_bound_kernel, one block per chunk.
+__global__ void k_level0_meta_chunks(DGraph g, u64* bounds, u64* sc) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    const int begin = g.off[v];
+    u64 d = 0;
+    u32 flags = 0;
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
+        const u64 w = edge_w(g.ew, e);
+        d += w;
+        if (e > begin && g.nbr[e] <= g.nbr[e - 1]) flags |= 1u;
+        if (!w) flags |= 2u;
+        if (w != 1) flags |= 4u;
+    }
+    d = warp_sum(d);
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if ((threadIdx.x & 31) == 0) {
+        if (d) atomicAdd(bounds + v, d);
+        if (flags & 1u) atomicOr(sc + 1, 1ULL);
+        if (flags & 2u) atomicOr(sc + 2, 1ULL);
+        if (flags & 4u) atomicOr(sc + 3, 1ULL);
+    }
+}
+__global__ void k_heavy_bound_max(i64 count, const int* heavy, const u64* bounds, u64* sc) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h < count) atomicMax(sc + 0, bounds[heavy[h]]);
 }
 
 // Directed edge-weight sum (packed-weight decision, src/coarsen.cu:1839-1848).
@@ -405,6 +435,83 @@ __global__ void __launch_bounds__(256) k_affinity_large(i64 count, const int* ro
     }
 }
 
+// Rows above kHeavyRow: every chunk inserts its entries into the row's
+// global open-addressing table; segments of the table are then summarised
+// block-wise and the partial summaries merged per row.
+__global__ void k_affinity_heavy_insert(DGraph g, const u64* table_off, int* keys, u64* vals, RoundParams p) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    int src;
+    if (!is_mover(p, v, src)) return;
+    const int h = g.chunk_hidx[c];
+    const u64 size = heavy_slots(g.off[v + 1] - g.off[v]);
+    int* K = keys + table_off[h];
+    u64* V = vals + table_off[h];
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
+        const int u = p.nbr[e];
+        if (u == v) continue;
+        const int cl = p.clusters[u];
+        u64 sl = mix32(static_cast<u32>(cl)) & (size - 1);
+        while (true) {
+            const int found = atomicCAS(K + sl, -1, cl);
+            if (found == -1 || found == cl) { atomicAdd(V + sl, static_cast<u64>(edge_w(p.ew, e))); break; }
+            sl = (sl + 1) & (size - 1);
+        }
+    }
+}
+__global__ void k_affinity_heavy_summary(const int* heavy, const int* seg_hidx, const int* seg_index,
+                                         const u64* table_off, const int* keys, const u64* vals, RoundParams p,
+                                         Summary* partial) {
+    __shared__ Summary warp_part[8];
+    const int sg = blockIdx.x, h = seg_hidx[sg], v = heavy[h];
+    int src;
+    if (!is_mover(p, v, src)) return;
+    const u64 base = table_off[h] + static_cast<u64>(seg_index[sg]) * kSegment;
+    Summary sm{0, 0, 0, 0};
+    for (int i = threadIdx.x; i < kSegment; i += blockDim.x) {
+        const int c = keys[base + i];
+        if (c >= 0) consider(p, sm, v, src, c, vals[base + i]);
+    }
+    reduce_summary<32>(sm);
+    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sm;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        sm = threadIdx.x < 8 ? warp_part[threadIdx.x] : Summary{0, 0, 0, 0};
+        reduce_summary<32>(sm);
+        if (threadIdx.x == 0) partial[sg] = sm;
+    }
+}
+__global__ void k_affinity_heavy_finish(i64 count, const int* heavy, const int* seg_off, const Summary* partial,
+                                        RoundParams p) {
+    const int lane = threadIdx.x & 31;
+    const i64 h = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (h >= count) return;
+    const int v = heavy[h];
+    int src;
+    if (!is_mover(p, v, src)) return;
+    Summary sm{0, 0, 0, 0};
+    for (int i = seg_off[h] + lane; i < seg_off[h + 1]; i += 32) merge(sm, partial[i]);
+    reduce_summary<32>(sm);
+    if (lane == 0) decode(p, v, src, sm);
+}
+struct HeavySegments {
+    const int* rows;
+    const int* off;
+    i64 count;
+    __device__ int operator()(i64 i) const {
+        return i >= count ? 0 : static_cast<int>(heavy_slots(off[rows[i] + 1] - off[rows[i]]) / kSegment);
+    }
+};
+__global__ void k_emit_segments(i64 count, const int* heavy, const int* off, const int* seg_off, int* seg_hidx,
+                                int* seg_index) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= count) return;
+    const int segs = static_cast<int>(heavy_slots(off[heavy[h] + 1] - off[heavy[h]]) / kSegment);
+    for (int i = 0; i < segs; ++i) {
+        seg_hidx[seg_off[h] + i] = static_cast<int>(h);
+        seg_index[seg_off[h] + i] = i;
+    }
+}
+
 // Admission (src/coarsen.cu:1015-1075).  Total demand per target first;
 // requests to a target whose whole demand fits are accepted without any
 // ordering, the rest are ordered by (target, regret desc, tie desc, vertex).
@@ -626,20 +733,35 @@ struct LoadInt {
 
 // contraction_row_scatter (contraction_rows.cuh:18-38): every fine row is
 // copied into its coarse row's raw segment; intra-cluster entries -> INT_MAX.
-__global__ void k_scatter(i64 n, const int* off, const int* nbr, const u32* ew, const int* map, int* cursor,
+// The row's slot in the segment is reserved first (one atomic per row), then
+// light rows are copied by 8 lanes and heavy rows chunk-parallel.
+__global__ void k_row_base(i64 n, const int* off, const int* map, int* cursor, int* base) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n) base[v] = atomicAdd(cursor + map[v], off[v + 1] - off[v]);
+}
+__global__ void k_scatter(i64 n, const int* off, const int* nbr, const u32* ew, const int* map, const int* base,
                           int* raw_t, u32* raw_w) {
     const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
     const int lane = threadIdx.x & 7;
     if (v >= n) return;
-    const int c = map[v];
     const int begin = off[v], end = off[v + 1];
-    int out = 0;
-    if (lane == 0) out = atomicAdd(cursor + c, end - begin);
-    out = __shfl_sync(0xffu << (threadIdx.x & 24), out, 0, 8);
+    if (end - begin > kHeavyRow) return;
+    const int c = map[v];
+    const int out = base[v] - begin;
     for (int e = begin + lane; e < end; e += 8) {
         const int t = map[nbr[e]];
-        raw_t[out + e - begin] = t == c ? INT_MAX : t;
-        raw_w[out + e - begin] = edge_w(ew, e);
+        raw_t[out + e] = t == c ? INT_MAX : t;
+        raw_w[out + e] = edge_w(ew, e);
+    }
+}
+__global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int* raw_t, u32* raw_w) {
+    const int ch = blockIdx.x, v = g.chunk_row[ch];
+    const int c = map[v];
+    const int out = base[v] - g.off[v];
+    for (int e = g.chunk_begin[ch] + threadIdx.x; e < chunk_end(g, ch, v); e += blockDim.x) {
+        const int t = map[g.nbr[e]];
+        raw_t[out + e] = t == c ? INT_MAX : t;
+        raw_w[out + e] = edge_w(g.ew, e);
     }
 }
 
@@ -648,7 +770,7 @@ __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u6
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int r = c < nc ? raw[c] : 0;
-    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kLargeDegree ? 2 : 3;
+    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kBlockSortRow ? 2 : 3;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const unsigned mask = __ballot_sync(0xffffffffu, cls == k);
@@ -754,9 +876,9 @@ __global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off,
 // thread per run of equal keys sums it.
 __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
                                                          int* ucount) {
-    __shared__ int keys[kLargeDegree];
-    __shared__ u32 vals[kLargeDegree];
-    __shared__ unsigned char heads[kLargeDegree];
+    __shared__ int keys[kBlockSortRow];
+    __shared__ u32 vals[kBlockSortRow];
+    __shared__ unsigned char heads[kBlockSortRow];
     __shared__ int scan_smem[9];
     const int c = rows[blockIdx.x];
     const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
@@ -807,18 +929,20 @@ __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const 
     if (threadIdx.x == 0) ucount[c] = total;
 }
 
-// Rows above 4096 raw entries: records (row rank, target) -> global radix sort.
-__global__ void k_large_records(i64 count, const int* rows, const int* raw_off, const int* rec_off, const int* raw_t,
-                                const u32* raw_w, int tbits, u64* keys, u32* vals) {
-    const int j = blockIdx.x;
-    const int c = rows[j];
-    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
-    const int out = rec_off[j];
+// Rows above 4096 raw entries: records (row rank, target) -> global radix
+// sort.  Flat over records; the row of a record is found by binary search.
+__global__ void k_large_records(i64 records, i64 count, const int* rows, const int* raw_off, const int* rec_off,
+                                const int* raw_t, const u32* raw_w, int tbits, u64* keys, u32* vals) {
     const u64 sentinel = (1ULL << tbits) - 1;
-    for (int i = threadIdx.x; i < degree; i += blockDim.x) {
-        const int t = raw_t[begin + i];
-        keys[out + i] = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
-        vals[out + i] = raw_w[begin + i];
+    for (i64 r = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; r < records;
+         r += static_cast<i64>(gridDim.x) * blockDim.x) {
+        int lo = 0, hi = static_cast<int>(count);  // last j with rec_off[j] <= r
+        while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (rec_off[mid] <= r) lo = mid; else hi = mid; }
+        const int j = lo;
+        const int pos = raw_off[rows[j]] + static_cast<int>(r - rec_off[j]);
+        const int t = raw_t[pos];
+        keys[r] = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
+        vals[r] = raw_w[pos];
     }
 }
 struct LargeRowSize {
@@ -864,16 +988,60 @@ __global__ void k_large_counts(i64 count, const int* rows, const int* rec_off, c
     ucount[rows[j]] = static_cast<int>(last - first);
 }
 
-// contraction_copy_rows (contraction_rows.cuh:140-154).
+// contraction_copy_rows (contraction_rows.cuh:140-154); heavy coarse rows by chunks.
 __global__ void k_copy_rows(i64 nc, const int* raw_off, const int* raw_t, const u32* raw_w, const int* off, int* nbr,
                             u32* ew) {
     const i64 c = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
     const int lane = threadIdx.x & 7;
     if (c >= nc) return;
     const int begin = off[c], end = off[c + 1], raw = raw_off[c];
+    if (end - begin > kHeavyRow) return;
     for (int e = begin + lane; e < end; e += 8) {
         nbr[e] = raw_t[raw + e - begin];
         ew[e] = raw_w[raw + e - begin];
+    }
+}
+__global__ void k_copy_chunks(DGraph g, const int* raw_off, const int* raw_t, const u32* raw_w) {
+    const int ch = blockIdx.x, c = g.chunk_row[ch];
+    const int shift = raw_off[c] - g.off[c];
+    for (int e = g.chunk_begin[ch] + threadIdx.x; e < chunk_end(g, ch, c); e += blockDim.x) {
+        g.nbr[e] = raw_t[shift + e];
+        g.ew[e] = raw_w[shift + e];
+    }
+}
+
+// ---------------------------------------------------------------- chunk lists
+
+__global__ void k_heavy_counts(i64 n, const int* off, u64* sc) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    u64 rows = 0, chunks = 0;
+    if (v < n) {
+        const int d = off[v + 1] - off[v];
+        if (d > kHeavyRow) { rows = 1; chunks = (d + kChunk - 1) / kChunk; }
+    }
+    rows = warp_sum(rows);
+    chunks = warp_sum(chunks);
+    if ((threadIdx.x & 31) == 0 && rows) { atomicAdd(sc, rows); atomicAdd(sc + 1, chunks); }
+}
+struct IsHeavyRow {
+    const int* off;
+    __device__ bool operator()(i64 v) const { return off[v + 1] - off[v] > kHeavyRow; }
+};
+struct ChunkCount {
+    const int* heavy;
+    const int* off;
+    __device__ int operator()(i64 h) const { return (off[heavy[h] + 1] - off[heavy[h]] + kChunk - 1) / kChunk; }
+};
+__global__ void k_emit_chunks(i64 count, const int* heavy, const int* off, const int* chunk_off, int* chunk_row,
+                              int* chunk_hidx, int* chunk_begin) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= count) return;
+    const int v = heavy[h], d = off[v + 1] - off[v];
+    const int chunks = (d + kChunk - 1) / kChunk;
+    for (int i = 0; i < chunks; ++i) {
+        chunk_row[chunk_off[h] + i] = v;
+        chunk_hidx[chunk_off[h] + i] = static_cast<int>(h);
+        chunk_begin[chunk_off[h] + i] = off[v] + i * kChunk;
     }
 }
 
@@ -948,9 +1116,16 @@ private:
     u32* ties = nullptr;
     int* lists[4] = {};
     i64 list_size[4] = {};
-    u64* heavy_offsets = nullptr;
-    int* heavy_keys = nullptr;
-    u64* heavy_vals = nullptr;
+    // Global tables of the heavy rows (see k_affinity_heavy_*).
+    u64* table_off = nullptr;
+    int* table_keys = nullptr;
+    u64* table_vals = nullptr;
+    u64 table_slots = 0;
+    int* seg_off = nullptr;
+    int* seg_hidx = nullptr;
+    int* seg_index = nullptr;
+    Summary* partial = nullptr;
+    i64 segments = 0;
     int gain_bits = 64, target_bits = 32;
 
     u64 count_clusters() {
@@ -986,9 +1161,16 @@ void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 
         launch(k_affinity_large<false>, static_cast<int>(list_size[2]), 256, smem, ctx.stream, 
             list_size[2], lists[2], static_cast<const u64*>(nullptr), static_cast<int*>(nullptr), static_cast<u64*>(nullptr), p);
     }
-    if (list_size[3])
-        launch(k_affinity_large<true>, static_cast<int>(list_size[3]), 256, 0, ctx.stream, 
-            list_size[3], lists[3], heavy_offsets, heavy_keys, heavy_vals, p);
+    if (g.heavy_count) {
+        GP_CUDA(cudaMemsetAsync(table_keys, 0xff, sizeof(int) * table_slots, ctx.stream));
+        GP_CUDA(cudaMemsetAsync(table_vals, 0, sizeof(u64) * table_slots, ctx.stream));
+        launch(k_affinity_heavy_insert, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, table_off, table_keys,
+               table_vals, p);
+        launch(k_affinity_heavy_summary, static_cast<int>(segments), 256, 0, ctx.stream, g.heavy, seg_hidx, seg_index,
+               table_off, table_keys, table_vals, p, partial);
+        launch(k_affinity_heavy_finish, blocks_for(g.heavy_count * 32, kThreads), kThreads, 0, ctx.stream,
+               g.heavy_count, g.heavy, seg_off, partial, p);
+    }
 }
 
 AggregateOut Aggregator::run() {
@@ -1046,13 +1228,23 @@ AggregateOut Aggregator::run() {
             out.stats_heavy = sc[1] != 0;
             for (int c = 0; c < 4; ++c) list_size[c] = static_cast<i64>(sc[2 + c]);
             isolated = static_cast<i64>(sc[7]);
-            if (list_size[3]) {
-                heavy_offsets = A.alloc<u64>(static_cast<size_t>(list_size[3]));
-                u64* slot_total = ctx.dev_scalars;
-                exclusive_scan<u64>(A, s, list_size[3], HeavySlots{lists[3], g.off}, heavy_offsets, slot_total);
-                const u64 slots = ctx.read_scalars(1)[0];
-                heavy_keys = A.alloc<int>(slots);
-                heavy_vals = A.alloc<u64>(slots);
+            if (g.heavy_count) {
+                const i64 hc = g.heavy_count;
+                table_off = A.alloc<u64>(hc);
+                seg_off = A.alloc<int>(hc + 1);
+                exclusive_scan<u64>(A, s, hc, HeavySlots{g.heavy, g.off}, table_off, ctx.dev_scalars);
+                exclusive_scan<int>(A, s, hc + 1, HeavySegments{g.heavy, g.off, hc}, seg_off,
+                                    reinterpret_cast<int*>(ctx.dev_scalars + 1));
+                const u64* hs = ctx.read_scalars(2);
+                table_slots = hs[0];
+                segments = static_cast<i64>(hs[1] & 0xffffffffULL);
+                table_keys = A.alloc<int>(table_slots);
+                table_vals = A.alloc<u64>(table_slots);
+                seg_hidx = A.alloc<int>(segments);
+                seg_index = A.alloc<int>(segments);
+                partial = A.alloc<Summary>(segments);
+                launch(k_emit_segments, blocks_for(hc, kThreads), kThreads, 0, s, hc, g.heavy, g.off, seg_off, seg_hidx,
+                       seg_index);
             }
         }
     }
@@ -1196,8 +1388,16 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     GP_CUDA(cudaMemcpyAsync(cursor, raw_off, sizeof(int) * nc, cudaMemcpyDeviceToDevice, s));
     int* raw_t = A.alloc<int>(fine.m);
     u32* raw_w = A.alloc<u32>(fine.m);
-    launch(k_scatter, blocks_for(n * 8, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map, cursor,
-                                                                     raw_t, raw_w);
+    {
+        ArenaScope bs(A);
+        int* base = A.alloc<int>(n);
+        launch(k_row_base, vb, kThreads, 0, s, n, fine.off, agg.map, cursor, base);
+        launch(k_scatter, blocks_for(n * 8, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map,
+               static_cast<const int*>(base), raw_t, raw_w);
+        if (fine.chunks)
+            launch(k_scatter_chunks, static_cast<int>(fine.chunks), 256, 0, s, fine, agg.map,
+                   static_cast<const int*>(base), raw_t, raw_w);
+    }
     // Row classes by raw size.
     int* lists = A.alloc<int>(static_cast<size_t>(nc) * 4);
     ctx.clear_scalars(5);
@@ -1228,8 +1428,9 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         u64* keys_alt = A.alloc<u64>(large_records);
         u32* vals = A.alloc<u32>(large_records);
         u32* vals_alt = A.alloc<u32>(large_records);
-        launch(k_large_records, static_cast<int>(count[3]), 256, 0, s, count[3], large, raw_off, rec_off, raw_t,
-                                                                         raw_w, tbits, keys, vals);
+        launch(k_large_records, std::min(blocks_for(large_records, kThreads), 148 * 16), kThreads, 0, s,
+               large_records, count[3], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
+               vals);
         radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, 0, tbits + jbits);
         u32* hpos = A.alloc<u32>(large_records);
         u32* heads_total = reinterpret_cast<u32*>(ctx.dev_scalars);
@@ -1251,8 +1452,12 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     coarse.m = *reinterpret_cast<const int*>(ctx.host_scalars);
     coarse.nbr = ctx.persist.alloc<int>(coarse.m);
     coarse.ew = ctx.persist.alloc<u32>(coarse.m);
+    build_chunks(ctx, coarse);
     launch(k_copy_rows, blocks_for(nc * 8, kThreads), kThreads, 0, s, nc, raw_off, raw_t, raw_w, coarse.off,
-                                                                       coarse.nbr, coarse.ew);
+           coarse.nbr, coarse.ew);
+    if (coarse.chunks)
+        launch(k_copy_chunks, static_cast<int>(coarse.chunks), 256, 0, s, coarse, static_cast<const int*>(raw_off),
+               static_cast<const int*>(raw_t), static_cast<const u32*>(raw_w));
     coarse.vw = agg.cvw;
     coarse.implicit_unit = false;
     coarse.incident_bound = row_bound;
@@ -1267,6 +1472,31 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
 
 }  // namespace
 
+// Heavy-row list and chunk list of a level, in the hierarchy's storage.
+void build_chunks(Context& ctx, DGraph& g) {
+    cudaStream_t s = ctx.stream;
+    g.heavy = nullptr;
+    g.heavy_count = 0;
+    g.chunks = 0;
+    if (g.n <= 0) return;
+    ctx.clear_scalars(2);
+    launch(k_heavy_counts, blocks_for(g.n, kThreads), kThreads, 0, s, g.n, g.off, ctx.dev_scalars);
+    const u64* sc = ctx.read_scalars(2);
+    g.heavy_count = static_cast<i64>(sc[0]);
+    g.chunks = static_cast<i64>(sc[1]);
+    if (!g.heavy_count) return;
+    g.heavy = ctx.persist.alloc<int>(g.heavy_count);
+    g.chunk_row = ctx.persist.alloc<int>(g.chunks);
+    g.chunk_hidx = ctx.persist.alloc<int>(g.chunks);
+    g.chunk_begin = ctx.persist.alloc<int>(g.chunks);
+    ArenaScope scope(ctx.scratch);
+    int* chunk_off = ctx.scratch.alloc<int>(g.heavy_count);
+    select_if(ctx.scratch, s, g.n, IsHeavyRow{g.off}, WriteIndex{g.heavy}, static_cast<u32*>(nullptr));
+    exclusive_scan<int>(ctx.scratch, s, g.heavy_count, ChunkCount{g.heavy, g.off}, chunk_off, static_cast<int*>(nullptr));
+    launch(k_emit_chunks, blocks_for(g.heavy_count, kThreads), kThreads, 0, s, g.heavy_count, g.heavy, g.off,
+           static_cast<const int*>(chunk_off), g.chunk_row, g.chunk_hidx, g.chunk_begin);
+}
+
 // coarsen_impl (src/coarsen.cu:1762-2060).
 Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
     cudaStream_t s = ctx.stream;
@@ -1274,6 +1504,7 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
     Workspace ws;
     DGraph current = input;
     if (current.n > 0) {
+        build_chunks(ctx, current);
         ws.row_bounds = ctx.persist.alloc<u64>(current.n);
         ctx.clear_scalars(7);
         if (current.m / current.n < 8)
@@ -1282,6 +1513,13 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
         else
             launch(k_level0_meta<32>, blocks_for(current.n * 32, kThreads), kThreads, 0, s, 
                 current.n, current.off, current.nbr, current.ew, current.vw, ws.row_bounds, ctx.dev_scalars);
+        if (current.chunks) {
+            // The row pass wrote 0 for heavy rows; their chunks add the sums.
+            launch(k_level0_meta_chunks, static_cast<int>(current.chunks), 256, 0, s, current, ws.row_bounds,
+                   ctx.dev_scalars);
+            launch(k_heavy_bound_max, blocks_for(current.heavy_count, kThreads), kThreads, 0, s, current.heavy_count,
+                   static_cast<const int*>(current.heavy), static_cast<const u64*>(ws.row_bounds), ctx.dev_scalars);
+        }
         const u64* sc = ctx.read_scalars(7);
         ws.original_vertices = current.n;
         ws.maximum_row_weight = sc[0];

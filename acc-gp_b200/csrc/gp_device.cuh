@@ -34,11 +34,29 @@ struct Failure : std::runtime_error {
 
 // Number of kernels this library launched; every launch goes through launch().
 extern thread_local u64 g_launches;
+
+// Optional per-kernel timing: when a profiler is installed, launches of the
+// kernels whose name contains its pattern are bracketed by CUDA events on
+// their own stream (gp_profile_begin / gp_profile_end).
+struct KernelProfiler {
+    std::string pattern;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    size_t used = 0;
+    bool matches(const void* kernel);
+    void before(cudaStream_t s);
+    void after(cudaStream_t s);
+    std::vector<std::pair<const void*, bool>> cache;
+};
+extern thread_local KernelProfiler* g_profiler;
+
 template <class... Params, class... Args>
 inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
                    Args&&... args) {
     ++g_launches;
+    const bool timed = g_profiler && g_profiler->matches(reinterpret_cast<const void*>(kernel));
+    if (timed) g_profiler->before(stream);
     kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
+    if (timed) g_profiler->after(stream);
 }
 
 inline int blocks_for(i64 items, int per_block) {

@@ -12,6 +12,12 @@ constexpr int kInvalid = 0x7fffffff;  // SCLP_INVALID (src/coarsen.cu:292)
 // ew == nullptr means unit edge weights.  The three metadata fields follow
 // the reference's meaning exactly: maximum_degree is a bound (exact after an
 // aggregation pass), incident_bound bounds every row's weight sum.
+// Rows longer than kHeavyRow entries are split into chunks of at most
+// kChunk entries so that row-parallel kernels give them many blocks instead
+// of one serial warp (R-MAT hubs have 10^5 neighbours).
+constexpr int kHeavyRow = 2048;
+constexpr int kChunk = 2048;
+
 struct DGraph {
     i64 n = 0, m = 0;
     int* off = nullptr;
@@ -22,7 +28,21 @@ struct DGraph {
     u64 maximum_degree = ~0ULL;
     bool has_heavy_rows = true;
     u64 incident_bound = ~0ULL;
+    // Heavy rows (ascending) and their chunks; built by build_chunks().
+    int* heavy = nullptr;
+    i64 heavy_count = 0;
+    int* chunk_row = nullptr;
+    int* chunk_hidx = nullptr;  // index of the chunk's row in `heavy`
+    int* chunk_begin = nullptr;
+    i64 chunks = 0;
 };
+
+// Chunk-parallel loop body helpers: the chunk's edge range.
+__device__ __forceinline__ int chunk_end(const DGraph& g, int chunk, int row) {
+    const int end = g.chunk_begin[chunk] + kChunk;
+    const int row_end = g.off[row + 1];
+    return end < row_end ? end : row_end;
+}
 
 struct Hierarchy {
     std::vector<DGraph> levels;  // level 0 is the input
@@ -77,6 +97,7 @@ struct Context {
 };
 
 // Entry points of the pipeline stages.
+void build_chunks(Context& ctx, DGraph& g);
 Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o);
 void keep_levels(Context& ctx, const Hierarchy& h);
 

@@ -15,12 +15,39 @@
 
 struct gp_context {
     gp::Context ctx;
+    gp::KernelProfiler profiler;
     gp::CoarsenOptions defaults;  // overridable per context, see gp_set_option
     bool seed_matching = true, fast_path = true;
     int cluster_size_factor = 0, fine_factor = 64, growth = 8, heavy_limit = 64;
 };
 
 namespace gp {
+
+thread_local KernelProfiler* g_profiler = nullptr;
+
+bool KernelProfiler::matches(const void* kernel) {
+    for (auto& entry : cache)
+        if (entry.first == kernel) return entry.second;
+    const char* name = nullptr;
+    bool hit = false;
+    if (cudaFuncGetName(&name, kernel) == cudaSuccess && name) hit = std::strstr(name, pattern.c_str()) != nullptr;
+    cache.emplace_back(kernel, hit);
+    return hit;
+}
+void KernelProfiler::before(cudaStream_t s) {
+    if (used == events.size()) {
+        cudaEvent_t a, b;
+        GP_CUDA(cudaEventCreate(&a));
+        GP_CUDA(cudaEventCreate(&b));
+        events.emplace_back(a, b);
+    }
+    GP_CUDA(cudaEventRecord(events[used].first, s));
+}
+void KernelProfiler::after(cudaStream_t s) {
+    GP_CUDA(cudaEventRecord(events[used].second, s));
+    ++used;
+}
+
 namespace {
 
 __global__ void k_fill_ones(i64 n, u32* p) {
@@ -29,34 +56,40 @@ __global__ void k_fill_ones(i64 n, u32* p) {
 }
 
 // Shape and range checks of a device CSR (validate_weighted_shape,
-// src/graph.cpp:118-155).  Scalars: 0 bad offsets, 1 bad neighbour,
-// 2 zero vertex weight, 3 total vertex weight, 4 odd-weight probe (directed
-// edge-weight sum).
-__global__ void k_validate(i64 n, i64 m, const int* off, const int* nbr, const u32* vw, const u32* ew, u64* sc) {
-    u64 total = 0, directed = 0;
-    u32 bad_off = 0, bad_nbr = 0, zero = 0;
+// src/graph.cpp:118-155), as two flat grid-stride sweeps so that long rows
+// do not serialise.  Scalars: 0 bad offsets, 1 bad neighbour, 2 zero vertex
+// weight, 3 total vertex weight, 4 directed edge-weight sum.
+__global__ void k_validate_vertices(i64 n, i64 m, const int* off, const u32* vw, u64* sc) {
+    u64 total = 0;
+    u32 bad = 0, zero = 0;
     for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
         const int b = off[v], e = off[v + 1];
-        if (b > e || b < 0 || e > m) { bad_off = 1; continue; }
+        bad |= b > e || b < 0 || e > m || (v == 0 && b != 0) || (v == n - 1 && e != m);
         const u32 w = vw ? vw[v] : 1u;
         zero |= w == 0;
         total += w;
-        for (int i = b; i < e; ++i) {
-            const int u = nbr[i];
-            bad_nbr |= u < 0 || u >= n;
-            directed += ew ? ew[i] : 1u;
-        }
     }
     total = warp_sum(total);
-    directed = warp_sum(directed);
-    bad_off = __any_sync(0xffffffffu, bad_off);
-    bad_nbr = __any_sync(0xffffffffu, bad_nbr);
+    bad = __any_sync(0xffffffffu, bad);
     zero = __any_sync(0xffffffffu, zero);
     if ((threadIdx.x & 31) == 0) {
-        if (bad_off) atomicOr(sc + 0, 1ULL);
-        if (bad_nbr) atomicOr(sc + 1, 1ULL);
+        if (bad) atomicOr(sc + 0, 1ULL);
         if (zero) atomicOr(sc + 2, 1ULL);
         if (total) atomicAdd(sc + 3, total);
+    }
+}
+__global__ void k_validate_edges(i64 n, i64 m, const int* nbr, const u32* ew, u64* sc) {
+    u64 directed = 0;
+    u32 bad = 0;
+    for (i64 e = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int u = nbr[e];
+        bad |= u < 0 || u >= n;
+        directed += ew ? ew[e] : 1u;
+    }
+    directed = warp_sum(directed);
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicOr(sc + 1, 1ULL);
         if (directed) atomicAdd(sc + 4, directed);
     }
 }
@@ -156,8 +189,8 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     // Device-side validation: it also yields the total weight and the
     // directed edge-weight sum the reference checks at the end.
     ctx.clear_scalars(5);
-    launch(k_validate, std::min(blocks_for(n, 256), 148 * 16), 256, 0, s, n, m, g.off, g.nbr, g.vw, g.ew,
-           ctx.dev_scalars);
+    launch(k_validate_vertices, std::min(blocks_for(n, 256), 148 * 16), 256, 0, s, n, m, g.off, g.vw, ctx.dev_scalars);
+    launch(k_validate_edges, std::min(blocks_for(m, 256), 148 * 16), 256, 0, s, n, m, g.nbr, g.ew, ctx.dev_scalars);
     const u64* vs = ctx.read_scalars(5);
     if (vs[0]) fail(GP_INVALID_ARGUMENT, "weighted CSR offsets are not monotone");
     if (vs[1]) fail(GP_INVALID_ARGUMENT, "weighted CSR contains an invalid neighbor");
@@ -319,6 +352,34 @@ gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
     else if (key == "heavy_edge_degree_limit" && value >= 2 && value <= 256) ctx->heavy_limit = static_cast<int>(value);
     else { set_error("unknown option or value out of range: " + key); return GP_INVALID_ARGUMENT; }
     return GP_OK;
+}
+
+gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring) {
+    if (!ctx || !kernel_substring) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    ctx->profiler.pattern = kernel_substring;
+    ctx->profiler.cache.clear();
+    ctx->profiler.used = 0;
+    g_profiler = &ctx->profiler;
+    return GP_OK;
+}
+
+gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms) {
+    if (!ctx) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    return guarded([&]() -> gp_status {
+        g_profiler = nullptr;
+        auto& p = ctx->profiler;
+        double ms = 0;
+        for (size_t i = 0; i < p.used; ++i) {
+            GP_CUDA(cudaEventSynchronize(p.events[i].second));
+            float t = 0;
+            GP_CUDA(cudaEventElapsedTime(&t, p.events[i].first, p.events[i].second));
+            ms += t;
+        }
+        if (launches) *launches = p.used;
+        if (total_ms) *total_ms = ms;
+        p.used = 0;
+        return GP_OK;
+    });
 }
 
 gp_status gp_level_count(gp_context* ctx, int32_t* levels) {

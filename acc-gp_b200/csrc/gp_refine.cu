@@ -26,12 +26,22 @@ struct Sample {
 
 // ---------------------------------------------------------------- small kernels
 
+__global__ void k_cut_chunks(DGraph g, const int* labels, u64* out) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    const int p = labels[v];
+    u64 local = 0;
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x)
+        if (labels[g.nbr[e]] != p) local += edge_w(g.ew, e);
+    local = warp_sum(local);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
 __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, u64* out) {
     const int lane = threadIdx.x & 31;
     u64 local = 0;
     for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
          v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int p = labels[v];
+        if (off[v + 1] - off[v] > kHeavyRow) continue;  // k_cut_chunks
         for (int e = off[v] + lane; e < off[v + 1]; e += 32)
             if (labels[nbr[e]] != p) local += edge_w(ew, e);
     }
@@ -108,9 +118,11 @@ __global__ void k_build(i64 n, const int* off, const int* nbr, const u32* ew, co
          v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         for (int p = lane; p < k; p += 32) row[p] = 0;
         __syncwarp();
-        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
-            const int u = nbr[e];
-            if (u != v) atomicAdd(row + labels[u], static_cast<C>(edge_w(ew, e)));
+        if (off[v + 1] - off[v] <= kHeavyRow) {  // heavy rows: zeros here, k_build_chunks adds
+            for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+                const int u = nbr[e];
+                if (u != v) atomicAdd(row + labels[u], static_cast<C>(edge_w(ew, e)));
+            }
         }
         __syncwarp();
         C total = 0;
@@ -123,6 +135,28 @@ __global__ void k_build(i64 n, const int* off, const int* nbr, const u32* ew, co
         if (lane == 0) totals[v] = total;
         __syncwarp();
     }
+}
+
+template <class C>
+__global__ void k_build_chunks(DGraph g, const int* labels, int k, C* A, C* totals) {
+    extern __shared__ unsigned char smem_build[];
+    C* hist = reinterpret_cast<C*>(smem_build);
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) hist[p] = 0;
+    __syncthreads();
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
+        const int u = g.nbr[e];
+        if (u != v) atomicAdd(hist + labels[u], static_cast<C>(edge_w(g.ew, e)));
+    }
+    __syncthreads();
+    C total = 0;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        const C x = hist[p];
+        if (x) atomicAdd(A + static_cast<i64>(v) * k + p, x);
+        total += x;
+    }
+    total = warp_sum(total);
+    if ((threadIdx.x & 31) == 0 && total) atomicAdd(totals + v, total);
 }
 
 // ---------------------------------------------------------------- label propagation
@@ -225,6 +259,7 @@ __global__ void k_filter(LpParams q) {
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
          i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int v = q.cand[i];
+        if (q.off[v + 1] - q.off[v] > kHeavyRow) continue;  // k_filter_chunks / k_filter_finish
         const int s = q.labels[v], t = q.targets[v];
         const long long gain = q.gains[v];
         long long corr = 0;
@@ -252,6 +287,48 @@ __global__ void k_filter(LpParams q) {
     }
 }
 
+// Heavy candidates: partial corrections per chunk, then the decision
+// (incremental_heavy_priority / incremental_finish_heavy_priority,
+// incremental.cuh:395-438).
+__global__ void k_filter_chunks(DGraph g, LpParams q, long long* corr_acc) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    const int t = q.targets[v];
+    if (t < 0) return;
+    const int s = q.labels[v];
+    const long long gain = q.gains[v];
+    long long corr = 0;
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
+        const int u = g.nbr[e];
+        if (u == v) continue;
+        const int tu = q.targets[u];
+        if (tu < 0) continue;
+        const long long gu = q.gains[u];
+        if (!(gu > gain || (gu == gain && u < v))) continue;
+        const int lu = q.labels[u];
+        corr += static_cast<long long>(edge_w(g.ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+    }
+    corr = warp_sum(corr);
+    if ((threadIdx.x & 31) == 0 && corr)
+        atomicAdd(reinterpret_cast<u64*>(corr_acc + g.chunk_hidx[c]), static_cast<u64>(corr));
+}
+__global__ void k_filter_finish(i64 count, const int* heavy, const long long* corr_acc, LpParams q) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= count) return;
+    const int v = heavy[h];
+    const int t = q.targets[v];
+    if (t < 0) return;
+    const int s = q.labels[v];
+    const long long total = q.gains[v] + corr_acc[h];
+    bool keep;
+    if (q.prices) {
+        const u64 w = q.vw[v];
+        const double adj = __dsub_rn(repair_cost(s, w, q.loads, q.capacity, q.prices),
+                                     repair_cost(t, w, q.loads, q.capacity, q.prices));
+        keep = __dadd_rn(static_cast<double>(total), adj) >= 0;
+    } else keep = total >= 0;
+    q.flags[v] = keep;
+}
+
 // Candidates with a kept move -> mover list (incremental_compact_candidates).
 __global__ void k_compact_movers(LpParams q) {
     const i64 count = static_cast<i64>(q.counters[0]);
@@ -275,6 +352,7 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
          i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int v = movers[i];
+        if (off[v + 1] - off[v] > kHeavyRow) continue;  // k_update_chunks
         const int s = labels[v], t = targets[v];
         long long gain = 0;
         for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
@@ -296,6 +374,35 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
         }
     }
     if (lane == 0 && total) atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(total));
+}
+
+// Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,
+// incremental.cuh:508-530); a row moves when its flag is set.
+template <class C>
+__global__ void k_update_chunks(DGraph g, const int* labels, const int* targets, const int* flags, int k, C* A,
+                                long long* delta, Sample* samples) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    if (!flags[v]) return;
+    const int s = labels[v], t = targets[v];
+    long long gain = 0;
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
+        const int u = g.nbr[e];
+        if (u == v) continue;
+        const int old = labels[u];
+        const bool moves = flags[u] != 0;
+        const int nw = moves ? targets[u] : old;
+        const u32 w = edge_w(g.ew, e);
+        atomicAdd(A + static_cast<i64>(u) * k + s, static_cast<C>(0) - static_cast<C>(w));
+        atomicAdd(A + static_cast<i64>(u) * k + t, static_cast<C>(w));
+        if (!moves || u > v) gain += static_cast<long long>(w) * ((s != old) - (t != nw));
+    }
+    gain = warp_sum(gain);
+    if ((threadIdx.x & 31) == 0 && gain) {
+        atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(gain));
+        if (samples) atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
+    }
+    if (samples && threadIdx.x == 0 && g.chunk_begin[c] == g.off[v])
+        atomicAdd(&samples[s].weight, static_cast<u64>(g.vw[v]));
 }
 
 // incremental_commit (incremental.cuh:532-547) with per-block aggregation of
@@ -331,23 +438,30 @@ __global__ void k_clear_flags(i64 count, const int* movers, const u64* live_coun
 
 // Deterministic gain bucket: smallest j with 1.5^j >= (current-best)/relief,
 // evaluated exactly (balance_gain_bucket, incremental.cuh:553-557, computes
-// the same ceil(log(x)/log(1.5)) in floating point).
+// the same ceil(log(x)/log(1.5)) in floating point).  1.5^j >= G/R is
+// 3^j R >= 2^j G for j >= 0 and 2^-j R >= 3^-j G for j < 0; a binary search
+// over j in [-23, 24] with 128-bit products settles it.
+__constant__ u64 c_pow3[25] = {1ULL, 3ULL, 9ULL, 27ULL, 81ULL, 243ULL, 729ULL, 2187ULL, 6561ULL, 19683ULL,
+                               59049ULL, 177147ULL, 531441ULL, 1594323ULL, 4782969ULL, 14348907ULL, 43046721ULL,
+                               129140163ULL, 387420489ULL, 1162261467ULL, 3486784401ULL, 10460353203ULL,
+                               31381059609ULL, 94143178827ULL, 282429536481ULL};
+__device__ __forceinline__ bool bucket_reaches(int j, u64 G, u64 R) {
+    const int a = j < 0 ? -j : j;
+    const unsigned __int128 p3 = c_pow3[a], p2 = static_cast<unsigned __int128>(1) << a;
+    return j >= 0 ? static_cast<unsigned __int128>(R) * p3 >= static_cast<unsigned __int128>(G) * p2
+                  : static_cast<unsigned __int128>(R) * p2 >= static_cast<unsigned __int128>(G) * p3;
+}
 __device__ int gain_bucket(u64 best, u64 current, u64 relief) {
     if (best > current) return 0;
     if (best == current) return 1;
-    const unsigned __int128 G = current - best, R = relief;
-    unsigned __int128 p3 = 1, p2 = 1;  // 3^a, 2^a
-    // j < 0: 2^-j R >= 3^-j G ; check j = -23 .. -1 in increasing order.
-    for (int j = -23; j <= 24; ++j) {
-        unsigned __int128 lhs = R, rhs = G;
-        const int a = j < 0 ? -j : j;
-        p3 = 1;
-        p2 = 1;
-        for (int i = 0; i < a; ++i) { p3 *= 3; p2 *= 2; }
-        if (j >= 0) { lhs *= p3; rhs *= p2; } else { lhs *= p2; rhs *= p3; }
-        if (lhs >= rhs) return max(2, min(49, 25 + j));
+    const u64 G = current - best, R = relief;
+    if (!bucket_reaches(24, G, R)) return 49;
+    int lo = -23, hi = 24;  // smallest j in [lo, hi] that reaches
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (bucket_reaches(mid, G, R)) hi = mid; else lo = mid + 1;
     }
-    return 49;
+    return max(2, min(49, 25 + lo));
 }
 
 // initialize_receiver_slack (rebalance_select.cuh:79-104) by one thread.
@@ -1022,6 +1136,7 @@ private:
     Sample* samples = nullptr;
     u32* rorder = nullptr;
     u64* counters = nullptr;  // device: 0 cand, 1 movers, 2 delta, 3 max load, 4.. scratch
+    long long* corr_acc = nullptr;  // per heavy row: priority-filter correction
     u64 cut = 0, revision = 0;
     u64 max_load_host = 0;
 
@@ -1031,6 +1146,9 @@ private:
     void build() {
         const size_t smem = 8 * k * sizeof(T);
         launch(k_build<T>, grid_for(n * 32, kThreads), kThreads, smem, s(), n, g.off, g.nbr, g.ew, labels, k, A, totals);
+        if (g.chunks)
+            launch(k_build_chunks<T>, static_cast<int>(g.chunks), 256, sizeof(T) * k, s(), g,
+                   static_cast<const int*>(labels), k, A, totals);
     }
     // Applies the movers listed in `list` (count on device at `live`):
     // cache/cut update, commit, flag reset.  Returns the cut decrease.
@@ -1039,6 +1157,10 @@ private:
         launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
                g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
                sample ? samples : static_cast<Sample*>(nullptr));
+        if (g.chunks)
+            launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
+                   static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
+                   reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr));
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
         launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
@@ -1065,6 +1187,12 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     else if (W == 16) launch(k_proposals<T, 16>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
     else launch(k_proposals<T, 32>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
     launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
+    if (g.chunks) {
+        GP_CUDA(cudaMemsetAsync(corr_acc, 0, sizeof(long long) * g.heavy_count, s()));
+        launch(k_filter_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, q, corr_acc);
+        launch(k_filter_finish, blocks_for(g.heavy_count, kThreads), kThreads, 0, s(), g.heavy_count,
+               static_cast<const int*>(g.heavy), static_cast<const long long*>(corr_acc), q);
+    }
     launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q);
     apply(movers, counters + 1, n, true, false);
     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters, 4 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
@@ -1300,6 +1428,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     cand = A_.alloc<int>(n);
     movers = A_.alloc<int>(n);
     counters = A_.alloc<u64>(8);
+    corr_acc = A_.alloc<long long>(g.heavy_count + 1);
     int* saved_labels = A_.alloc<int>(n);
     u64* saved_loads = A_.alloc<u64>(k);
     GP_CUDA(cudaMemsetAsync(locks, 0, n, s()));
@@ -1391,6 +1520,7 @@ u64 device_cut(Context& ctx, const DGraph& g, const int* labels) {
     ctx.clear_scalars(1);
     launch(k_cut, std::min(blocks_for(g.n * 32, 256), 148 * 32), 256, 0, ctx.stream, g.n, g.off, g.nbr, g.ew, labels,
            ctx.dev_scalars);
+    if (g.chunks) launch(k_cut_chunks, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, labels, ctx.dev_scalars);
     const u64 d = ctx.read_scalars(1)[0];
     if (d & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
     return d / 2;

@@ -1,0 +1,335 @@
+"""Benchmark of the gpart_b200 partitioner on its headline workload.
+
+Workload: R-MAT scale 22 (4,194,304 vertices, edge factor 16,
+a=0.57 b=0.19 c=0.19, symmetrised, self loops and duplicates removed,
+~125M directed CSR entries, unit weights), k=64, epsilon=1.03, seed 0.
+A step is one complete partition of that graph (coarsening, the METIS step,
+refinement) through the C ABI.  The graph is seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  `value` is whole-job throughput in graphs/s with the
+input resident in HBM; `e2e` is the same metric through gp_partition with the
+graph in pinned host memory (host->device copy and label read-back inside the
+timed region).  Multi-GPU runs are independent replicas (one graph per rank,
+no collective on the data path): weak scaling.
+
+--impl reference times the reference partitioner's own build
+(oracle/_ref/gpart_partition_standard, compiled for sm_100a from its unmodified
+sources) on the same graph, metric and config.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+WORKLOAD = dict(workload="rmat22_k64", graph="R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, seed 0",
+                k=64, epsilon=1.03, seed=0, vertices=4194304)
+METRIC = "partition ms & batched graphs/s at k=64 ε=1.03; cut vs ref; HBM GB/s"
+# Kernel whose roofline fraction is reported.
+DOMINANT_KERNEL = "k_update"
+
+
+def load_package():
+    pkg = os.path.join(ROOT, "acc-gp_b200")
+    spec = importlib.util.spec_from_file_location("acc_gp_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["acc_gp_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, device_index: int):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        indices = sorted({r[0] for r in rows})
+        pick = str(device_index) if str(device_index) in indices else indices[0]
+        rows = [r for r in rows if r[0] == pick]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, value in zip(names, r[5:9]):
+                if value.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def cpu_baseline(gp, seconds_budget=30.0):
+    """The serial CPU restatement (oracle/) on a bounded sample: R-MAT scale 19
+    with the workload's generator parameters and k; graphs/s is scaled to the
+    full workload by directed entries (linear in edges)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: E402  (test infrastructure; CPU baseline leg only)
+    sample = gp.rmat(19, 16, 0.57, 0.19, 0.19, 0)
+    t = time.perf_counter()
+    oracle.partition(sample, WORKLOAD["k"], WORKLOAD["epsilon"], WORKLOAD["seed"])
+    seconds = time.perf_counter() - t
+    full_m = 125_000_000  # directed entries of the R-MAT scale-22 workload (approximate)
+    value = (1.0 / seconds) * (sample.m / full_m)
+    return {"value": value, "unit": "graphs/s", "cores": 1, "kind": "port",
+            "sample": f"R-MAT scale 19 (n={sample.n}, m={sample.m}) k=64 in {seconds:.2f}s on 1 core; "
+                      f"graphs/s scaled to the scale-22 workload by directed entries"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    gp = load_package()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
+    n, m = g.n, g.m
+    k, eps, seed = WORKLOAD["k"], WORKLOAD["epsilon"], WORKLOAD["seed"]
+    dev = torch.device("cuda", local)
+    off_d = torch.from_numpy(g.offsets).to(dev)
+    nbr_d = torch.from_numpy(g.neighbors).to(dev)
+    labels_d = torch.empty(n, dtype=torch.int32, device=dev)
+    ctx = gp.Context(local)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(profile=False):
+        return ctx.partition_device(off_d.data_ptr(), nbr_d.data_ptr(), n, m, None, None, k, eps, seed,
+                                    labels_d.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler()
+    clocks.start()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.profile_begin(DOMINANT_KERNEL)
+    launches = 0
+    stats = []
+    start.record(stream)
+    for _ in range(args.steps):
+        st = step()
+        stats.append(st)
+        launches += st.kernel_launches
+    end.record(stream)
+    torch.cuda.synchronize()
+    dom_launches, dom_ms = ctx.profile_end()
+    if dist:
+        dist.barrier()
+    elapsed = start.elapsed_time(end) / 1000.0
+    clk = clocks.stop(local)
+    if dist:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * args.steps / elapsed
+    labels = labels_d.cpu().numpy()
+    verdict = gp.verify(g, labels, k, eps)
+    # End to end through gp_partition with the graph in pinned host memory.
+    off_h = torch.from_numpy(g.offsets).pin_memory()
+    nbr_h = torch.from_numpy(g.neighbors).pin_memory()
+    lab_h = torch.empty(n, dtype=torch.int32).pin_memory()
+    e2e_times = []
+    for i in range(args.steps + 1):
+        t0 = time.perf_counter()
+        ctx.partition_host_ptrs(off_h.data_ptr(), nbr_h.data_ptr(), n, m, None, None, k, eps, seed, lab_h.data_ptr())
+        t1 = time.perf_counter()
+        if i:  # first call warms the pinned path
+            e2e_times.append(t1 - t0)
+    e2e_elapsed = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    e2e_value = world * len(e2e_times) / e2e_elapsed
+    # Roofline of the dominant kernel: algorithmic bytes per launch / duration.
+    per_launch_ms = dom_ms / max(1, dom_launches)
+    dom_bytes = stats[-1].dominant_bytes if hasattr(stats[-1], "dominant_bytes") else None
+    peak, peak_kind = measured_peak_hbm()
+    roof = None
+    if dom_launches:
+        alg = dominant_bytes_per_launch(stats, dom_launches, args.steps)
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+        roof = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "launches": dom_launches, "avg_launch_ms": per_launch_ms,
+                "share_of_step": dom_ms / (elapsed * 1e3 / world) if elapsed > 0 else None}
+    vcycle_bytes = stats[-1].algorithmic_bytes
+    line = {
+        "metric": METRIC, "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}", l2="inputs larger than L2 (0.52 GB CSR)"),
+        "partition_ms": elapsed / args.steps * 1e3, "cut": int(stats[-1].edge_cut),
+        "verifier": {"cut": verdict["cut"], "max_load": verdict["max_load"], "capacity": verdict["capacity"],
+                     "capacity_ok": verdict["capacity_ok"]},
+        "stages_ms": {"coarsen": stats[-1].coarsen_seconds * 1e3, "initial": stats[-1].initial_seconds * 1e3,
+                      "uncoarsen": stats[-1].uncoarsen_seconds * 1e3},
+        "vcycle_hbm": {"algorithmic_bytes": vcycle_bytes,
+                       "achieved_gbs": vcycle_bytes / (elapsed / args.steps) / 1e9},
+        "e2e": {"value": e2e_value, "unit": "graphs/s", "h2d_bytes_per_step": 4 * (n + 1) + 4 * m,
+                "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_elapsed / len(e2e_times) * 1e3},
+        "gpu_launches": launches, "roofline": roof, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(gp)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def dominant_bytes_per_launch(stats, launches, steps):
+    """Algorithmic bytes of one k_update launch: every mover's row is read
+    (4 B neighbour + label, flag and target gathers of the neighbour, 16 B
+    per entry) and two 4-byte cache counters change per entry (8 B read +
+    8 B write).  The library reports the entries its update launches touched."""
+    total = sum(getattr(s, "update_entries", 0) for s in stats)
+    if not total:
+        return 0.0
+    return 32.0 * total / launches
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    binary = os.path.join(ROOT, "oracle", "_ref", "gpart_partition_standard")
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
+        return
+    gp = load_package()
+    g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
+    times, cuts = [], []
+    with tempfile.TemporaryDirectory() as tmp:
+        ip, ix, part = os.path.join(tmp, "g.indptr"), os.path.join(tmp, "g.indices"), os.path.join(tmp, "g.part")
+        gp.write_csr_int64(g, ip, ix)
+        walls = []
+        for i in range(args.warmup + args.steps):
+            w0 = time.perf_counter()
+            proc = subprocess.run([binary, ip, ix, str(WORKLOAD["k"]), part, repr(WORKLOAD["epsilon"]),
+                                   str(WORKLOAD["seed"])], capture_output=True, text=True)
+            w1 = time.perf_counter()
+            if proc.returncode != 0:
+                print(json.dumps({"impl": "reference", "unavailable": "reference run failed: " +
+                                  proc.stderr.strip()[-200:]}))
+                return
+            if i >= args.warmup:
+                times.append(float(re.search(r"algorithm_total_seconds=([0-9.eE+-]+)", proc.stdout).group(1)))
+                cuts.append(int(re.search(r"final_edge_cut=(\d+)", proc.stdout).group(1)))
+                walls.append(w1 - w0)
+    elapsed = sum(times)
+    value = len(times) / elapsed
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "graphs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / len(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="replicas1"), "cut": cuts[-1],
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": "full workload through the reference's own build (app/partition_main.cu compiled "
+                                   "for sm_100a from its sources), one process per step, its algorithm_total_seconds"},
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "process_wall_s_per_step": sum(walls) / len(walls),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def launch_list(args):
+    import torch
+    gp = load_package()
+    g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
+    dev = torch.device("cuda", 0)
+    off_d = torch.from_numpy(g.offsets).to(dev)
+    nbr_d = torch.from_numpy(g.neighbors).to(dev)
+    labels_d = torch.empty(g.n, dtype=torch.int32, device=dev)
+    ctx = gp.Context(0)
+    for _ in range(args.warmup + 1):
+        st = ctx.partition_device(off_d.data_ptr(), nbr_d.data_ptr(), g.n, g.m, None, None, WORKLOAD["k"],
+                                  WORKLOAD["epsilon"], WORKLOAD["seed"], labels_d.data_ptr())
+    torch.cuda.synchronize()
+    print(json.dumps({"launch_list": True, "launches_per_partition": st.kernel_launches,
+                      "algorithm_ms": st.algorithm_seconds * 1e3, "cut": st.edge_cut}), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch-list", action="store_true",
+                    help="run `--warmup` + one partition and exit (for the ncu launch list)")
+    args = ap.parse_args()
+    if args.launch_list:
+        launch_list(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

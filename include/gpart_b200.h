@@ -115,6 +115,13 @@ gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k,
                               int32_t* labels_out_device, void* stream,
                               gp_stats* stats);
 
+/* Kernel timing for measurement: between begin and end, every launch of a
+ * kernel whose name contains `kernel_substring` is bracketed by CUDA events
+ * on the stream it runs on; end returns the launch count and the summed
+ * device time in milliseconds.  Profiling is per host thread. */
+gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring);
+gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms);
+
 /* Hierarchy of the last call made with GP_FLAG_KEEP_HIERARCHY.  Level 0 is
  * the input.  gp_level_copy fills any non-NULL array; `map` (length n of the
  * level) maps this level's vertices to the next level and is absent for the
