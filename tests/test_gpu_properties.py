@@ -1,0 +1,118 @@
+"""GPU edge cases and size-independent properties: tiny and disconnected
+graphs, k at both ends, exact balance, invalid inputs, the device-pointer
+entry point, determinism, and a large R-MAT checked by the verifier."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def check(gp, g, labels, st, k, eps):
+    verdict = gp.verify(g, labels, k, eps)
+    assert verdict["capacity_ok"], verdict
+    assert verdict["cut"] == st.edge_cut
+    assert labels.min() >= 0 and labels.max() < k
+    return verdict
+
+
+@pytest.mark.parametrize("k", [2, 3, 8, 64, 128])
+def test_k_range_matches_oracle(gp, ctx, oracle, k):
+    g = gp.mesh3d(24, 24, 24)
+    labels, st = ctx.partition(g, k, 1.03, 5)
+    check(gp, g, labels, st, k, 1.03)
+    expected, cut = oracle.partition(g, k, 1.03, 5)
+    np.testing.assert_array_equal(labels, expected)
+
+
+def test_graph_below_cutoff_skips_coarsening(gp, ctx, oracle):
+    g = gp.grid2d(12, 12)  # n=144 <= 64*8: METIS on the input, then refinement
+    labels, st = ctx.partition(g, 8, 1.03, 0)
+    assert st.levels == 1
+    check(gp, g, labels, st, 8, 1.03)
+    np.testing.assert_array_equal(labels, oracle.partition(g, 8, 1.03, 0)[0])
+
+
+def test_isolated_vertices_and_components(gp, ctx, oracle):
+    base = gp.grid2d(60, 60)
+    n = base.n + 500  # 500 isolated vertices
+    off = np.concatenate([base.offsets, np.full(500, base.offsets[-1], np.int32)])
+    g = gp.Graph(off, base.neighbors)
+    labels, st = ctx.partition(g, 4, 1.03, 1)
+    check(gp, g, labels, st, 4, 1.03)
+    np.testing.assert_array_equal(labels, oracle.partition(g, 4, 1.03, 1)[0])
+
+
+def test_exact_balance(gp, ctx, oracle):
+    g = gp.grid2d(64, 64)
+    labels, st = ctx.partition(g, 4, 1.0, 2)
+    v = check(gp, g, labels, st, 4, 1.0)
+    assert v["max_load"] == 1024
+    np.testing.assert_array_equal(labels, oracle.partition(g, 4, 1.0, 2)[0])
+
+
+def test_weighted_rmat(gp, ctx, oracle):
+    g = gp.with_weights(gp.rmat(15, 12, 0.57, 0.19, 0.19, 3), 9, (1, 16), (1, 64))
+    labels, st = ctx.partition(g, 50, 1.05, 4)
+    check(gp, g, labels, st, 50, 1.05)
+    np.testing.assert_array_equal(labels, oracle.partition(g, 50, 1.05, 4)[0])
+
+
+def test_fewer_vertices_than_parts_is_rejected(gp, ctx):
+    g = gp.grid2d(3, 3)
+    with pytest.raises(gp.GpartError) as e:
+        ctx.partition(g, 16, 2.0, 0)
+    assert e.value.status in (1, 2)
+
+
+@pytest.mark.parametrize("defect", ["neighbor", "offsets", "zero_weight", "k"])
+def test_invalid_inputs_raise(gp, ctx, defect):
+    g = gp.grid2d(20, 20)
+    off, nbr = g.offsets.copy(), g.neighbors.copy()
+    vw = None
+    k = 4
+    if defect == "neighbor":
+        nbr[7] = g.n + 3
+    elif defect == "offsets":
+        off[10], off[11] = off[11], off[10]
+    elif defect == "zero_weight":
+        vw = np.ones(g.n, np.uint32)
+        vw[5] = 0
+    else:
+        k = 200
+    with pytest.raises(gp.GpartError) as e:
+        ctx.partition(gp.Graph(off, nbr, vw), k, 1.03, 0)
+    assert e.value.status == 1
+
+
+def test_device_entry_point_equals_host(gp, ctx):
+    import torch
+    g = gp.rmat(16, 16, 0.57, 0.19, 0.19, 2)
+    host_labels, st = ctx.partition(g, 32, 1.03, 7)
+    off = torch.from_numpy(g.offsets).cuda()
+    nbr = torch.from_numpy(g.neighbors).cuda()
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    st2 = ctx.partition_device(off.data_ptr(), nbr.data_ptr(), g.n, g.m, None, None, 32, 1.03, 7, out.data_ptr(),
+                               stream.cuda_stream)
+    np.testing.assert_array_equal(out.cpu().numpy(), host_labels)
+    assert st2.edge_cut == st.edge_cut
+
+
+def test_deterministic_and_independent_of_context(gp, ctx):
+    g = gp.rmat(18, 16, 0.57, 0.19, 0.19, 5)
+    a, sa = ctx.partition(g, 64, 1.03, 0)
+    b, sb = ctx.partition(g, 64, 1.03, 0)
+    with gp.Context(0) as other:
+        c, sc = other.partition(g, 64, 1.03, 0)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+    check(gp, g, a, sa, 64, 1.03)
+
+
+def test_rmat20_properties(gp, ctx):
+    """Full-size-class property check: reported cut == independent recount,
+    capacity respected, repeatable."""
+    g = gp.rmat(20, 16, 0.57, 0.19, 0.19, 0)
+    labels, st = ctx.partition(g, 64, 1.03, 0)
+    check(gp, g, labels, st, 64, 1.03)
+    assert st.levels >= 5 and st.kernel_launches > 0

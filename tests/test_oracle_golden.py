@@ -1,0 +1,69 @@
+"""The CPU oracle against golden vectors produced by the reference's own
+CUDA build (tests/golden/make_golden.py): every level of the hierarchy
+(sizes, metadata, CSR, weights, map) and the METIS labels must match
+bit-for-bit; the final partition must be feasible."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+CASE_NAMES = ["g2_k8", "g512_k16", "rmat14_k16", "rmat16_k64", "rmat18_k64", "mesh16w_k32", "mesh48_k64",
+              "mesh32w_k128", "odd_k32"]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+def test_oracle_hierarchy_matches_reference(name, gp, oracle, cases):
+    CASES, build = cases
+    spec, fx = CASES[name], golden(name)
+    g = build(gp, spec)
+    labels, cut = oracle.partition(g, spec["k"], spec["eps"], spec["seed"])
+    levels = oracle.levels()
+    assert len(levels) == len(fx["levels"])
+    for i, (a, b) in enumerate(zip(levels, fx["levels"])):
+        assert (a["n"], a["m"]) == (b["n"], b["m"]), f"level {i} size"
+        for key in ("maximum_degree", "has_heavy_rows", "incident_weight_bound"):
+            assert a[key] == b[key], f"level {i} {key}"
+        for key in ("offsets", "neighbors", "edge_weights", "vertex_weights", "map"):
+            if b[key] is None:
+                assert a[key] is None
+            else:
+                assert digest(a[key]) == b[key], f"level {i} {key}"
+    assert digest(oracle.initial_labels(levels[-1]["n"])) == fx["metis_labels"]
+    verdict = gp.verify(g, labels, spec["k"], spec["eps"])
+    assert verdict["capacity_ok"] and verdict["cut"] == cut
+    # The reference's repair is nondeterministic; its cut is a neighbour.
+    assert abs(cut - fx["reference_final_cut"]) <= 0.03 * fx["reference_final_cut"]
+
+
+def test_oracle_reproduces_reference_failure(gp, oracle, cases):
+    """odd_k4 has an odd self-loop weight sum; the reference exits with
+    'symmetric graph has odd directed edge weight' (src/refine.cu:713-715)."""
+    CASES, build = cases
+    fx = golden("odd_k4")
+    assert "odd directed edge weight" in fx["error"]
+    g = build(gp, CASES["odd_k4"])
+    with pytest.raises(oracle.OracleError, match="odd directed edge weight"):
+        oracle.partition(g, 4, 1.03, 11)
+
+
+def test_small_fixture_arrays(gp, oracle, cases):
+    """The stored full arrays of g2_k8 equal the oracle's level by level."""
+    import os
+    from conftest import GOLDEN
+    CASES, build = cases
+    arrays = np.load(os.path.join(GOLDEN, "g2_k8.npz"))
+    g = build(gp, CASES["g2_k8"])
+    oracle.partition(g, 8, 1.03, 0)
+    levels = oracle.levels()
+    for i, lv in enumerate(levels):
+        for key in ("offsets", "neighbors", "edge_weights", "vertex_weights", "map"):
+            name = f"l{i}_{key}"
+            if name in arrays.files:
+                np.testing.assert_array_equal(lv[key], arrays[name], err_msg=name)
+    np.testing.assert_array_equal(oracle.initial_labels(levels[-1]["n"]), arrays["metis"])
