@@ -296,6 +296,15 @@ class Context:
                                       _C.c_uint32(seed), _C.c_uint32(flags), _C.c_void_p(labels_ptr), _C.byref(stats)))
         return Stats._from(stats)
 
+    def evaluate_device(self, offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
+                        edge_weights_ptr, labels_ptr: int, k: int, cut_ptr: int, loads_ptr: int,
+                        stream_ptr=None) -> None:
+        """gp_evaluate_device: cut and part loads of device labels into device outputs."""
+        g = _Csr(n, m, offsets_ptr, neighbors_ptr, vertex_weights_ptr, edge_weights_ptr)
+        _check(self._lib.gp_evaluate_device(self._handle, _C.byref(g), _C.c_void_p(labels_ptr), _C.c_int32(k),
+                                            _C.c_void_p(cut_ptr), _C.c_void_p(loads_ptr),
+                                            _C.c_void_p(stream_ptr) if stream_ptr else None))
+
     def profile_begin(self, kernel_substring: str) -> None:
         """Time every launch of kernels whose name contains the substring."""
         _check(self._lib.gp_profile_begin(self._handle, kernel_substring.encode()))

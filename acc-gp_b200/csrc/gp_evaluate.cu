@@ -1,0 +1,111 @@
+// Evaluation of a labelling on a device-resident graph: the undirected cut
+// and the part loads, the two quantities refine_cut_kernel and
+// accumulate_part_weights_kernel (src/refine.cu:63-126) produce.  The
+// reduction is deterministic: every block of a fixed grid writes its partial
+// loads and partial cut to a scratch array, and one block sums the partials
+// in block order.
+#include "gp_graph.h"
+#include "gp_primitives.cuh"
+
+namespace gp {
+namespace {
+
+constexpr int kEvalBlocks = 148 * 4;
+constexpr int kEvalThreads = 256;
+constexpr int kEvalStride = kMaxParts + 1;  // k loads + 1 directed cut per block
+
+// Pass 1: block b writes partial[b * kEvalStride + p] for p < k (loads) and
+// partial[b * kEvalStride + k] (directed cut of the rows it scanned).
+__global__ void __launch_bounds__(kEvalThreads) k_eval_partials(i64 n, const int* off, const int* nbr, const u32* ew,
+                                                                const u32* vw, const int* labels, int k, u64* partial) {
+    __shared__ u64 loads[kMaxParts];
+    __shared__ u64 warp_cut[kEvalThreads / 32];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) loads[p] = 0;
+    __syncthreads();
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x)
+        atomicAdd(loads + labels[v], static_cast<u64>(vw ? vw[v] : 1u));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64 cut = 0;
+    for (i64 v = static_cast<i64>(blockIdx.x) * (blockDim.x / 32) + warp; v < n; v += static_cast<i64>(gridDim.x) * (blockDim.x / 32)) {
+        const int p = labels[v];
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32)
+            if (labels[nbr[e]] != p) cut += edge_w(ew, e);
+    }
+    cut = warp_sum(cut);
+    if (lane == 0) warp_cut[warp] = cut;
+    __syncthreads();
+    u64* out = partial + static_cast<i64>(blockIdx.x) * kEvalStride;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) out[p] = loads[p];
+    if (threadIdx.x == 0) {
+        u64 c = 0;
+        for (int w = 0; w < kEvalThreads / 32; ++w) c += warp_cut[w];
+        out[k] = c;
+    }
+}
+
+// Pass 2: sums the partials of all blocks in block order.
+__global__ void k_eval_reduce(int blocks, int k, const u64* partial, u64* cut_out, u64* loads_out) {
+    for (int p = threadIdx.x; p <= k; p += blockDim.x) {
+        u64 s = 0;
+        for (int b = 0; b < blocks; ++b) s += partial[static_cast<i64>(b) * kEvalStride + p];
+        if (p < k) loads_out[p] = s;
+        else *cut_out = s / 2;
+    }
+}
+
+void check_evaluate_args(const gp_csr* g, const int32_t* labels, int32_t k, const uint64_t* cut_out,
+                         const uint64_t* loads_out) {
+    if (!g || !labels || !cut_out || !loads_out || !g->offsets || (g->m > 0 && !g->neighbors))
+        fail(GP_INVALID_ARGUMENT, "graph, labels and outputs must not be NULL");
+    if (g->n <= 0 || g->m < 0 || g->n > 0x7fffffff || g->m > 0x7fffffff)
+        fail(GP_INVALID_ARGUMENT, "graph exceeds supported 32-bit CSR limits");
+    if (k < 1 || k > kMaxParts) fail(GP_INVALID_ARGUMENT, "k must be in 1..128");
+}
+
+void launch_evaluate(const gp_csr* g, const int32_t* labels, int32_t k, uint64_t* cut_out, uint64_t* loads_out,
+                     u64* partial, cudaStream_t s) {
+    launch(k_eval_partials, kEvalBlocks, kEvalThreads, 0, s, static_cast<i64>(g->n), g->offsets, g->neighbors,
+           g->edge_weights, g->vertex_weights, labels, static_cast<int>(k), partial);
+    launch(k_eval_reduce, 1, 128, 0, s, kEvalBlocks, static_cast<int>(k), static_cast<const u64*>(partial),
+           reinterpret_cast<u64*>(cut_out), reinterpret_cast<u64*>(loads_out));
+    GP_CUDA(cudaGetLastError());
+}
+
+template <class F>
+gp_status guarded_eval(F&& f) {
+    try {
+        return f();
+    } catch (const Failure& e) {
+        set_error(e.what());
+        return e.status;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return GP_INTERNAL;
+    }
+}
+
+}  // namespace
+}  // namespace gp
+
+using namespace gp;
+
+// Context accessor defined in gp_partition.cu.
+namespace gp { Context& context_of(gp_context* ctx); }
+
+extern "C" gp_status gp_evaluate_device(gp_context* ctx, const gp_csr* graph, const int32_t* labels, int32_t k,
+                                        uint64_t* cut_out, uint64_t* loads_out, void* stream) {
+    return guarded_eval([&]() -> gp_status {
+        if (!ctx) fail(GP_INVALID_ARGUMENT, "context is NULL");
+        check_evaluate_args(graph, labels, k, cut_out, loads_out);
+        Context& c = context_of(ctx);
+        GP_CUDA(cudaSetDevice(c.device));
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+        ArenaScope scope(c.scratch);
+        u64* partial = c.scratch.alloc<u64>(static_cast<size_t>(kEvalBlocks) * kEvalStride);
+        launch_evaluate(graph, labels, k, cut_out, loads_out, partial, s);
+        // The partials live in the context arena: keep them until the
+        // reduction has read them.
+        GP_CUDA(cudaStreamSynchronize(s));
+        return GP_OK;
+    });
+}

@@ -284,6 +284,10 @@ gp_status guarded(F&& f) {
 }  // namespace
 }  // namespace gp
 
+namespace gp {
+Context& context_of(gp_context* ctx) { return ctx->ctx; }
+}  // namespace gp
+
 using namespace gp;
 
 extern "C" {

@@ -115,6 +115,16 @@ gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k,
                               int32_t* labels_out_device, void* stream,
                               gp_stats* stats);
 
+/* Cut and part loads of a labelling of a device-resident graph
+ * (refine_cut_kernel + accumulate_part_weights_kernel, src/refine.cu:63-126).
+ * graph pointers, labels (n int32 in [0,k)), cut_out (1 uint64) and
+ * loads_out (k uint64) are device memory; cut_out receives the directed
+ * cut / 2.  Ordered on `stream` (NULL: the context stream); returns after the
+ * results are written.  Per-block partial sums live in the context arena. */
+gp_status gp_evaluate_device(gp_context* ctx, const gp_csr* graph, const int32_t* labels,
+                             int32_t k, uint64_t* cut_out, uint64_t* loads_out,
+                             void* stream);
+
 /* Kernel timing for measurement: between begin and end, every launch of a
  * kernel whose name contains `kernel_substring` is bracketed by CUDA events
  * on the stream it runs on; end returns the launch count and the summed

@@ -116,3 +116,18 @@ def test_rmat20_properties(gp, ctx):
     labels, st = ctx.partition(g, 64, 1.03, 0)
     check(gp, g, labels, st, 64, 1.03)
     assert st.levels >= 5 and st.kernel_launches > 0
+
+
+def test_evaluate_device_matches_verifier(gp, ctx):
+    import torch
+    g = gp.with_weights(gp.rmat(14, 16, 0.57, 0.19, 0.19, 6), 2, (1, 5), (1, 7))
+    k = 37
+    labels = (np.arange(g.n) * 7919 % k).astype(np.int32)
+    dev = [torch.from_numpy(a).cuda() for a in (g.offsets, g.neighbors, g.vertex_weights, g.edge_weights, labels)]
+    cut = torch.zeros(1, dtype=torch.int64, device="cuda")
+    loads = torch.zeros(k, dtype=torch.int64, device="cuda")
+    ctx.evaluate_device(dev[0].data_ptr(), dev[1].data_ptr(), g.n, g.m, dev[2].data_ptr(), dev[3].data_ptr(),
+                        dev[4].data_ptr(), k, cut.data_ptr(), loads.data_ptr())
+    verdict = gp.verify(g, labels, k, 2.0)
+    assert int(cut.item()) == verdict["cut"]
+    assert [int(x) for x in loads.cpu()] == verdict["loads"]
