@@ -346,6 +346,24 @@ class Context:
         return out
 
 
+def evaluate_device_static(offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
+                           edge_weights_ptr, labels_ptr: int, k: int, cut_ptr: int, loads_ptr: int,
+                           stream_ptr=None) -> None:
+    """gp_evaluate_device_static: the allocation-free twin of Context.evaluate_device.
+
+    For callers that must not let the library allocate device memory (a
+    framework allocator that owns the memory budget, an allocation-free
+    serving loop).  Scratch is a fixed 611 KB device array shared by all
+    calls on a device; overlapping calls race, k must be <= 128, and the
+    first call on a device should precede any stream capture.  Does not wait
+    for the results.
+    """
+    g = _Csr(n, m, offsets_ptr, neighbors_ptr, vertex_weights_ptr, edge_weights_ptr)
+    _check(library().gp_evaluate_device_static(_C.byref(g), _C.c_void_p(labels_ptr), _C.c_int32(k),
+                                               _C.c_void_p(cut_ptr), _C.c_void_p(loads_ptr),
+                                               _C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
 def partition(graph: Graph, k: int, epsilon: float = 1.03, seed: int = 0, flags: int = FLAG_QUIET):
     """One-shot partition on device 0; returns (labels, Stats)."""
     with Context(0) as ctx:

@@ -7,6 +7,8 @@
 #include "gp_graph.h"
 #include "gp_primitives.cuh"
 
+#include <mutex>
+
 namespace gp {
 namespace {
 
@@ -87,7 +89,57 @@ gp_status guarded_eval(F&& f) {
 }  // namespace
 }  // namespace gp
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot let a library call cudaMalloc:
+// a framework whose caching allocator owns the whole device-memory budget (a
+// raw cudaMalloc would bypass that budget and, on a full device, fail), or a
+// serving loop that must not allocate or free device memory once it runs,
+// because cudaMalloc/cudaFree may synchronise the device and stall the other
+// streams.  gp_evaluate_device_static needs no context and no allocation: its
+// per-block partial sums live in the fixed array below, which every GPU that
+// loads this library holds until the process exits.
+constexpr size_t kStaticScratchWords = static_cast<size_t>(gp::kEvalBlocks) * gp::kEvalStride;  // 611 KB
+static __device__ __align__(256) unsigned long long g_eval_static_scratch[kStaticScratchWords];
+
+namespace gp {
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+u64* g_static_address[kMaxDevices] = {};
+
+// Device address of the static scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device, with that device current, and cached.
+u64* static_scratch_address() {
+    int device = 0;
+    GP_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= kMaxDevices) fail(GP_INVALID_ARGUMENT, "device ordinal beyond 63");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_address[device]) {
+        void* address = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&address, g_eval_static_scratch);
+        if (err != cudaSuccess || !address)
+            fail(GP_CUDA_ERROR, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(err));
+        g_static_address[device] = static_cast<u64*>(address);
+    }
+    return g_static_address[device];
+}
+}  // namespace
+}  // namespace gp
+
 using namespace gp;
+
+extern "C" gp_status gp_evaluate_device_static(const gp_csr* graph, const int32_t* labels, int32_t k,
+                                               uint64_t* cut_out, uint64_t* loads_out, void* stream) {
+    return guarded_eval([&]() -> gp_status {
+        check_evaluate_args(graph, labels, k, cut_out, loads_out);
+        // Every partial the reduction reads is rewritten by the first pass of
+        // this call, so nothing in the shared array needs clearing first.
+        u64* partial = static_scratch_address();
+        launch_evaluate(graph, labels, k, cut_out, loads_out, partial, static_cast<cudaStream_t>(stream));
+        return GP_OK;
+    });
+}
 
 // Context accessor defined in gp_partition.cu.
 namespace gp { Context& context_of(gp_context* ctx); }

@@ -125,6 +125,26 @@ gp_status gp_evaluate_device(gp_context* ctx, const gp_csr* graph, const int32_t
                              int32_t k, uint64_t* cut_out, uint64_t* loads_out,
                              void* stream);
 
+/* Allocation-free twin of gp_evaluate_device, with no counterpart in the
+ * reference.  For callers that cannot let a library allocate device memory:
+ * a framework whose caching allocator owns the device-memory budget, or a
+ * serving loop that must not call cudaMalloc/cudaFree (which can synchronise
+ * the device) once it is running.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine and needs no context: the per-block partial sums live
+ * in one fixed file-scope device array of 592 x 129 uint64 (611 KB) that every
+ * GPU loading this library holds until the process exits.  k is limited to
+ * 1..128 (the array's capacity); larger k returns GP_INVALID_ARGUMENT.
+ * Runs on the current device and `stream` (NULL: the legacy default stream)
+ * and returns without waiting for the results.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * caches it; make that first call before any stream capture.  All calls on a
+ * device share the one array and it keeps the last call's contents: calls
+ * whose work overlaps on the GPU (different streams, or different host
+ * threads) race on it and must be serialised by the caller. */
+gp_status gp_evaluate_device_static(const gp_csr* graph, const int32_t* labels,
+                                    int32_t k, uint64_t* cut_out,
+                                    uint64_t* loads_out, void* stream);
+
 /* Kernel timing for measurement: between begin and end, every launch of a
  * kernel whose name contains `kernel_substring` is bracketed by CUDA events
  * on the stream it runs on; end returns the launch count and the summed
