@@ -309,11 +309,11 @@ class Context:
         """Time every launch of kernels whose name contains the substring."""
         _check(self._lib.gp_profile_begin(self._handle, kernel_substring.encode()))
 
-    def profile_end(self) -> tuple[int, float]:
-        """(launches, total device milliseconds) since profile_begin."""
-        launches, ms = _C.c_uint64(), _C.c_double()
-        _check(self._lib.gp_profile_end(self._handle, _C.byref(launches), _C.byref(ms)))
-        return launches.value, ms.value
+    def profile_end(self) -> tuple[int, float, float]:
+        """(launches, total device milliseconds, algorithmic bytes) since profile_begin."""
+        launches, ms, nbytes = _C.c_uint64(), _C.c_double(), _C.c_double()
+        _check(self._lib.gp_profile_end(self._handle, _C.byref(launches), _C.byref(ms), _C.byref(nbytes)))
+        return launches.value, ms.value, nbytes.value
 
     def set_option(self, name: str, value: int) -> None:
         _check(self._lib.gp_set_option(self._handle, name.encode(), _C.c_int64(value)))

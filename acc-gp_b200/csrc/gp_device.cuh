@@ -38,10 +38,14 @@ extern thread_local u64 g_launches;
 // Optional per-kernel timing: when a profiler is installed, launches of the
 // kernels whose name contains its pattern are bracketed by CUDA events on
 // their own stream (gp_profile_begin / gp_profile_end).
+// A launch site may also report the algorithmic bytes of the launch it just
+// made (account_bytes); the profiler sums them for the timed launches.
 struct KernelProfiler {
     std::string pattern;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     size_t used = 0;
+    bool last_timed = false;
+    double bytes = 0;
     bool matches(const void* kernel);
     void before(cudaStream_t s);
     void after(cudaStream_t s);
@@ -49,11 +53,16 @@ struct KernelProfiler {
 };
 extern thread_local KernelProfiler* g_profiler;
 
+inline void account_bytes(double bytes) {
+    if (g_profiler && g_profiler->last_timed) g_profiler->bytes += bytes;
+}
+
 template <class... Params, class... Args>
 inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
                    Args&&... args) {
     ++g_launches;
     const bool timed = g_profiler && g_profiler->matches(reinterpret_cast<const void*>(kernel));
+    if (g_profiler) g_profiler->last_timed = timed;
     if (timed) g_profiler->before(stream);
     kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
     if (timed) g_profiler->after(stream);

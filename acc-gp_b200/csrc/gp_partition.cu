@@ -363,11 +363,13 @@ gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring) {
     ctx->profiler.pattern = kernel_substring;
     ctx->profiler.cache.clear();
     ctx->profiler.used = 0;
+    ctx->profiler.bytes = 0;
+    ctx->profiler.last_timed = false;
     g_profiler = &ctx->profiler;
     return GP_OK;
 }
 
-gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms) {
+gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms, double* algorithmic_bytes) {
     if (!ctx) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
     return guarded([&]() -> gp_status {
         g_profiler = nullptr;
@@ -381,7 +383,9 @@ gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms) 
         }
         if (launches) *launches = p.used;
         if (total_ms) *total_ms = ms;
+        if (algorithmic_bytes) *algorithmic_bytes = p.bytes;
         p.used = 0;
+        p.bytes = 0;
         return GP_OK;
     });
 }

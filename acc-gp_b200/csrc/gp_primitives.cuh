@@ -223,56 +223,138 @@ __global__ void k_radix_upsweep(i64 count, const u64* keys, int shift, u32* hist
     for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[static_cast<i64>(d) * gridDim.x + blockIdx.x] = local[d];
 }
 
-template <bool WithValues>
-__global__ void k_radix_downsweep(i64 count, const u64* keys, const u32* vals, int shift, const u32* offsets,
-                                  u64* keys_out, u32* vals_out) {
-    __shared__ u32 warp_count[kSortThreads / 32][kRadix];
-    __shared__ u32 digit_base[kRadix];
+// Shared state of one sort tile: per-warp digit counts (turned into per-warp
+// prefixes), the tile's digit prefix, the global base of each digit for this
+// tile, and the tile's items in digit order.
+struct SortTileSmem {
+    u32 warp_count[kSortThreads / 32][kRadix];
+    u32 local_base[kRadix];
+    u32 digit_base[kRadix];
+    u32 scan[9];
+    u64 keys[kSortTile];
+    u32 vals[kSortTile];
+};
+static_assert(kSortThreads == kRadix, "one digit per thread in the tile prefix");
+
+// Position of every valid item of the tile in the tile's stable digit order:
+// local_base[d] (items of smaller digits) + items of digit d in earlier warps
+// + items of digit d earlier in this warp.  Returns the digit (-1: invalid).
+__device__ __forceinline__ void tile_positions(SortTileSmem& sm, const u64 (&k)[kSortItems], const bool (&valid)[kSortItems],
+                                               int shift, u32 (&pos)[kSortItems], int (&digit)[kSortItems]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int d = lane; d < kRadix; d += 32) warp_count[warp][d] = 0;
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
-        digit_base[d] = offsets[static_cast<i64>(d) * gridDim.x + blockIdx.x];
+    for (int d = lane; d < kRadix; d += 32) sm.warp_count[warp][d] = 0;
     __syncwarp();
-    const i64 base = static_cast<i64>(blockIdx.x) * kSortTile;
-    u64 k[kSortItems];
-    u32 v[kSortItems];
     u32 rank[kSortItems];
-    int digit[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const i64 i = sort_index(base, j);
-        const bool valid = i < count;
-        k[j] = valid ? keys[i] : 0;
-        if (WithValues) v[j] = valid ? vals[i] : 0;
-        digit[j] = valid ? static_cast<int>((k[j] >> shift) & (kRadix - 1)) : -1;
-        const unsigned active = __ballot_sync(0xffffffffu, valid);
-        if (valid) {
+        digit[j] = valid[j] ? static_cast<int>((k[j] >> shift) & (kRadix - 1)) : -1;
+        const unsigned active = __ballot_sync(0xffffffffu, valid[j]);
+        if (valid[j]) {
             const unsigned peers = __match_any_sync(active, digit[j]);
             const unsigned below = peers & ((1u << lane) - 1u);
-            rank[j] = warp_count[warp][digit[j]] + __popc(below);
+            rank[j] = sm.warp_count[warp][digit[j]] + __popc(below);
             __syncwarp(active);
-            if (below == 0) warp_count[warp][digit[j]] += __popc(peers);
+            if (below == 0) sm.warp_count[warp][digit[j]] += __popc(peers);
         }
         __syncwarp();
     }
     __syncthreads();
-    // Exclusive prefix over warps for every digit.
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
-        u32 run = 0;
+    const int d = threadIdx.x;
+    u32 run = 0;
 #pragma unroll
-        for (int w = 0; w < kSortThreads / 32; ++w) {
-            const u32 c = warp_count[w][d];
-            warp_count[w][d] = run;
-            run += c;
-        }
+    for (int w = 0; w < kSortThreads / 32; ++w) {
+        const u32 c = sm.warp_count[w][d];
+        sm.warp_count[w][d] = run;
+        run += c;
     }
+    u32 total;
+    sm.local_base[d] = block_exclusive_scan<u32>(run, total, sm.scan);
     __syncthreads();
 #pragma unroll
+    for (int j = 0; j < kSortItems; ++j)
+        if (valid[j]) pos[j] = sm.local_base[digit[j]] + sm.warp_count[warp][digit[j]] + rank[j];
+}
+
+// One pass of a multi-tile sort.  The tile is ordered by digit in shared
+// memory first, so the scatter writes runs of equal digits to consecutive
+// addresses instead of one isolated element per thread.
+template <bool WithValues>
+__global__ void __launch_bounds__(kSortThreads) k_radix_downsweep(i64 count, const u64* keys, const u32* vals, int shift,
+                                                                  const u32* offsets, u64* keys_out, u32* vals_out) {
+    __shared__ SortTileSmem sm;
+    const i64 base = static_cast<i64>(blockIdx.x) * kSortTile;
+    const int tile_items = static_cast<int>(count - base < kSortTile ? count - base : kSortTile);
+    sm.digit_base[threadIdx.x] = offsets[static_cast<i64>(threadIdx.x) * gridDim.x + blockIdx.x];
+    u64 k[kSortItems];
+    u32 v[kSortItems];
+    bool valid[kSortItems];
+#pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        if (digit[j] < 0) continue;
-        const u32 pos = digit_base[digit[j]] + warp_count[warp][digit[j]] + rank[j];
-        keys_out[pos] = k[j];
-        if (WithValues) vals_out[pos] = v[j];
+        const i64 i = sort_index(base, j);
+        valid[j] = i < count;
+        k[j] = valid[j] ? keys[i] : 0;
+        if (WithValues) v[j] = valid[j] ? vals[i] : 0;
+    }
+    u32 pos[kSortItems];
+    int digit[kSortItems];
+    tile_positions(sm, k, valid, shift, pos, digit);
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        if (!valid[j]) continue;
+        sm.keys[pos[j]] = k[j];
+        if (WithValues) sm.vals[pos[j]] = v[j];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tile_items; i += kSortThreads) {
+        const u64 key = sm.keys[i];
+        const int d = static_cast<int>((key >> shift) & (kRadix - 1));
+        const u32 out = sm.digit_base[d] + static_cast<u32>(i) - sm.local_base[d];
+        keys_out[out] = key;
+        if (WithValues) vals_out[out] = sm.vals[i];
+    }
+}
+
+// Whole sort of at most one tile by one block: every pass reorders the items
+// in shared memory; the result is written back in place.
+template <bool WithValues>
+__global__ void __launch_bounds__(kSortThreads) k_radix_tile_sort(int count, u64* keys, u32* vals, int begin_bit, int end_bit) {
+    __shared__ SortTileSmem sm;
+    u64 k[kSortItems];
+    u32 v[kSortItems];
+    bool valid[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const i64 i = sort_index(0, j);
+        valid[j] = i < count;
+        k[j] = valid[j] ? keys[i] : 0;
+        if (WithValues) v[j] = valid[j] ? vals[i] : 0;
+    }
+    for (int shift = begin_bit; shift < end_bit; shift += kRadixBits) {
+        u32 pos[kSortItems];
+        int digit[kSortItems];
+        tile_positions(sm, k, valid, shift, pos, digit);
+#pragma unroll
+        for (int j = 0; j < kSortItems; ++j) {
+            if (!valid[j]) continue;
+            sm.keys[pos[j]] = k[j];
+            if (WithValues) sm.vals[pos[j]] = v[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSortItems; ++j) {
+            if (!valid[j]) continue;
+            const i64 i = sort_index(0, j);
+            k[j] = sm.keys[i];
+            if (WithValues) v[j] = sm.vals[i];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        if (!valid[j]) continue;
+        const i64 i = sort_index(0, j);
+        keys[i] = k[j];
+        if (WithValues) vals[i] = v[j];
     }
 }
 
@@ -282,6 +364,13 @@ __global__ void k_radix_downsweep(i64 count, const u64* keys, const u32* vals, i
 inline void radix_sort_pairs(Arena& arena, cudaStream_t s, i64 count, u64*& keys, u32*& vals, u64*& keys_alt,
                              u32*& vals_alt, int begin_bit, int end_bit) {
     if (count <= 1 || end_bit <= begin_bit) return;
+    if (count <= kSortTile) {
+        if (vals)
+            launch(k_radix_tile_sort<true>, 1, kSortThreads, 0, s, static_cast<int>(count), keys, vals, begin_bit, end_bit);
+        else
+            launch(k_radix_tile_sort<false>, 1, kSortThreads, 0, s, static_cast<int>(count), keys, vals, begin_bit, end_bit);
+        return;
+    }
     ArenaScope scope(arena);
     const int tiles = blocks_for(count, kSortTile);
     u32* hist = arena.alloc<u32>(static_cast<size_t>(tiles) * kRadix);
@@ -292,6 +381,7 @@ inline void radix_sort_pairs(Arena& arena, cudaStream_t s, i64 count, u64*& keys
             launch(k_radix_downsweep<true>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
         else
             launch(k_radix_downsweep<false>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
+        account_bytes(static_cast<double>(count) * (vals ? 24.0 : 16.0) + static_cast<double>(tiles) * kRadix * 4.0);
         std::swap(keys, keys_alt);
         if (vals) std::swap(vals, vals_alt);
     }

@@ -182,71 +182,111 @@ struct LpParams {
     u64* counters;  // 0 candidates, 1 movers, 2 delta (signed), 3 max load
 };
 
-// incremental_lp_proposal (incremental.cuh:166-198) with the warp layout of
-// incremental_warp_lp_proposals (:229-289): W lanes per vertex scan its k
-// affinities; ties keep the lowest part id.
-template <class C, int W>
-__global__ void k_proposals(LpParams q, const C* A, const C* totals) {
-    const int sub = threadIdx.x & (W - 1);
-    const i64 groups = (static_cast<i64>(gridDim.x) * blockDim.x) / W;
-    const i64 rounds = (q.n + groups - 1) / groups;
-    for (i64 r = 0; r < rounds; ++r) {
-        const i64 v = r * groups + (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
-        const bool valid = v < q.n;
-        // The group leader resets the slot, consumes the lock and decides
-        // whether the row is a boundary row; the group follows its decision.
-        int act = 0, src = 0;
+// 16-byte loads of affinity rows when a row starts on a 16-byte boundary.
+template <class C> struct AffinityVec;
+template <> struct AffinityVec<u32> { using V = uint4; static constexpr int N = 4; };
+template <> struct AffinityVec<u64> { using V = ulonglong2; static constexpr int N = 2; };
+
+// incremental_lp_proposal (incremental.cuh:166-198).  A warp takes 32
+// consecutive vertices: each lane reads its vertex's lock, label, own-part
+// affinity and row total (coalesced), and only boundary rows are scanned, by
+// groups of W lanes, 32/W rows at a time.  Ties keep the lowest part id.
+// Proposers are appended once per warp pass.
+template <class C, int W, bool Vectorized>
+__global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, const C* totals) {
+    using Vec = AffinityVec<C>;
+    constexpr int N = Vectorized ? Vec::N : 1;
+    constexpr int G = 32 / W;
+    __shared__ u64 s_slack[kMaxParts];
+    __shared__ double s_price[kMaxParts];
+    __shared__ unsigned char s_propose[kThreads];
+    const int k = q.k;
+    if (q.prices)
+        for (int p = threadIdx.x; p < k; p += blockDim.x) { s_slack[p] = q.capacity - q.loads[p]; s_price[p] = q.prices[p]; }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < q.n; base += warps * 32) {
+        const i64 v = base + lane;
+        int src = 0;
         u64 current = 0;
-        if (valid && sub == 0) {
-            q.targets[v] = -1;
-            q.gains[v] = LLONG_MIN;
+        bool act = false;
+        if (v < q.n) {
             if (q.locks[v]) {
                 q.locks[v] = 0;
             } else {
                 src = q.labels[v];
-                current = A[v * q.k + src];
+                current = A[v * k + src];
                 act = current != static_cast<u64>(totals[v]);
             }
+            if (!act) {
+                q.targets[v] = -1;
+                q.gains[v] = LLONG_MIN;
+            }
         }
-        const bool active = __shfl_sync(0xffffffffu, act, 0, W) != 0;
-        src = __shfl_sync(0xffffffffu, src, 0, W);
-        current = __shfl_sync(0xffffffffu, current, 0, W);
-        int target = -1;
-        u64 best = 0;
-        double best_score = -DBL_MAX;
-        if (active) {
-            const u64 weight = q.vw[v];
-            for (int p = sub; p < q.k; p += W) {
-                const u64 conn = A[v * q.k + p];
-                if (p == src || !conn) continue;
-                if (q.prices) {
-                    const double score = __dsub_rn(static_cast<double>(conn), repair_cost(p, weight, q.loads, q.capacity, q.prices));
-                    if (target < 0 || score > best_score) { target = p; best = conn; best_score = score; }
-                } else if (target < 0 || conn > best) {
-                    target = p;
-                    best = conn;
+        s_propose[threadIdx.x] = 0;
+        __syncwarp();
+        unsigned pending = __ballot_sync(0xffffffffu, act);
+        while (pending) {
+            unsigned mine = pending;
+            for (int i = 0; i < gid; ++i) mine &= mine - 1;
+            for (int i = 0; i < G; ++i) pending &= pending - 1;
+            const int owner = mine ? __ffs(mine) - 1 : -1;
+            const int osrc = __shfl_sync(0xffffffffu, src, owner < 0 ? 0 : owner);
+            const u64 ocur = __shfl_sync(0xffffffffu, current, owner < 0 ? 0 : owner);
+            const i64 vv = base + owner;
+            int target = -1;
+            u64 best = 0;
+            double best_score = -DBL_MAX;
+            if (owner >= 0) {
+                const C* row = A + vv * k;
+                const u64 weight = q.prices ? q.vw[vv] : 0;
+                for (int p0 = sub * N; p0 < k; p0 += W * N) {
+                    C val[N];
+                    if constexpr (Vectorized) {
+                        const typename Vec::V x = *reinterpret_cast<const typename Vec::V*>(row + p0);
+                        if constexpr (N == 4) { val[0] = x.x; val[1] = x.y; val[2] = x.z; val[3] = x.w; }
+                        else { val[0] = x.x; val[1] = x.y; }
+                    } else {
+                        val[0] = row[p0];
+                    }
+#pragma unroll
+                    for (int e = 0; e < N; ++e) {
+                        const int p = p0 + e;
+                        const u64 conn = val[e];
+                        if (p == osrc || !conn) continue;
+                        if (q.prices) {
+                            const double cost = weight > s_slack[p] ? __dmul_rn(s_price[p], static_cast<double>(weight - s_slack[p])) : 0.0;
+                            const double score = __dsub_rn(static_cast<double>(conn), cost);
+                            if (target < 0 || score > best_score) { target = p; best = conn; best_score = score; }
+                        } else if (target < 0 || conn > best) {
+                            target = p;
+                            best = conn;
+                        }
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int d = W / 2; d; d >>= 1) {
-            const int ot = __shfl_xor_sync(0xffffffffu, target, d, W);
-            const u64 ob = __shfl_xor_sync(0xffffffffu, best, d, W);
-            const double os = __shfl_xor_sync(0xffffffffu, best_score, d, W);
-            if (ot >= 0) {
-                const bool greater = q.prices ? os > best_score : ob > best;
-                const bool equal = q.prices ? os == best_score : ob == best;
-                if (target < 0 || greater || (equal && ot < target)) { target = ot; best = ob; best_score = os; }
+            for (int d = W / 2; d; d >>= 1) {
+                const int ot = __shfl_xor_sync(0xffffffffu, target, d, W);
+                const u64 ob = __shfl_xor_sync(0xffffffffu, best, d, W);
+                const double os = __shfl_xor_sync(0xffffffffu, best_score, d, W);
+                if (ot >= 0) {
+                    const bool greater = q.prices ? os > best_score : ob > best;
+                    const bool equal = q.prices ? os == best_score : ob == best;
+                    if (target < 0 || greater || (equal && ot < target)) { target = ot; best = ob; best_score = os; }
+                }
+            }
+            if (owner >= 0 && sub == 0) {
+                const bool propose = target >= 0 && (best >= ocur || ocur - best < static_cast<u64>(q.filter * static_cast<double>(ocur)));
+                q.targets[vv] = propose ? target : -1;
+                q.gains[vv] = !propose ? LLONG_MIN
+                              : best >= ocur ? static_cast<long long>(best - ocur) : -static_cast<long long>(ocur - best);
+                s_propose[(threadIdx.x & ~31) + owner] = propose;
             }
         }
-        bool propose = false;
-        if (active && sub == 0 && target >= 0 &&
-            (best >= current || current - best < static_cast<u64>(q.filter * static_cast<double>(current)))) {
-            q.targets[v] = target;
-            q.gains[v] = best >= current ? static_cast<long long>(best - current) : -static_cast<long long>(current - best);
-            propose = true;
-        }
-        append(static_cast<int>(v), propose, q.cand, q.counters + 0);
+        __syncwarp();
+        append(static_cast<int>(v), s_propose[threadIdx.x] != 0, q.cand, q.counters + 0);
     }
 }
 
@@ -1166,6 +1206,26 @@ private:
         launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
         launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     }
+    // Group width: about four 16-byte loads (or four scalars) per lane.
+    void proposals(const LpParams& q) {
+        const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
+        const int per_lane = vec ? 4 * AffinityVec<T>::N : 4;
+        const int W = k <= 2 * per_lane ? 2 : k <= 4 * per_lane ? 4 : k <= 8 * per_lane ? 8 : 16;
+        const int grid = grid_for(n, kThreads);
+        const T* a = A;
+        const T* t = totals;
+        if (vec) {
+            if (W == 2) launch(k_proposals<T, 2, true>, grid, kThreads, 0, s(), q, a, t);
+            else if (W == 4) launch(k_proposals<T, 4, true>, grid, kThreads, 0, s(), q, a, t);
+            else if (W == 8) launch(k_proposals<T, 8, true>, grid, kThreads, 0, s(), q, a, t);
+            else launch(k_proposals<T, 16, true>, grid, kThreads, 0, s(), q, a, t);
+        } else {
+            if (W == 2) launch(k_proposals<T, 2, false>, grid, kThreads, 0, s(), q, a, t);
+            else if (W == 4) launch(k_proposals<T, 4, false>, grid, kThreads, 0, s(), q, a, t);
+            else if (W == 8) launch(k_proposals<T, 8, false>, grid, kThreads, 0, s(), q, a, t);
+            else launch(k_proposals<T, 16, false>, grid, kThreads, 0, s(), q, a, t);
+        }
+    }
     void account(long long delta) {
         if (delta >= 0) {
             if (static_cast<u64>(delta) > cut) fail(GP_INTERNAL, "incremental cut underflow");
@@ -1181,11 +1241,7 @@ template <class T>
 i64 LevelRefiner<T>::lp_round(double filter) {
     GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
     LpParams q{n, k, C, filter, g.off, g.nbr, g.ew, g.vw, labels, loads, prices, targets, gains, locks, flags, cand, movers, counters};
-    const int W = k <= 8 ? 8 : k <= 16 ? 16 : 32;
-    const int grid = grid_for(n * W, kThreads);
-    if (W == 8) launch(k_proposals<T, 8>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
-    else if (W == 16) launch(k_proposals<T, 16>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
-    else launch(k_proposals<T, 32>, grid, kThreads, 0, s(), q, static_cast<const T*>(A), static_cast<const T*>(totals));
+    proposals(q);
     launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
     if (g.chunks) {
         GP_CUDA(cudaMemsetAsync(corr_acc, 0, sizeof(long long) * g.heavy_count, s()));

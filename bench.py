@@ -35,8 +35,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 WORKLOAD = dict(workload="rmat22_k64", graph="R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, seed 0",
                 k=64, epsilon=1.03, seed=0, vertices=4194304)
 METRIC = "partition ms & batched graphs/s at k=64 ε=1.03; cut vs ref; HBM GB/s"
-# Kernel whose roofline fraction is reported.
-DOMINANT_KERNEL = "k_update"
+# Kernel whose roofline fraction is reported: the largest share of device
+# time in the ncu launch list of this workload (profiles/).  Its launch site
+# reports the algorithmic bytes of every launch (keys and values read once
+# and written once per pass, plus the tile histogram).
+DOMINANT_KERNEL = "k_radix_downsweep"
+# ncu DRAM bytes (read + write) per algorithmic byte of that kernel, from the
+# capture summarised in this file ("traffic_per_algorithmic_byte: x").
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_radix_downsweep_rmat.md")
 
 
 def load_package():
@@ -173,7 +179,7 @@ def run_ours(args):
         launches += st.kernel_launches
     end.record(stream)
     torch.cuda.synchronize()
-    dom_launches, dom_ms = ctx.profile_end()
+    dom_launches, dom_ms, dom_bytes = ctx.profile_end()
     if dist:
         dist.barrier()
     elapsed = start.elapsed_time(end) / 1000.0
@@ -203,16 +209,17 @@ def run_ours(args):
         e2e_elapsed = float(t.item())
     e2e_value = world * len(e2e_times) / e2e_elapsed
     # Roofline of the dominant kernel: algorithmic bytes per launch / duration.
-    per_launch_ms = dom_ms / max(1, dom_launches)
-    dom_bytes = stats[-1].dominant_bytes if hasattr(stats[-1], "dominant_bytes") else None
     peak, peak_kind = measured_peak_hbm()
     roof = None
-    if dom_launches:
-        alg = dominant_bytes_per_launch(stats, dom_launches, args.steps)
-        achieved = alg / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    if dom_launches and dom_ms > 0:
+        per_launch_ms = dom_ms / dom_launches
+        alg = dom_bytes / dom_launches
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9
+        ratio = traffic_ratio()
         roof = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
-                "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                "launches": dom_launches, "avg_launch_ms": per_launch_ms,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": alg * ratio if ratio else None,
+                "algorithmic_bytes_per_launch": alg, "launches": dom_launches, "avg_launch_ms": per_launch_ms,
                 "share_of_step": dom_ms / (elapsed * 1e3 / world) if elapsed > 0 else None}
     vcycle_bytes = stats[-1].algorithmic_bytes
     line = {
@@ -240,15 +247,18 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def dominant_bytes_per_launch(stats, launches, steps):
-    """Algorithmic bytes of one k_update launch: every mover's row is read
-    (4 B neighbour + label, flag and target gathers of the neighbour, 16 B
-    per entry) and two 4-byte cache counters change per entry (8 B read +
-    8 B write).  The library reports the entries its update launches touched."""
-    total = sum(getattr(s, "update_entries", 0) for s in stats)
-    if not total:
-        return 0.0
-    return 32.0 * total / launches
+def traffic_ratio():
+    """DRAM bytes per algorithmic byte of the dominant kernel, as measured by
+    ncu on the capture described in TRAFFIC_PROFILE (None if absent)."""
+    try:
+        with open(TRAFFIC_PROFILE) as f:
+            for line in f:
+                m = re.search(r"traffic_per_algorithmic_byte:\s*([0-9.]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args):
@@ -298,7 +308,7 @@ def run_reference(args):
 def launch_list(args):
     import torch
     gp = load_package()
-    g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
+    g = gp.rmat(args.scale, 16, 0.57, 0.19, 0.19, 0)
     dev = torch.device("cuda", 0)
     off_d = torch.from_numpy(g.offsets).to(dev)
     nbr_d = torch.from_numpy(g.neighbors).to(dev)
@@ -322,6 +332,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
+    ap.add_argument("--scale", type=int, default=22,
+                    help="R-MAT scale of the --launch-list graph (smaller cases for ncu captures)")
     args = ap.parse_args()
     if args.launch_list:
         launch_list(args)

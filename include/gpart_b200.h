@@ -147,10 +147,13 @@ gp_status gp_evaluate_device_static(const gp_csr* graph, const int32_t* labels,
 
 /* Kernel timing for measurement: between begin and end, every launch of a
  * kernel whose name contains `kernel_substring` is bracketed by CUDA events
- * on the stream it runs on; end returns the launch count and the summed
- * device time in milliseconds.  Profiling is per host thread. */
+ * on the stream it runs on; end returns the launch count, the summed device
+ * time in milliseconds and the summed algorithmic bytes of those launches
+ * (compulsory HBM traffic, reported by the kernels that model it; 0 for the
+ * others).  Profiling is per host thread. */
 gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring);
-gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms);
+gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms,
+                         double* algorithmic_bytes);
 
 /* Hierarchy of the last call made with GP_FLAG_KEEP_HIERARCHY.  Level 0 is
  * the input.  gp_level_copy fills any non-NULL array; `map` (length n of the
