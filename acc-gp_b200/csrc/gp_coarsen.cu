@@ -37,50 +37,48 @@ constexpr int kMediumWarps = 4;
 // 2 zero weight, 3 non-unit weight, 4 max raw degree, 5 total vertex
 // weight, 6 max vertex weight.
 template <int W>
-__global__ void k_level0_meta(i64 n, const int* off, const int* nbr, const u32* ew, const u32* vw, u64* bounds,
-                              u64* sc) {
-    __shared__ u64 s_max, s_raw, s_total, s_vmax;
-    __shared__ u32 s_flags;
-    if (threadIdx.x == 0) { s_max = s_raw = s_total = s_vmax = 0; s_flags = 0; }
-    __syncthreads();
-    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+__global__ void __launch_bounds__(256) k_level0_meta(i64 n, const int* off, const int* nbr, const u32* ew,
+                                                     const u32* vw, u64* bounds, u64* sc) {
     const int lane = threadIdx.x & (W - 1);
-    const bool valid = v < n;
-    u64 d = 0;
+    constexpr int kGroups = 32 / W;  // rows per warp and pass
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    u64 d_max = 0, raw_max = 0, total = 0, v_max = 0;
     u32 flags = 0;
-    const i64 begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
-    const bool heavy = end - begin > kHeavyRow;  // summed by k_level0_meta_chunks
-    for (i64 e = begin + lane; !heavy && e < end; e += W) {
-        const u64 w = edge_w(ew, e);
-        d = ~0ULL - d < w ? ~0ULL : d + w;
-        if (e > begin && nbr[e] <= nbr[e - 1]) flags |= 1u;
-        if (!w) flags |= 2u;
-        if (w != 1) flags |= 4u;
-    }
+    // Warp-uniform pass count, so the group shuffles see the whole warp.
+    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kGroups; base < n;
+         base += warps * kGroups) {
+        const i64 v = base + (threadIdx.x & 31) / W;
+        const bool valid = v < n;
+        const i64 begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
+        const bool heavy = end - begin > kHeavyRow;  // summed by k_level0_meta_chunks
+        u64 d = 0;
+        for (i64 e = begin + lane; !heavy && e < end; e += W) {
+            const u64 w = edge_w(ew, e);
+            d = ~0ULL - d < w ? ~0ULL : d + w;
+            if (e > begin && nbr[e] <= nbr[e - 1]) flags |= 1u;
+            if (!w) flags |= 2u;
+            if (w != 1) flags |= 4u;
+        }
 #pragma unroll
-    for (int s = W / 2; s; s >>= 1) {
-        const u64 o = __shfl_xor_sync(0xffffffffu, d, s, W);
-        d = ~0ULL - d < o ? ~0ULL : d + o;
-        flags |= __shfl_xor_sync(0xffffffffu, flags, s, W);
+        for (int s = W / 2; s; s >>= 1) {
+            const u64 o = __shfl_xor_sync(0xffffffffu, d, s, W);
+            d = ~0ULL - d < o ? ~0ULL : d + o;
+        }
+        if (valid && lane == 0) {
+            bounds[v] = d;
+            d_max = d > d_max ? d : d_max;
+            raw_max = static_cast<u64>(end - begin) > raw_max ? static_cast<u64>(end - begin) : raw_max;
+            total += vw[v];
+            v_max = vw[v] > v_max ? vw[v] : v_max;
+        }
     }
-    if (valid && lane == 0) {
-        bounds[v] = d;
-        atomicMax(&s_max, d);
-        atomicMax(&s_raw, static_cast<u64>(end - begin));
-        atomicAdd(&s_total, static_cast<u64>(vw[v]));
-        atomicMax(&s_vmax, static_cast<u64>(vw[v]));
-        if (flags) atomicOr(&s_flags, flags);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        atomicMax(sc + 0, s_max);
-        if (s_flags & 1u) atomicOr(sc + 1, 1ULL);
-        if (s_flags & 2u) atomicOr(sc + 2, 1ULL);
-        if (s_flags & 4u) atomicOr(sc + 3, 1ULL);
-        atomicMax(sc + 4, s_raw);
-        atomicAdd(sc + 5, s_total);
-        atomicMax(sc + 6, s_vmax);
-    }
+    block_atomic_max(sc + 0, d_max);
+    if (__syncthreads_or(flags & 1u) && threadIdx.x == 0) atomicOr(sc + 1, 1ULL);
+    if (__syncthreads_or(flags & 2u) && threadIdx.x == 0) atomicOr(sc + 2, 1ULL);
+    if (__syncthreads_or(flags & 4u) && threadIdx.x == 0) atomicOr(sc + 3, 1ULL);
+    block_atomic_max(sc + 4, raw_max);
+    block_atomic_add(sc + 5, total);
+    block_atomic_max(sc + 6, v_max);
 }
 
 // Heavy rows of record_bound_kernel, one block per chunk.
@@ -123,27 +121,27 @@ __global__ void k_weight_sum(i64 m, const u32* ew, u64* out) {
 // max degree, heavy flag and class lists.  Scalars: 0 max degree, 1 heavy,
 // 2..5 list sizes (low, medium, large, heavy), 6 heavy hash slots,
 // 7 isolated vertices.
-__global__ void k_degree_classes(i64 n, const int* off, int* low, int* medium, int* large, int* heavy, u64* sc) {
-    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    const bool valid = v < n;
-    const i64 deg = valid ? off[v + 1] - off[v] : 0;
-    const u32 dmax = __reduce_max_sync(0xffffffffu, static_cast<u32>(deg));
-    if (lane == 0 && dmax) atomicMax(sc + 0, static_cast<u64>(dmax));
-    if (__any_sync(0xffffffffu, valid && deg >= 4096) && lane == 0) atomicOr(sc + 1, 1ULL);
-    const int cls = !valid ? -1 : deg <= kLowDegree ? 0 : deg <= kMediumDegree ? 1 : deg <= kLargeDegree ? 2 : 3;
-    int* lists[4] = {low, medium, large, heavy};
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const unsigned mask = __ballot_sync(0xffffffffu, cls == c);
-        if (!mask) continue;
-        u64 base = 0;
-        if (lane == 0) base = atomicAdd(sc + 2 + c, static_cast<u64>(__popc(mask)));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (cls == c) lists[c][base + __popc(mask & ((1u << lane) - 1u))] = static_cast<int>(v);
+__global__ void __launch_bounds__(256) k_degree_classes(i64 n, const int* off, int* low, int* medium, int* large,
+                                                        int* heavy, u64* sc) {
+    u64 d_max = 0, isolated = 0;
+    int big = 0;
+    // Block-uniform passes: the appends synchronise the block.
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < n; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 v = base + threadIdx.x;
+        const bool valid = v < n;
+        const i64 deg = valid ? off[v + 1] - off[v] : 0;
+        d_max = static_cast<u64>(deg) > d_max ? static_cast<u64>(deg) : d_max;
+        big |= valid && deg >= 4096;
+        isolated += valid && deg == 0;
+        const int cls = !valid ? -1 : deg <= kLowDegree ? 0 : deg <= kMediumDegree ? 1 : deg <= kLargeDegree ? 2 : 3;
+        block_append(static_cast<int>(v), cls == 0, low, sc + 2);
+        block_append(static_cast<int>(v), cls == 1, medium, sc + 3);
+        block_append(static_cast<int>(v), cls == 2, large, sc + 4);
+        block_append(static_cast<int>(v), cls == 3, heavy, sc + 5);
     }
-    const unsigned iso = __ballot_sync(0xffffffffu, valid && deg == 0);
-    if (iso && lane == 0) atomicAdd(sc + 7, static_cast<u64>(__popc(iso)));
+    block_atomic_max(sc + 0, d_max);
+    if (__syncthreads_or(big) && threadIdx.x == 0) atomicOr(sc + 1, 1ULL);
+    block_atomic_add(sc + 7, isolated);
 }
 
 __host__ __device__ inline u64 heavy_slots(i64 deg) {
@@ -208,8 +206,7 @@ __global__ void k_cluster_weights(i64 n, const int* clusters, const u32* vw, u64
 
 __global__ void k_count_nonzero(i64 n, const u64* values, u64* out) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const unsigned b = __ballot_sync(0xffffffffu, i < n && values[i] != 0);
-    if ((threadIdx.x & 31) == 0 && b) atomicAdd(out, static_cast<u64>(__popc(b)));
+    block_atomic_add(out, i < n && values[i] != 0 ? 1ULL : 0ULL);
 }
 
 // ---------------------------------------------------------------- rounds
@@ -682,8 +679,7 @@ __global__ void k_iota_clusters(i64 n, const u32* vw, int* clusters, u64* cw) {
 }
 __global__ void k_count_isolated(i64 n, const int* off, u64* out) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const unsigned b = __ballot_sync(0xffffffffu, v < n && off[v] == off[v + 1]);
-    if ((threadIdx.x & 31) == 0 && b) atomicAdd(out, static_cast<u64>(__popc(b)));
+    block_atomic_add(out, v < n && off[v] == off[v + 1] ? 1ULL : 0ULL);
 }
 __global__ void k_map(i64 n, const int* clusters, const int* ids, const u32* vw, int* map, u32* cvw) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -694,9 +690,7 @@ __global__ void k_map(i64 n, const int* clusters, const int* ids, const u32* vw,
 }
 __global__ void k_max_u32(i64 n, const u32* values, u64* out) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const u32 v = i < n ? values[i] : 0u;
-    const u32 m = __reduce_max_sync(0xffffffffu, v);
-    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, static_cast<u64>(m));
+    block_atomic_max(out, i < n ? static_cast<u64>(values[i]) : 0ULL);
 }
 
 // ---------------------------------------------------------------- contraction
@@ -721,9 +715,8 @@ __global__ void k_contract_bounds(i64 n, const int* map, const int* off, const u
 }
 __global__ void k_max_pair(i64 n, const u64* a, const int* b, u64* out) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const u64 x = i < n ? a[i] : 0, y = i < n ? static_cast<u64>(b[i]) : 0;
-    const u64 mx = warp_max(x), my = warp_max(y);
-    if ((threadIdx.x & 31) == 0) { if (mx) atomicMax(out, mx); if (my) atomicMax(out + 1, my); }
+    block_atomic_max(out, i < n ? a[i] : 0ULL);
+    block_atomic_max(out + 1, i < n ? static_cast<u64>(b[i]) : 0ULL);
 }
 
 struct LoadInt {
@@ -768,19 +761,11 @@ __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int*
 // Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 larger.
 __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u64* sc) {
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
     const int r = c < nc ? raw[c] : 0;
     const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kBlockSortRow ? 2 : 3;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const unsigned mask = __ballot_sync(0xffffffffu, cls == k);
-        if (!mask) continue;
-        u64 base = 0;
-        if (lane == 0) base = atomicAdd(sc + k, static_cast<u64>(__popc(mask)));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (cls == k) lists[k * stride + base + __popc(mask & ((1u << lane) - 1u))] = static_cast<int>(c);
-    }
-    if (cls == 3) atomicAdd(sc + 4, static_cast<u64>(r));
+    for (int k = 0; k < 4; ++k) block_append(static_cast<int>(c), cls == k, lists + k * stride, sc + k);
+    block_atomic_add(sc + 4, cls == 3 ? static_cast<u64>(r) : 0ULL);
 }
 
 // contraction_warp_sort / contraction_sort_row (contraction_rows.cuh:40-116):
@@ -872,55 +857,61 @@ __global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off,
     if (lane == 0) ucount[c] = out;
 }
 
-// Rows of 513..4096 raw entries: bitonic sort in shared memory, then one
-// thread per run of equal keys sums it.
+// Rows of 513..4096 raw entries: stable LSD radix sort by target in shared
+// memory (8-bit digits over the bits of nc; dropped intra-cluster entries
+// take the key nc and sort last), then one thread per run of equal keys sums
+// it and writes the unique run back at the row's start.
 __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
-                                                         int* ucount) {
+                                                         int* ucount, int nc, int bits) {
+    constexpr int kItems = kBlockSortRow / 256;
     __shared__ int keys[kBlockSortRow];
     __shared__ u32 vals[kBlockSortRow];
-    __shared__ unsigned char heads[kBlockSortRow];
+    __shared__ u32 warp_count[8][kRadix];
+    __shared__ u32 local_base[kRadix];
+    __shared__ u32 scan_u[9];
     __shared__ int scan_smem[9];
     const int c = rows[blockIdx.x];
     const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
-    int size = 1;
-    while (size < degree) size <<= 1;
-    for (int i = threadIdx.x; i < size; i += blockDim.x) {
-        keys[i] = i < degree ? raw_t[begin + i] : INT_MAX;
-        vals[i] = i < degree ? raw_w[begin + i] : 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int k[kItems];
+    u32 v[kItems];
+    bool valid[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int i = warp * (32 * kItems) + j * 32 + lane;
+        valid[j] = i < degree;
+        const int t = valid[j] ? raw_t[begin + i] : 0;
+        k[j] = t == INT_MAX ? nc : t;
+        v[j] = valid[j] ? raw_w[begin + i] : 0u;
     }
-    __syncthreads();
-    for (int k = 2; k <= size; k <<= 1)
-        for (int j = k >> 1; j; j >>= 1) {
-            for (int i = threadIdx.x; i < size; i += blockDim.x) {
-                const int x = i ^ j;
-                if (x > i) {
-                    const bool up = (i & k) == 0;
-                    if ((keys[i] > keys[x]) == up) {
-                        const int tk = keys[i]; keys[i] = keys[x]; keys[x] = tk;
-                        const u32 tv = vals[i]; vals[i] = vals[x]; vals[x] = tv;
-                    }
-                }
-            }
-            __syncthreads();
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        u32 pos[kItems];
+        rank_tile<kItems, int>(warp_count, local_base, scan_u, k, valid, shift, pos);
+#pragma unroll
+        for (int j = 0; j < kItems; ++j)
+            if (valid[j]) { keys[pos[j]] = k[j]; vals[pos[j]] = v[j]; }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const int i = warp * (32 * kItems) + j * 32 + lane;
+            if (valid[j]) { k[j] = keys[i]; v[j] = vals[i]; }
         }
-    // Head flags and their exclusive scan (16 items per thread).
-    const int per = (size + blockDim.x - 1) / blockDim.x;
+        __syncthreads();
+    }
+    // keys/vals hold the sorted row; heads of runs and their exclusive scan.
+    const int per = (degree + blockDim.x - 1) / blockDim.x;
     int local = 0;
     for (int q = 0; q < per; ++q) {
         const int i = threadIdx.x * per + q;
-        if (i < size) {
-            const bool h = keys[i] != INT_MAX && (i == 0 || keys[i] != keys[i - 1]);
-            heads[i] = h;
-            local += h;
-        }
+        if (i < degree) local += keys[i] != nc && (i == 0 || keys[i] != keys[i - 1]);
     }
     int total;
     int run = block_exclusive_scan<int>(local, total, scan_smem);
     for (int q = 0; q < per; ++q) {
         const int i = threadIdx.x * per + q;
-        if (i < size && heads[i]) {
+        if (i < degree && keys[i] != nc && (i == 0 || keys[i] != keys[i - 1])) {
             u64 sum = 0;
-            for (int j = i; j < size && keys[j] == keys[i]; ++j) sum += vals[j];
+            for (int j = i; j < degree && keys[j] == keys[i]; ++j) sum += vals[j];
             raw_t[begin + run] = keys[i];
             raw_w[begin + run] = static_cast<u32>(sum);
             ++run;
@@ -1019,9 +1010,8 @@ __global__ void k_heavy_counts(i64 n, const int* off, u64* sc) {
         const int d = off[v + 1] - off[v];
         if (d > kHeavyRow) { rows = 1; chunks = (d + kChunk - 1) / kChunk; }
     }
-    rows = warp_sum(rows);
-    chunks = warp_sum(chunks);
-    if ((threadIdx.x & 31) == 0 && rows) { atomicAdd(sc, rows); atomicAdd(sc + 1, chunks); }
+    block_atomic_add(sc, rows);
+    block_atomic_add(sc + 1, chunks);
 }
 struct IsHeavyRow {
     const int* off;
@@ -1222,7 +1212,8 @@ AggregateOut Aggregator::run() {
             int* storage = A.alloc<int>(static_cast<size_t>(n) * 4);
             for (int c = 0; c < 4; ++c) lists[c] = storage + static_cast<size_t>(n) * c;
             ctx.clear_scalars(8);
-            launch(k_degree_classes, vb, kThreads, 0, s, n, g.off, lists[0], lists[1], lists[2], lists[3], ctx.dev_scalars);
+            launch(k_degree_classes, static_cast<int>(std::min<i64>(vb, 148 * 8)), kThreads, 0, s, n, g.off, lists[0],
+                   lists[1], lists[2], lists[3], ctx.dev_scalars);
             const u64* sc = ctx.read_scalars(8);
             out.stats_max_degree = sc[0];
             out.stats_heavy = sc[1] != 0;
@@ -1415,7 +1406,7 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
             count[1], lists + nc, raw_off, raw_t, raw_w, ucount);
     if (count[2])
         launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
-                                                                            ucount);
+               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[3]) {
         ArenaScope ls(A);
         const int* large = lists + 3 * nc;
@@ -1507,12 +1498,13 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
         build_chunks(ctx, current);
         ws.row_bounds = ctx.persist.alloc<u64>(current.n);
         ctx.clear_scalars(7);
+        const int meta_grid = static_cast<int>(std::min<i64>(blocks_for(current.n * 8, kThreads), 148 * 16));
         if (current.m / current.n < 8)
-            launch(k_level0_meta<8>, blocks_for(current.n * 8, kThreads), kThreads, 0, s, 
-                current.n, current.off, current.nbr, current.ew, current.vw, ws.row_bounds, ctx.dev_scalars);
+            launch(k_level0_meta<8>, meta_grid, kThreads, 0, s, current.n, current.off, current.nbr, current.ew,
+                   current.vw, ws.row_bounds, ctx.dev_scalars);
         else
-            launch(k_level0_meta<32>, blocks_for(current.n * 32, kThreads), kThreads, 0, s, 
-                current.n, current.off, current.nbr, current.ew, current.vw, ws.row_bounds, ctx.dev_scalars);
+            launch(k_level0_meta<32>, meta_grid, kThreads, 0, s, current.n, current.off, current.nbr, current.ew,
+                   current.vw, ws.row_bounds, ctx.dev_scalars);
         if (current.chunks) {
             // The row pass wrote 0 for heavy rows; their chunks add the sums.
             launch(k_level0_meta_chunks, static_cast<int>(current.chunks), 256, 0, s, current, ws.row_bounds,

@@ -162,4 +162,72 @@ __device__ __forceinline__ T warp_max(T v) {
 
 __device__ __forceinline__ u32 edge_w(const u32* w, i64 e) { return w ? w[e] : 1u; }
 
+// Block-wide reductions into one global atomic per block.  Every thread of
+// the block must call them (they synchronise the block); many blocks
+// updating one address would otherwise serialise on it, one atomic per warp.
+template <class T>
+__device__ __forceinline__ T block_sum(T v) {
+    __shared__ T part[32];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T s = 0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : T(0);
+        s = warp_sum(s);
+    }
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+template <class T>
+__device__ __forceinline__ T block_max(T v) {
+    __shared__ T part[32];
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T s = 0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : T(0);
+        s = warp_max(s);
+    }
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+__device__ __forceinline__ void block_atomic_add(unsigned long long* out, unsigned long long v) {
+    v = block_sum(v);
+    if (threadIdx.x == 0 && v) atomicAdd(out, v);
+}
+__device__ __forceinline__ void block_atomic_add(long long* out, long long v) {
+    v = block_sum(v);
+    if (threadIdx.x == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(out), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ void block_atomic_max(unsigned long long* out, unsigned long long v) {
+    v = block_max(v);
+    if (threadIdx.x == 0 && v) atomicMax(out, v);
+}
+
+// Block-aggregated append: every `active` thread writes v to its own slot of
+// queue; one atomic on *count per block.  All threads of the block call it.
+template <class V>
+__device__ __forceinline__ void block_append(V v, bool active, V* queue, unsigned long long* count) {
+    __shared__ u32 warp_base[32];
+    __shared__ unsigned long long base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned mask = __ballot_sync(0xffffffffu, active);
+    if (lane == 0) warp_base[warp] = __popc(mask);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u32 total = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            const u32 c = warp_base[w];
+            warp_base[w] = total;
+            total += c;
+        }
+        base = total ? atomicAdd(count, static_cast<unsigned long long>(total)) : 0ULL;
+    }
+    __syncthreads();
+    if (active) queue[base + warp_base[warp] + __popc(mask & ((1u << lane) - 1u))] = v;
+    __syncthreads();
+}
+
 }  // namespace gp

@@ -275,6 +275,48 @@ __device__ __forceinline__ void tile_positions(SortTileSmem& sm, const u64 (&k)[
         if (valid[j]) pos[j] = sm.local_base[digit[j]] + sm.warp_count[warp][digit[j]] + rank[j];
 }
 
+// The same ranking for a tile of Items items per thread held in registers in
+// the warp-striped layout (item j of lane l of warp w is tile index
+// w*32*Items + j*32 + l), keys of any integer type.  warp_count is
+// [blockDim/32][kRadix], local_base [kRadix]; blockDim.x must be kRadix.
+template <int Items, class K>
+__device__ __forceinline__ void rank_tile(u32 (*warp_count)[kRadix], u32* local_base, u32* scan, const K (&k)[Items],
+                                          const bool (&valid)[Items], int shift, u32 (&pos)[Items]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = lane; d < kRadix; d += 32) warp_count[warp][d] = 0;
+    __syncwarp();
+    u32 rank[Items];
+#pragma unroll
+    for (int j = 0; j < Items; ++j) {
+        const int digit = static_cast<int>((static_cast<u64>(k[j]) >> shift) & (kRadix - 1));
+        const unsigned active = __ballot_sync(0xffffffffu, valid[j]);
+        if (valid[j]) {
+            const unsigned peers = __match_any_sync(active, digit);
+            const unsigned below = peers & ((1u << lane) - 1u);
+            rank[j] = warp_count[warp][digit] + __popc(below);
+            __syncwarp(active);
+            if (below == 0) warp_count[warp][digit] += __popc(peers);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    const int d = threadIdx.x;
+    u32 run = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+        const u32 c = warp_count[w][d];
+        warp_count[w][d] = run;
+        run += c;
+    }
+    u32 total;
+    local_base[d] = block_exclusive_scan<u32>(run, total, scan);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < Items; ++j) {
+        const int digit = static_cast<int>((static_cast<u64>(k[j]) >> shift) & (kRadix - 1));
+        if (valid[j]) pos[j] = local_base[digit] + warp_count[warp][digit] + rank[j];
+    }
+}
+
 // One pass of a multi-tile sort.  The tile is ordered by digit in shared
 // memory first, so the scatter writes runs of equal digits to consecutive
 // addresses instead of one isolated element per thread.

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <climits>
+#include <type_traits>
 #include <cstdio>
 
 namespace gp {
@@ -32,8 +33,7 @@ __global__ void k_cut_chunks(DGraph g, const int* labels, u64* out) {
     u64 local = 0;
     for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x)
         if (labels[g.nbr[e]] != p) local += edge_w(g.ew, e);
-    local = warp_sum(local);
-    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+    block_atomic_add(out, local);
 }
 __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, u64* out) {
     const int lane = threadIdx.x & 31;
@@ -45,8 +45,7 @@ __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, cons
         for (int e = off[v] + lane; e < off[v + 1]; e += 32)
             if (labels[nbr[e]] != p) local += edge_w(ew, e);
     }
-    local = warp_sum(local);
-    if (lane == 0 && local) atomicAdd(out, local);
+    block_atomic_add(out, local);
 }
 
 __global__ void k_project(i64 n, const int* map, const int* coarse, int* fine) {
@@ -76,8 +75,7 @@ __global__ void k_max_edge(i64 m, const u32* ew, u64* out) {
     u32 mx = 0;
     for (i64 e = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += static_cast<i64>(gridDim.x) * blockDim.x)
         mx = max(mx, ew[e]);
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, static_cast<u64>(mx));
+    block_atomic_max(out, static_cast<u64>(mx));
 }
 
 // publish_repair_prices (incremental.cuh:161-164).
@@ -85,16 +83,6 @@ __global__ void k_prices(int k, const Sample* samples, double* prices) {
     for (int p = threadIdx.x; p < k; p += blockDim.x)
         if (samples[p].weight)
             prices[p] = samples[p].loss > 0 ? static_cast<double>(samples[p].loss) / static_cast<double>(samples[p].weight) : 0.0;
-}
-
-// Warp-aggregated append of `v` when `active` (append_warp, incremental.cuh:201-208).
-__device__ __forceinline__ void append(int v, bool active, int* queue, u64* count) {
-    const int lane = threadIdx.x & 31;
-    const unsigned mask = __ballot_sync(0xffffffffu, active);
-    u64 base = 0;
-    if (lane == 0 && mask) base = atomicAdd(count, static_cast<u64>(__popc(mask)));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (active) queue[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
 
 // estimated_repair_cost (incremental.cuh:156-160).  Products and sums use
@@ -106,40 +94,101 @@ __device__ __forceinline__ double repair_cost(int part, u64 weight, const u64* l
 
 // ---------------------------------------------------------------- affinity cache
 
-// incremental_build_affinity (incremental.cuh:61-140), dense layout: one warp
-// per row accumulates a k-wide histogram in shared memory.
-template <class C>
-__global__ void k_build(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, int k, C* A,
-                        C* totals) {
-    extern __shared__ unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    C* row = reinterpret_cast<C*>(smem_raw) + warp * k;
-    for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
-         v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
-        for (int p = lane; p < k; p += 32) row[p] = 0;
+// 16-byte loads of affinity rows when a row starts on a 16-byte boundary.
+template <class C> struct AffinityVec;
+template <> struct AffinityVec<u32> { using V = uint4; static constexpr int N = 4; };
+template <> struct AffinityVec<u64> { using V = ulonglong2; static constexpr int N = 2; };
+
+// incremental_build_affinity (incremental.cuh:61-140), dense layout.  A warp
+// builds 32/W rows at a time, W lanes per row, each row's k-wide histogram in
+// shared memory; rows longer than kBuildShort entries are accumulated by the
+// whole warp afterwards.  Heavy rows are written as zeros (k_build_chunks
+// adds their sums).  Optionally sums the directed cut of the light rows,
+// total - own-part affinity per row.
+constexpr int kBuildShort = 64;
+template <class C, int W, bool Vectorized>
+__global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const int* nbr, const u32* ew,
+                                                    const int* labels, int k, C* A, C* totals, u64* directed_cut,
+                                                    const u64* gate, u64 threshold) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (gate && *gate <= threshold) return;  // incremental update chosen
+    constexpr int N = Vectorized ? AffinityVec<C>::N : 1;
+    constexpr int G = 32 / W;
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
+    C* warp_hist = reinterpret_cast<C*>(smem_raw) + static_cast<size_t>(threadIdx.x >> 5) * G * k;
+    C* hist = warp_hist + gid * k;
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    unsigned leaders = 0;
+    for (int g = 0; g < G; ++g) leaders |= 1u << (g * W);
+    u64 cut = 0;
+    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; base < n; base += warps * G) {
+        const i64 v = base + gid;
+        const bool valid = v < n;
+        const int begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
+        const int deg = end - begin;
+        for (int p = sub; p < k; p += W) hist[p] = 0;
         __syncwarp();
-        if (off[v + 1] - off[v] <= kHeavyRow) {  // heavy rows: zeros here, k_build_chunks adds
-            for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+        if (deg <= kBuildShort) {
+            for (int e = begin + sub; e < end; e += W) {
                 const int u = nbr[e];
-                if (u != v) atomicAdd(row + labels[u], static_cast<C>(edge_w(ew, e)));
+                if (u != v) atomicAdd(hist + labels[u], static_cast<C>(edge_w(ew, e)));
+            }
+        }
+        for (unsigned rest = __ballot_sync(0xffffffffu, deg > kBuildShort && deg <= kHeavyRow) & leaders; rest;
+             rest &= rest - 1) {
+            const int leader = __ffs(rest) - 1;
+            const int vv = static_cast<int>(base) + leader / W;
+            const int b = __shfl_sync(0xffffffffu, begin, leader), e_end = __shfl_sync(0xffffffffu, end, leader);
+            C* h = warp_hist + (leader / W) * k;
+            for (int e = b + lane; e < e_end; e += 32) {
+                const int u = nbr[e];
+                if (u != vv) atomicAdd(h + labels[u], static_cast<C>(edge_w(ew, e)));
             }
         }
         __syncwarp();
         C total = 0;
-        for (int p = lane; p < k; p += 32) {
-            const C x = row[p];
-            A[static_cast<i64>(v) * k + p] = x;
-            total += x;
+        if (valid) {
+            C* row = A + v * k;
+            for (int p0 = sub * N; p0 < k; p0 += W * N) {
+                if constexpr (Vectorized) {
+                    const typename AffinityVec<C>::V x = *reinterpret_cast<const typename AffinityVec<C>::V*>(hist + p0);
+                    *reinterpret_cast<typename AffinityVec<C>::V*>(row + p0) = x;
+                    if constexpr (N == 4) total += x.x + x.y + x.z + x.w;
+                    else total += x.x + x.y;
+                } else {
+                    row[p0] = hist[p0];
+                    total += hist[p0];
+                }
+            }
         }
-        total = warp_sum(total);
-        if (lane == 0) totals[v] = total;
+#pragma unroll
+        for (int d = W / 2; d; d >>= 1) total += __shfl_xor_sync(0xffffffffu, total, d, W);
+        if (valid && sub == 0) {
+            totals[v] = total;
+            if (directed_cut) cut += static_cast<u64>(total - hist[labels[v]]);
+        }
         __syncwarp();
     }
+    if (directed_cut) block_atomic_add(directed_cut, cut);
+}
+
+// Directed cut of the heavy rows once k_build_chunks has completed them.
+template <class C>
+__global__ void k_heavy_cut(i64 count, const int* heavy, const int* labels, int k, const C* A, const C* totals,
+                            u64* directed_cut, const u64* gate, u64 threshold) {
+    if (gate && *gate <= threshold) return;
+    u64 cut = 0;
+    for (i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; h < count; h += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = heavy[h];
+        cut += static_cast<u64>(totals[v] - A[static_cast<i64>(v) * k + labels[v]]);
+    }
+    block_atomic_add(directed_cut, cut);
 }
 
 template <class C>
-__global__ void k_build_chunks(DGraph g, const int* labels, int k, C* A, C* totals) {
+__global__ void k_build_chunks(DGraph g, const int* labels, int k, C* A, C* totals, const u64* gate, u64 threshold) {
     extern __shared__ unsigned char smem_build[];
+    if (gate && *gate <= threshold) return;
     C* hist = reinterpret_cast<C*>(smem_build);
     const int c = blockIdx.x, v = g.chunk_row[c];
     for (int p = threadIdx.x; p < k; p += blockDim.x) hist[p] = 0;
@@ -182,16 +231,13 @@ struct LpParams {
     u64* counters;  // 0 candidates, 1 movers, 2 delta (signed), 3 max load
 };
 
-// 16-byte loads of affinity rows when a row starts on a 16-byte boundary.
-template <class C> struct AffinityVec;
-template <> struct AffinityVec<u32> { using V = uint4; static constexpr int N = 4; };
-template <> struct AffinityVec<u64> { using V = ulonglong2; static constexpr int N = 2; };
-
 // incremental_lp_proposal (incremental.cuh:166-198).  A warp takes 32
 // consecutive vertices: each lane reads its vertex's lock, label, own-part
 // affinity and row total (coalesced), and only boundary rows are scanned, by
 // groups of W lanes, 32/W rows at a time.  Ties keep the lowest part id.
-// Proposers are appended once per warp pass.
+// Proposers are appended with one atomic per block pass (the reference
+// appends per warp, append_warp, incremental.cuh:201-208; the order of the
+// candidate list does not affect any result).
 template <class C, int W, bool Vectorized>
 __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, const C* totals) {
     using Vec = AffinityVec<C>;
@@ -205,8 +251,11 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
         for (int p = threadIdx.x; p < k; p += blockDim.x) { s_slack[p] = q.capacity - q.loads[p]; s_price[p] = q.prices[p]; }
     __syncthreads();
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
-    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
-    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < q.n; base += warps * 32) {
+    // Block-uniform passes (the append synchronises the block); warp w of the
+    // block takes vertices [32w, 32w + 32) of the block's 256.
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < q.n;
+         block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 base = block_base + (threadIdx.x & ~31);
         const i64 v = base + lane;
         int src = 0;
         u64 current = 0;
@@ -286,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
             }
         }
         __syncwarp();
-        append(static_cast<int>(v), s_propose[threadIdx.x] != 0, q.cand, q.counters + 0);
+        block_append(static_cast<int>(v), s_propose[threadIdx.x] != 0, q.cand, q.counters + 0);
     }
 }
 
@@ -375,7 +424,7 @@ __global__ void k_compact_movers(LpParams q) {
     for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < count; base += static_cast<i64>(gridDim.x) * blockDim.x) {
         const i64 i = base + threadIdx.x;
         const int v = i < count ? q.cand[i] : 0;
-        append(v, i < count && q.flags[v], q.movers, q.counters + 1);
+        block_append(v, i < count && q.flags[v], q.movers, q.counters + 1);
     }
 }
 
@@ -385,8 +434,9 @@ __global__ void k_compact_movers(LpParams q) {
 template <class C>
 __global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
                          const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
-                         C* A, long long* delta, Sample* samples) {
+                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold) {
     const int lane = threadIdx.x & 31;
+    if (gate && *gate > threshold) return;  // rebuild chosen
     if (live_count) count = static_cast<i64>(*live_count);
     long long total = 0;
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
@@ -413,14 +463,15 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
             atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
         }
     }
-    if (lane == 0 && total) atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(total));
+    block_atomic_add(delta, lane == 0 ? total : 0LL);
 }
 
 // Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,
 // incremental.cuh:508-530); a row moves when its flag is set.
 template <class C>
 __global__ void k_update_chunks(DGraph g, const int* labels, const int* targets, const int* flags, int k, C* A,
-                                long long* delta, Sample* samples) {
+                                long long* delta, Sample* samples, const u64* gate, u64 threshold) {
+    if (gate && *gate > threshold) return;
     const int c = blockIdx.x, v = g.chunk_row[c];
     if (!flags[v]) return;
     const int s = labels[v], t = targets[v];
@@ -436,13 +487,23 @@ __global__ void k_update_chunks(DGraph g, const int* labels, const int* targets,
         atomicAdd(A + static_cast<i64>(u) * k + t, static_cast<C>(w));
         if (!moves || u > v) gain += static_cast<long long>(w) * ((s != old) - (t != nw));
     }
-    gain = warp_sum(gain);
-    if ((threadIdx.x & 31) == 0 && gain) {
+    gain = block_sum(gain);
+    if (threadIdx.x == 0 && gain) {
         atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(gain));
         if (samples) atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
     }
     if (samples && threadIdx.x == 0 && g.chunk_begin[c] == g.off[v])
         atomicAdd(&samples[s].weight, static_cast<u64>(g.vw[v]));
+}
+
+// Entries of the rows of a mover list: decides between updating the cache
+// entry by entry and rebuilding it after the commit.
+__global__ void k_mover_entries(i64 count, const int* movers, const u64* live_count, const int* off, u64* out) {
+    if (live_count) count = static_cast<i64>(*live_count);
+    u64 entries = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        entries += static_cast<u64>(off[movers[i] + 1] - off[movers[i]]);
+    block_atomic_add(out, entries);
 }
 
 // incremental_commit (incremental.cuh:532-547) with per-block aggregation of
@@ -532,68 +593,122 @@ struct WriteOrdered {
     __device__ void operator()(u32 slot, i64 i) const { out[slot] = order[i]; }
 };
 
+// Loads N consecutive affinities of a row (one 16-byte load when N > 1).
+template <class C, int N>
+__device__ __forceinline__ void load_affinities(const C* p, C (&val)[N]) {
+    if constexpr (N == 1) {
+        val[0] = *p;
+    } else {
+        const typename AffinityVec<C>::V x = *reinterpret_cast<const typename AffinityVec<C>::V*>(p);
+        if constexpr (N == 4) { val[0] = x.x; val[1] = x.y; val[2] = x.z; val[3] = x.w; }
+        else { val[0] = x.x; val[1] = x.y; }
+    }
+}
+
 // enumerate_repair_destination (rebalance_select.cuh:9-75), dense layout, plus
 // the bucket of incremental_rebalance_proposals (incremental.cuh:559-622).
-// One warp per donor.
-template <class C>
-__global__ void k_repair_dest(i64 count, const u32* donors, const C* A, const C* totals, const int* labels,
-                              const u32* vw, int k, const u64* loads, u64 capacity, const u64* cdf, int* targets,
-                              u64* bucket_keys) {
-    const int lane = threadIdx.x & 31;
-    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
-         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
-        const int v = static_cast<int>(donors[i]);
-        const int src = labels[v];
-        const u64 w = vw[v];
-        const u64 current = A[static_cast<i64>(v) * k + src];
+// W lanes per donor; the parts' free room is staged per block.  A part p is a
+// feasible destination for weight w when w <= room[p] (room = C - load for
+// parts under capacity, else 0; vertex weights are positive).
+template <class C, int W, bool Vectorized>
+__global__ void __launch_bounds__(kThreads) k_repair_dest(i64 count, const u32* donors, const C* A, const C* totals,
+                                                          const int* labels, const u32* vw, int k, const u64* loads,
+                                                          u64 capacity, const u64* cdf, int* targets, u64* bucket_keys) {
+    constexpr int N = Vectorized ? AffinityVec<C>::N : 1;
+    constexpr int G = 32 / W;
+    __shared__ u64 s_room[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_room[p] = loads[p] < capacity ? capacity - loads[p] : 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    const int span = (k + W - 1) / W;  // contiguous parts per lane for the fallback ticket
+    for (i64 i0 = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; i0 < count; i0 += warps * G) {
+        const i64 i = i0 + gid;
+        const bool valid = i < count;
+        const int v = valid ? static_cast<int>(donors[i]) : 0;
+        const int src = valid ? labels[v] : 0;
+        const u64 w = valid ? vw[v] : 0;
+        const u64 current = valid ? static_cast<u64>(A[static_cast<i64>(v) * k + src]) : 0;
+        const bool scan = valid && current != static_cast<u64>(totals[v]);
         int part = -1;
-        u64 conn = 0, best_slack = 0;
-        if (current != static_cast<u64>(totals[v])) {
-            for (int p = lane; p < k; p += 32) {
-                if (p == src || loads[p] >= capacity || w > capacity - loads[p]) continue;
-                const u64 value = A[static_cast<i64>(v) * k + p], slack = capacity - loads[p];
-                if (part < 0 || value > conn || (value == conn && slack > best_slack)) { part = p; conn = value; best_slack = slack; }
-            }
-            for (int d = 16; d; d >>= 1) {
-                const int op = __shfl_xor_sync(0xffffffffu, part, d);
-                const u64 oc = __shfl_xor_sync(0xffffffffu, conn, d);
-                const u64 os = __shfl_xor_sync(0xffffffffu, best_slack, d);
-                if (op >= 0 && (part < 0 || oc > conn || (oc == conn && (os > best_slack || (os == best_slack && op < part))))) {
-                    part = op; conn = oc; best_slack = os;
+        u64 conn = 0, best_room = 0;
+        if (scan) {
+            const C* row = A + static_cast<i64>(v) * k;
+            for (int p0 = sub * N; p0 < k; p0 += W * N) {
+                C val[N];
+                load_affinities<C, N>(row + p0, val);
+#pragma unroll
+                for (int e = 0; e < N; ++e) {
+                    const int p = p0 + e;
+                    const u64 room = s_room[p];
+                    if (p == src || w > room) continue;
+                    const u64 value = val[e];
+                    if (part < 0 || value > conn || (value == conn && room > best_room)) { part = p; conn = value; best_room = room; }
                 }
             }
-            if (!conn) part = -1;
         }
-        if (lane == 0) {
-            if (part < 0) {
+#pragma unroll
+        for (int d = W / 2; d; d >>= 1) {
+            const int op = __shfl_xor_sync(0xffffffffu, part, d, W);
+            const u64 oc = __shfl_xor_sync(0xffffffffu, conn, d, W);
+            const u64 orm = __shfl_xor_sync(0xffffffffu, best_room, d, W);
+            if (op >= 0 && (part < 0 || oc > conn || (oc == conn && (orm > best_room || (orm == best_room && op < part))))) {
+                part = op; conn = oc; best_room = orm;
+            }
+        }
+        if (!conn) part = -1;
+        // Fallback ticket over the parts' room when no connected destination
+        // fits: from the slack CDF when the source is at capacity, else over
+        // the parts that fit w, in part order (saturating sums).
+        const bool ticket = valid && part < 0 && !(loads[src] >= capacity && w <= cdf[k]);
+        const u32 hash = mix32(static_cast<u32>(v));
+        if (__any_sync(0xffffffffu, ticket)) {
+            const int lo = sub * span, hi = min(k, lo + span);
+            u64 mine = 0;
+            if (ticket)
+                for (int p = lo; p < hi; ++p)
+                    if (p != src && w <= s_room[p]) mine = ~0ULL - mine < s_room[p] ? ~0ULL : mine + s_room[p];
+            u64 upto = mine;  // inclusive scan over the group, saturating
+#pragma unroll
+            for (int d = 1; d < W; d <<= 1) {
+                const u64 o = __shfl_up_sync(0xffffffffu, upto, d, W);
+                if (sub >= d) upto = ~0ULL - upto < o ? ~0ULL : upto + o;
+            }
+            const u64 total = __shfl_sync(0xffffffffu, upto, W - 1, W);
+            // Exclusive prefix, saturated: exact for the lane holding the
+            // ticket (ticket < total), above the ticket for every later lane.
+            const u64 prev = __shfl_up_sync(0xffffffffu, upto, 1, W);
+            const u64 before = sub == 0 ? 0 : prev;
+            int found = -1;
+            if (ticket && total) {
+                u64 t = static_cast<u64>(hash) % total;
+                if (t >= before && (t - before) < mine) {
+                    t -= before;
+                    for (int p = lo; p < hi; ++p)
+                        if (p != src && w <= s_room[p]) {
+                            if (t < s_room[p]) { found = p; break; }
+                            t -= s_room[p];
+                        }
+                }
+            }
+#pragma unroll
+            for (int d = W / 2; d; d >>= 1) found = max(found, __shfl_xor_sync(0xffffffffu, found, d, W));
+            if (ticket) part = found;
+        }
+        if (valid && sub == 0) {
+            if (part < 0 && !ticket) {
                 conn = 0;
-                const u32 hash = mix32(static_cast<u32>(v));
                 if (loads[src] >= capacity && w <= cdf[k]) {
-                    const u64 total = cdf[k - 1];
-                    if (total) {
-                        const u64 ticket = static_cast<u64>(hash) % total;
+                    const u64 sum = cdf[k - 1];
+                    if (sum) {
+                        const u64 t = static_cast<u64>(hash) % sum;
                         int lo = 0, hi = k;
-                        while (lo < hi) { const int mid = (lo + hi) / 2; if (cdf[mid] <= ticket) lo = mid + 1; else hi = mid; }
+                        while (lo < hi) { const int mid = (lo + hi) / 2; if (cdf[mid] <= t) lo = mid + 1; else hi = mid; }
                         part = lo;
                     }
-                } else {
-                    u64 total = 0;
-                    for (int p = 0; p < k; ++p)
-                        if (p != src && loads[p] < capacity && w <= capacity - loads[p]) {
-                            const u64 s = capacity - loads[p];
-                            total = ~0ULL - total < s ? ~0ULL : total + s;
-                        }
-                    if (total) {
-                        u64 ticket = static_cast<u64>(hash) % total;
-                        for (int p = 0; p < k; ++p)
-                            if (p != src && loads[p] < capacity && w <= capacity - loads[p]) {
-                                const u64 s = capacity - loads[p];
-                                if (ticket < s) { part = p; break; }
-                                ticket -= s;
-                            }
-                    }
                 }
             }
+            if (ticket) conn = 0;
             targets[v] = part;
             u64 key = ~0ULL;
             if (part >= 0) {
@@ -656,47 +771,72 @@ struct WriteFrom {
 
 // One attempt of the receiver reservation: choose a part for every active,
 // unplaced donor (attempt 0: its proposal; later: best affinity among parts
-// not yet tried whose remaining virtual room holds it).
-template <class C>
-__global__ void k_choose(i64 count, const u32* active, int attempt, const C* A, const int* labels, const u32* vw,
-                         int k, const int* proposal, const u64* slack, const u64* requests, u64* tried,
-                         unsigned char* state, int* want, u64* requesters) {
-    const int lane = threadIdx.x & 31;
-    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
-         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
-        if (state[i]) {  // placed or out of options
-            if (lane == 0) want[i] = -1;
-            continue;
-        }
-        const int v = static_cast<int>(active[i]);
-        const u64 w = vw[v];
+// not yet tried whose remaining virtual room holds it).  W lanes per donor;
+// the parts' remaining room is staged per block.
+template <class C, int W, bool Vectorized>
+__global__ void __launch_bounds__(kThreads) k_choose(i64 count, const u32* active, int attempt, const C* A,
+                                                     const int* labels, const u32* vw, int k, const int* proposal,
+                                                     const u64* slack, const u64* requests, u64* tried,
+                                                     unsigned char* state, int* want, u64* requesters) {
+    constexpr int N = Vectorized ? AffinityVec<C>::N : 1;
+    constexpr int G = 32 / W;
+    __shared__ u64 s_avail[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_avail[p] = requests[p] < slack[p] ? slack[p] - requests[p] : 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    u64 asked = 0;
+    for (i64 i0 = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; i0 < count; i0 += warps * G) {
+        const i64 i = i0 + gid;
+        const bool valid = i < count;
+        const unsigned char st = valid ? state[i] : 1;  // placed or out of options
+        const bool open = valid && !st;
+        const int v = open ? static_cast<int>(active[i]) : 0;
         int target = -1;
         if (attempt == 0) {
-            target = proposal[v];
+            if (open) target = proposal[v];
         } else {
             u64 best = 0, room = 0;
-            for (int p = lane; p < k; p += 32) {
-                if (p == labels[v] || ((tried[2 * i + (p >> 6)] >> (p & 63)) & 1)) continue;
-                const u64 avail = requests[p] < slack[p] ? slack[p] - requests[p] : 0;
-                if (avail < w) continue;
-                const u64 c = A[static_cast<i64>(v) * k + p];
-                if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+            if (open) {
+                const u64 w = vw[v];
+                const int src = labels[v];
+                const u64 t0 = tried[2 * i], t1 = tried[2 * i + 1];
+                const C* row = A + static_cast<i64>(v) * k;
+                for (int p0 = sub * N; p0 < k; p0 += W * N) {
+                    C val[N];
+                    load_affinities<C, N>(row + p0, val);
+#pragma unroll
+                    for (int e = 0; e < N; ++e) {
+                        const int p = p0 + e;
+                        if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+                        const u64 avail = s_avail[p];
+                        if (avail < w) continue;
+                        const u64 c = val[e];
+                        if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                    }
+                }
             }
-            for (int d = 16; d; d >>= 1) {
-                const int ot = __shfl_xor_sync(0xffffffffu, target, d);
-                const u64 ob = __shfl_xor_sync(0xffffffffu, best, d);
-                const u64 orr = __shfl_xor_sync(0xffffffffu, room, d);
+#pragma unroll
+            for (int d = W / 2; d; d >>= 1) {
+                const int ot = __shfl_xor_sync(0xffffffffu, target, d, W);
+                const u64 ob = __shfl_xor_sync(0xffffffffu, best, d, W);
+                const u64 orr = __shfl_xor_sync(0xffffffffu, room, d, W);
                 if (ot >= 0 && (target < 0 || ob > best || (ob == best && (orr > room || (orr == room && ot < target))))) {
                     target = ot; best = ob; room = orr;
                 }
             }
         }
-        if (lane == 0) {
-            want[i] = target;
-            if (target < 0) state[i] = 2;
-            else atomicAdd(requesters, 1ULL);
+        if (valid && sub == 0) {
+            if (!open) {
+                want[i] = -1;
+            } else {
+                want[i] = target;
+                if (target < 0) state[i] = 2;
+                else ++asked;
+            }
         }
     }
+    block_atomic_add(requesters, asked);
 }
 
 struct WantsPart {
@@ -817,6 +957,36 @@ __global__ void k_bitonic(int size, int count, const JointMove* moves, int* idx,
     else greater = cmp(moves[b], moves[a]);
     const bool up = (i & kk) == 0;
     if (greater == up) { idx[i] = b; idx[x] = a; }
+}
+// Bitonic stages on segments of kBitonicSegment indices held in shared
+// memory: for kk from kk_first to kk_last, every jj below the segment size
+// (the first kk starts at jj_first).  Same compare-exchange as k_bitonic.
+constexpr int kBitonicSegment = 4096;
+template <class Cmp>
+__global__ void __launch_bounds__(1024) k_bitonic_local(int size, int count, const JointMove* moves, int* idx, int kk_first,
+                                                       int kk_last, int jj_first, Cmp cmp) {
+    __shared__ int s_idx[kBitonicSegment];
+    const int base = blockIdx.x * kBitonicSegment;
+    const int seg = min(kBitonicSegment, size - base);
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) s_idx[i] = idx[base + i];
+    __syncthreads();
+    for (int kk = kk_first; kk <= kk_last; kk <<= 1) {
+        for (int jj = kk == kk_first ? jj_first : kk >> 1; jj; jj >>= 1) {
+            for (int p = threadIdx.x; p < seg / 2; p += blockDim.x) {
+                const int i = (p / jj) * 2 * jj + p % jj;
+                const int x = i + jj;
+                const int a = s_idx[i], b = s_idx[x];
+                bool greater;
+                if (a >= count) greater = b < count;
+                else if (b >= count) greater = false;
+                else greater = cmp(moves[b], moves[a]);
+                const bool up = ((base + i) & kk) == 0;
+                if (greater == up) { s_idx[i] = b; s_idx[x] = a; }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) idx[base + i] = s_idx[i];
 }
 __global__ void k_iota(int n, int* idx) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1178,53 +1348,91 @@ private:
     u64* counters = nullptr;  // device: 0 cand, 1 movers, 2 delta, 3 max load, 4.. scratch
     long long* corr_acc = nullptr;  // per heavy row: priority-filter correction
     u64 cut = 0, revision = 0;
+    u64 rebuild_entries = ~0ULL;  // mover entries above which apply() rebuilds the cache
     u64 max_load_host = 0;
 
     cudaStream_t s() const { return ctx.stream; }
     int grid_for(i64 items, int per_block) const { return static_cast<int>(std::min<i64>(blocks_for(items, per_block), 148 * 32)); }
 
-    void build() {
-        const size_t smem = 8 * k * sizeof(T);
-        launch(k_build<T>, grid_for(n * 32, kThreads), kThreads, smem, s(), n, g.off, g.nbr, g.ew, labels, k, A, totals);
-        if (g.chunks)
+    // Rebuilds the cache and row totals from the labels; with directed_cut
+    // also sums the directed cut (device counter, cleared by the caller).
+    void build(u64* directed_cut = nullptr, const u64* gate = nullptr, u64 threshold = 0) {
+        constexpr int W = 8;
+        const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
+        const size_t smem = static_cast<size_t>(kThreads / 32) * (32 / W) * k * sizeof(T);
+        const int grid = grid_for(n * W, kThreads);
+        if (vec)
+            launch(k_build<T, W, true>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
+                   k, A, totals, directed_cut, gate, threshold);
+        else
+            launch(k_build<T, W, false>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
+                   k, A, totals, directed_cut, gate, threshold);
+        if (g.chunks) {
             launch(k_build_chunks<T>, static_cast<int>(g.chunks), 256, sizeof(T) * k, s(), g,
-                   static_cast<const int*>(labels), k, A, totals);
+                   static_cast<const int*>(labels), k, A, totals, gate, threshold);
+            if (directed_cut)
+                launch(k_heavy_cut<T>, blocks_for(g.heavy_count, kThreads), kThreads, 0, s(), g.heavy_count,
+                       static_cast<const int*>(g.heavy), static_cast<const int*>(labels), k, static_cast<const T*>(A),
+                       static_cast<const T*>(totals), directed_cut, gate, threshold);
+        }
     }
     // Applies the movers listed in `list` (count on device at `live`):
-    // cache/cut update, commit, flag reset.  Returns the cut decrease.
+    // cache/cut update, commit, flag reset.  Without repair samples, a batch
+    // whose rows hold more entries than rebuild_entries rebuilds the cache
+    // after the commit instead (identical values: the cache is an exact sum);
+    // settle() then takes the new cut from the rebuild.  counters: 2 delta,
+    // 3 max load, 6 mover entries, 7 directed cut of a rebuild.
     void apply(const int* list, const u64* live, i64 host_count, bool lp, bool sample) {
         GP_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(u64), s()));
+        GP_CUDA(cudaMemsetAsync(counters + 6, 0, 2 * sizeof(u64), s()));
+        const u64* gate = sample ? nullptr : counters + 6;
+        const u64 threshold = sample ? ~0ULL : rebuild_entries;
+        if (gate)
+            launch(k_mover_entries, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
+                   counters + 6);
         launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
                g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
-               sample ? samples : static_cast<Sample*>(nullptr));
+               sample ? samples : static_cast<Sample*>(nullptr), gate, threshold);
         if (g.chunks)
             launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
                    static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
-                   reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr));
+                   reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr), gate,
+                   threshold);
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
         launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
+        if (gate) build(counters + 7, gate, threshold);
         launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     }
-    // Group width: about four 16-byte loads (or four scalars) per lane.
-    void proposals(const LpParams& q) {
+    // Cut decrease of the last apply from host copies of counters[2..7].
+    long long settled_delta(const u64* h) const {
+        if (h[4] <= rebuild_entries) return static_cast<long long>(h[0]);
+        if (h[5] & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
+        return static_cast<long long>(cut) - static_cast<long long>(h[5] / 2);
+    }
+    // Lanes per row of the affinity cache: about four 16-byte loads (or four
+    // scalars) per lane.  f(width, vectorized) launches the instantiation.
+    template <class F>
+    void with_groups(F&& f) const {
         const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
         const int per_lane = vec ? 4 * AffinityVec<T>::N : 4;
         const int W = k <= 2 * per_lane ? 2 : k <= 4 * per_lane ? 4 : k <= 8 * per_lane ? 8 : 16;
+        auto go = [&](auto width) {
+            if (vec) f(width, std::true_type{});
+            else f(width, std::false_type{});
+        };
+        if (W == 2) go(std::integral_constant<int, 2>{});
+        else if (W == 4) go(std::integral_constant<int, 4>{});
+        else if (W == 8) go(std::integral_constant<int, 8>{});
+        else go(std::integral_constant<int, 16>{});
+    }
+    void proposals(const LpParams& q) {
         const int grid = grid_for(n, kThreads);
         const T* a = A;
         const T* t = totals;
-        if (vec) {
-            if (W == 2) launch(k_proposals<T, 2, true>, grid, kThreads, 0, s(), q, a, t);
-            else if (W == 4) launch(k_proposals<T, 4, true>, grid, kThreads, 0, s(), q, a, t);
-            else if (W == 8) launch(k_proposals<T, 8, true>, grid, kThreads, 0, s(), q, a, t);
-            else launch(k_proposals<T, 16, true>, grid, kThreads, 0, s(), q, a, t);
-        } else {
-            if (W == 2) launch(k_proposals<T, 2, false>, grid, kThreads, 0, s(), q, a, t);
-            else if (W == 4) launch(k_proposals<T, 4, false>, grid, kThreads, 0, s(), q, a, t);
-            else if (W == 8) launch(k_proposals<T, 8, false>, grid, kThreads, 0, s(), q, a, t);
-            else launch(k_proposals<T, 16, false>, grid, kThreads, 0, s(), q, a, t);
-        }
+        with_groups([&](auto width, auto vec) {
+            launch(k_proposals<T, decltype(width)::value, decltype(vec)::value>, grid, kThreads, 0, s(), q, a, t);
+        });
     }
     void account(long long delta) {
         if (delta >= 0) {
@@ -1251,10 +1459,10 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     }
     launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q);
     apply(movers, counters + 1, n, true, false);
-    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters, 4 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters, 8 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
     GP_CUDA(cudaStreamSynchronize(s()));
     const i64 count = static_cast<i64>(ctx.host_scalars[1]);
-    const long long delta = static_cast<long long>(ctx.host_scalars[2]);
+    const long long delta = settled_delta(ctx.host_scalars + 2);
     max_load_host = ctx.host_scalars[3];
     if (count) {
         account(delta);
@@ -1295,8 +1503,12 @@ bool LevelRefiner<T>::repair() {
             u64* keys_alt = A_.alloc<u64>(dcount);
             u32* items = A_.alloc<u32>(dcount);
             u32* items_alt = A_.alloc<u32>(dcount);
-            launch(k_repair_dest<T>, grid_for(dcount * 32, kThreads), kThreads, 0, s(), dcount, donors,
-                   static_cast<const T*>(A), static_cast<const T*>(totals), labels, g.vw, k, loads, C, cdf, targets, keys);
+            with_groups([&](auto width, auto vec) {
+                constexpr int W = decltype(width)::value;
+                launch(k_repair_dest<T, W, decltype(vec)::value>, grid_for(dcount * W, kThreads), kThreads, 0, s(),
+                       dcount, donors, static_cast<const T*>(A), static_cast<const T*>(totals), labels, g.vw, k, loads,
+                       C, cdf, targets, keys);
+            });
             GP_CUDA(cudaMemcpyAsync(items, donors, sizeof(u32) * dcount, cudaMemcpyDeviceToDevice, s()));
             // Stable sort by bucket keeps the repair order inside a bucket;
             // bucket keys are below k*800 < 2^17, the sentinel sorts last.
@@ -1326,9 +1538,12 @@ bool LevelRefiner<T>::repair() {
                 u64* rprefix = A_.alloc<u64>(acount);
                 for (int attempt = 0; attempt < k; ++attempt) {
                     GP_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(u64), s()));
-                    launch(k_choose<T>, grid_for(acount * 32, kThreads), kThreads, 0, s(), acount, active, attempt,
-                           static_cast<const T*>(A), labels, g.vw, k, targets, slack, requests, tried, state, want,
-                           counters + 5);
+                    with_groups([&](auto width, auto vec) {
+                        constexpr int W = decltype(width)::value;
+                        launch(k_choose<T, W, decltype(vec)::value>, grid_for(acount * W, kThreads), kThreads, 0, s(),
+                               acount, active, attempt, static_cast<const T*>(A), labels, g.vw, k, targets, slack,
+                               requests, tried, state, want, counters + 5);
+                    });
                     select_if(A_, s(), acount, WantsPart{want}, WriteIdx{reqs}, donor_count);
                     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
                     GP_CUDA(cudaStreamSynchronize(s()));
@@ -1353,9 +1568,9 @@ bool LevelRefiner<T>::repair() {
                 placed = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
                 if (placed) {
                     apply(movers, nullptr, placed, false, samples != nullptr);
-                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 6 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
                     GP_CUDA(cudaStreamSynchronize(s()));
-                    delta = static_cast<long long>(ctx.host_scalars[0]);
+                    delta = settled_delta(ctx.host_scalars);
                     max_load_host = ctx.host_scalars[1];
                     account(delta);
                     ++revision;
@@ -1403,10 +1618,19 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         int size = 1;
         while (size < count) size <<= 1;
         launch(k_iota, blocks_for(size, kThreads), kThreads, 0, s(), size, idx);
-        for (int kk = 2; kk <= size; kk <<= 1)
-            for (int jj = kk >> 1; jj; jj >>= 1)
-                launch(k_bitonic<decltype(cmp)>, blocks_for(size, kThreads), kThreads, 0, s(), size, count,
-                       static_cast<const JointMove*>(in), idx, kk, jj, cmp);
+        // Stages whose partner distance stays inside a segment run in shared
+        // memory, the rest one launch per stage.
+        const int segments = std::max(1, size / kBitonicSegment);
+        const JointMove* m = in;
+        launch(k_bitonic_local<decltype(cmp)>, segments, 1024, 0, s(), size, count, m, idx, 2,
+               std::min(size, kBitonicSegment), 1, cmp);
+        for (int kk = 2 * kBitonicSegment; kk <= size; kk <<= 1) {
+            for (int jj = kk >> 1; jj >= kBitonicSegment; jj >>= 1)
+                launch(k_bitonic<decltype(cmp)>, blocks_for(size, kThreads), kThreads, 0, s(), size, count, m, idx, kk,
+                       jj, cmp);
+            launch(k_bitonic_local<decltype(cmp)>, segments, 1024, 0, s(), size, count, m, idx, kk, kk,
+                   kBitonicSegment / 2, cmp);
+        }
         launch(k_gather_moves, blocks_for(count, kThreads), kThreads, 0, s(), count, static_cast<const int*>(idx),
                static_cast<const JointMove*>(in), out);
     };
@@ -1453,9 +1677,9 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         if (!count) { if (++empty >= 2) break; continue; }
         empty = 0;
         apply(movers, nullptr, count, false, false);
-        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 6 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
         GP_CUDA(cudaStreamSynchronize(s()));
-        const long long delta = static_cast<long long>(ctx.host_scalars[0]);
+        const long long delta = settled_delta(ctx.host_scalars);
         max_load_host = ctx.host_scalars[1];
         account(delta);
         ++revision;
@@ -1504,12 +1728,22 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
         launch(k_repair_keys, blocks_for(n, kThreads), kThreads, 0, s(), n, keys, rorder);
         radix_sort_pairs(A_, s(), n, keys, rorder, keys_alt, rorder_alt, 0, 32);
     }
-    build();
-    cut = has_known ? known : device_cut(ctx, g, labels);
+    // An entry-by-entry update touches two random cache counters per entry
+    // (about 128 bytes of DRAM traffic); a rebuild writes the whole cache and
+    // reads the CSR once.
+    rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) / 128;
+    GP_CUDA(cudaMemsetAsync(counters + 7, 0, sizeof(u64), s()));
+    build(has_known ? nullptr : counters + 7);
     launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
-    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, 5 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
     GP_CUDA(cudaStreamSynchronize(s()));
     max_load_host = ctx.host_scalars[0];
+    if (has_known) {
+        cut = known;
+    } else {
+        if (ctx.host_scalars[4] & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
+        cut = ctx.host_scalars[4] / 2;
+    }
     LevelResult res;
     if (max_load_host > C) {
         if (!repair()) {
