@@ -1564,6 +1564,10 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
         }
         DGraph coarse = contract(ctx, current, agg, ws);
         ctx.scratch.release(mark);
+        if (o.verify) {
+            verify_level(ctx, current, coarse, agg.map, agg.capacity);
+            if (o.log) std::printf("ml_layer_verify level=%d map=ok weights=ok csr=ok projection_cut=ok\n", level);
+        }
         h.levels.push_back(current);
         h.maps.push_back(agg.map);
         current = coarse;

@@ -62,6 +62,7 @@ struct CoarsenOptions {
     bool seed_matching = true, fast_path = true;
     int heavy_limit = 64;
     bool log = true;
+    bool verify = false;  // GP_FLAG_VERIFY: strict per-level checks
 };
 
 // Device-resident scalars read back in batches through pinned memory.
@@ -109,9 +110,13 @@ struct RefineOutcome {
 // Refines from the coarsest level down to level 0 (refine_hierarchy_impl,
 // src/refine.cu:483-730); `labels` (device, level-0 sized) receives the result.
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
-                        int* labels, bool log);
+                        int* labels, bool log, bool verify);
 
 // Device edge cut of labels (directed sum / 2); throws on an odd sum.
 u64 device_cut(Context& ctx, const DGraph& g, const int* labels);
+
+// GP_FLAG_VERIFY checks (gp_verify.cu); failures throw with `status` or GP_INTERNAL.
+void verify_csr(Context& ctx, const DGraph& g, bool allow_self_loops, gp_status status);
+void verify_level(Context& ctx, const DGraph& fine, const DGraph& coarse, const int* map, u64 cluster_cap);
 
 }  // namespace gp

@@ -213,6 +213,10 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     o.seed_matching = handle->seed_matching && !(flags & GP_FLAG_NO_SEED_MATCHING);
     o.fast_path = handle->fast_path;
     o.log = !(flags & GP_FLAG_QUIET);
+    o.verify = (flags & GP_FLAG_VERIFY) != 0;
+    // --verify: the input must be bidirectional with equal reverse weights
+    // (validate_weighted_csr, src/graph.cpp:157-182).
+    if (o.verify) verify_csr(ctx, g, true, GP_INVALID_ARGUMENT);
     Hierarchy h = coarsen(ctx, g, o);
     GP_CUDA(cudaEventRecord(ctx.ev[2], s));
     if (flags & GP_FLAG_KEEP_HIERARCHY) keep_levels(ctx, h);
@@ -236,7 +240,7 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     ctx.initial_labels = coarse_labels;
     GP_CUDA(cudaEventRecord(ctx.ev[3], s));
     int* labels_dev = device_input ? labels_out : ctx.persist.alloc<int>(n);
-    RefineOutcome r = uncoarsen(ctx, h, coarse_labels, k, eps, labels_dev, o.log);
+    RefineOutcome r = uncoarsen(ctx, h, coarse_labels, k, eps, labels_dev, o.log, o.verify);
     GP_CUDA(cudaEventRecord(ctx.ev[4], s));
     if (directed & 1ULL) fail(GP_INTERNAL, "symmetric graph has odd directed edge weight");
     if (!device_input)

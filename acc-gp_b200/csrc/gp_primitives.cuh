@@ -202,6 +202,7 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kDirectTiles = 64;  // up to this many tiles, downsweeps read the raw histogram
 
 // Item i of a tile lives in warp i/256, register slot (i%256)/32, lane i%32,
 // so the order (warp, slot, lane) is the input order and ranks stay stable.
@@ -320,13 +321,27 @@ __device__ __forceinline__ void rank_tile(u32 (*warp_count)[kRadix], u32* local_
 // One pass of a multi-tile sort.  The tile is ordered by digit in shared
 // memory first, so the scatter writes runs of equal digits to consecutive
 // addresses instead of one isolated element per thread.
-template <bool WithValues>
+// Direct: `offsets` is the raw digit-major tile histogram and every block
+// derives its own digit bases from it (for few tiles, instead of a scan).
+template <bool WithValues, bool Direct>
 __global__ void __launch_bounds__(kSortThreads) k_radix_downsweep(i64 count, const u64* keys, const u32* vals, int shift,
                                                                   const u32* offsets, u64* keys_out, u32* vals_out) {
     __shared__ SortTileSmem sm;
     const i64 base = static_cast<i64>(blockIdx.x) * kSortTile;
     const int tile_items = static_cast<int>(count - base < kSortTile ? count - base : kSortTile);
-    sm.digit_base[threadIdx.x] = offsets[static_cast<i64>(threadIdx.x) * gridDim.x + blockIdx.x];
+    if constexpr (Direct) {
+        const u32* row = offsets + static_cast<i64>(threadIdx.x) * gridDim.x;
+        u32 total = 0, before = 0;
+        for (int t = 0; t < static_cast<int>(gridDim.x); ++t) {
+            const u32 c = row[t];
+            total += c;
+            before += t < static_cast<int>(blockIdx.x) ? c : 0u;
+        }
+        u32 all;
+        sm.digit_base[threadIdx.x] = block_exclusive_scan<u32>(total, all, sm.scan) + before;
+    } else {
+        sm.digit_base[threadIdx.x] = offsets[static_cast<i64>(threadIdx.x) * gridDim.x + blockIdx.x];
+    }
     u64 k[kSortItems];
     u32 v[kSortItems];
     bool valid[kSortItems];
@@ -416,13 +431,19 @@ inline void radix_sort_pairs(Arena& arena, cudaStream_t s, i64 count, u64*& keys
     ArenaScope scope(arena);
     const int tiles = blocks_for(count, kSortTile);
     u32* hist = arena.alloc<u32>(static_cast<size_t>(tiles) * kRadix);
+    const bool direct = tiles <= kDirectTiles;
     for (int shift = begin_bit; shift < end_bit; shift += kRadixBits) {
         launch(k_radix_upsweep, tiles, kSortThreads, 0, s, count, keys, shift, hist);
-        exclusive_scan<u32>(arena, s, static_cast<i64>(tiles) * kRadix, LoadOf<u32>{hist}, hist, static_cast<u32*>(nullptr));
-        if (vals)
-            launch(k_radix_downsweep<true>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
+        if (!direct)
+            exclusive_scan<u32>(arena, s, static_cast<i64>(tiles) * kRadix, LoadOf<u32>{hist}, hist, static_cast<u32*>(nullptr));
+        if (vals && direct)
+            launch(k_radix_downsweep<true, true>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
+        else if (vals)
+            launch(k_radix_downsweep<true, false>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
+        else if (direct)
+            launch(k_radix_downsweep<false, true>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
         else
-            launch(k_radix_downsweep<false>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
+            launch(k_radix_downsweep<false, false>, tiles, kSortThreads, 0, s, count, keys, vals, shift, hist, keys_alt, vals_alt);
         account_bytes(static_cast<double>(count) * (vals ? 24.0 : 16.0) + static_cast<double>(tiles) * kRadix * 4.0);
         std::swap(keys, keys_alt);
         if (vals) std::swap(vals, vals_alt);

@@ -172,6 +172,17 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
     if (directed_cut) block_atomic_add(directed_cut, cut);
 }
 
+// GP_FLAG_VERIFY: the incremental cache against an independent rebuild.
+template <class C>
+__global__ void k_compare_cache(i64 cells, const C* A, const C* B, i64 n, const C* ta, const C* tb, u64* mismatch) {
+    u32 bad = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        bad |= A[i] != B[i];
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x)
+        bad |= ta[v] != tb[v];
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(mismatch, 1ULL);
+}
+
 // Directed cut of the heavy rows once k_build_chunks has completed them.
 template <class C>
 __global__ void k_heavy_cut(i64 count, const int* heavy, const int* labels, int k, const C* A, const C* totals,
@@ -885,6 +896,108 @@ __global__ void k_admit(i64 count, const u32* reqs, const u64* keys, const u32* 
 __global__ void k_merge_requests(int k, u64* requests, u64* added) {
     for (int p = threadIdx.x; p < k; p += blockDim.x) { requests[p] += added[p]; added[p] = 0; }
 }
+// The remaining attempts of a receiver reservation by one block, for a small
+// set of open donors: the choice of k_choose and the ticket rule of k_admit,
+// attempt after attempt, without a round trip to the host.  open[j] (j <
+// *count, ascending) indexes the active donors, so the requests of one target
+// are admitted in repair order exactly as the device-wide path does.
+constexpr int kAttemptThreads = 1024;
+constexpr int kAttemptCap = 2048;  // open donors handled by one block
+template <class C>
+__global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, const u32* count_ptr, int first_attempt,
+                                                              const u32* active, const C* A, const int* labels,
+                                                              const u32* vw, int k, const int* proposal,
+                                                              const u64* slack, u64* requests, u64* tried,
+                                                              unsigned char* state, int* targets, int* flags) {
+    constexpr int kWarps = kAttemptThreads / 32;
+    __shared__ u64 s_slack[kMaxParts], s_requests[kMaxParts], s_base[kMaxParts];
+    __shared__ u64 s_warp[kWarps][kMaxParts];  // per-warp weight requested per part
+    __shared__ int s_want[kAttemptCap];
+    __shared__ int s_any;
+    const int count = static_cast<int>(*count_ptr);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) { s_slack[p] = slack[p]; s_requests[p] = requests[p]; }
+    __syncthreads();
+    for (int attempt = first_attempt; attempt < k; ++attempt) {
+        if (threadIdx.x == 0) s_any = 0;
+        __syncthreads();
+        // Choice (k_choose).
+        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+            const u32 i = open[j];
+            int target = -1;
+            if (!state[i]) {
+                const int v = static_cast<int>(active[i]);
+                if (attempt == 0) {
+                    target = proposal[v];
+                } else {
+                    const u64 w = vw[v];
+                    const int src = labels[v];
+                    const u64 t0 = tried[2 * i], t1 = tried[2 * i + 1];
+                    u64 best = 0, room = 0;
+                    for (int p = 0; p < k; ++p) {
+                        if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+                        const u64 avail = s_requests[p] < s_slack[p] ? s_slack[p] - s_requests[p] : 0;
+                        if (avail < w) continue;
+                        const u64 c = A[static_cast<i64>(v) * k + p];
+                        if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                    }
+                }
+                if (target < 0) state[i] = 2;
+                else s_any = 1;
+            }
+            s_want[j] = target;
+        }
+        __syncthreads();
+        if (!s_any) break;
+        // Admission in chunks of one request per thread, in j order: each
+        // request starts after the weight requested for its part by earlier
+        // requests (earlier chunks, earlier warps, earlier lanes).
+        for (int p = threadIdx.x; p < k; p += blockDim.x) s_base[p] = s_requests[p];
+        for (int chunk = 0; chunk < count; chunk += blockDim.x) {
+            for (int x = threadIdx.x; x < kWarps * k; x += blockDim.x) s_warp[x / k][x % k] = 0;
+            __syncthreads();
+            const int j = chunk + threadIdx.x;
+            const int t = j < count ? s_want[j] : -1;
+            const u32 i = j < count ? open[j] : 0;
+            const u64 w = t >= 0 ? vw[active[i]] : 0;
+            const unsigned peers = __match_any_sync(0xffffffffu, t);
+            u64 before = 0, sum = 0;
+            for (unsigned rest = peers; rest; rest &= rest - 1) {
+                const int l = __ffs(rest) - 1;
+                const u64 o = __shfl_sync(peers, w, l);
+                sum += o;
+                if (l < lane) before += o;
+            }
+            if (t >= 0 && lane == __ffs(peers) - 1) s_warp[warp][t] = sum;
+            __syncthreads();
+            if (t >= 0) {
+                u64 begin = s_base[t] + before;
+                for (int w2 = 0; w2 < warp; ++w2) begin += s_warp[w2][t];
+                tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
+                if (begin <= s_slack[t] && w <= s_slack[t] - begin) {
+                    targets[active[i]] = t;
+                    flags[active[i]] = 1;
+                    state[i] = 1;
+                }
+            }
+            __syncthreads();
+            for (int p = threadIdx.x; p < k; p += blockDim.x) {
+                u64 add = 0;
+                for (int w2 = 0; w2 < kWarps; ++w2) add += s_warp[w2][p];
+                s_base[p] += add;
+            }
+            __syncthreads();
+        }
+        for (int p = threadIdx.x; p < k; p += blockDim.x) s_requests[p] = s_base[p];
+        __syncthreads();
+    }
+    for (int p = threadIdx.x; p < k; p += blockDim.x) requests[p] = s_requests[p];
+}
+struct IsOpen {
+    const unsigned char* state;
+    __device__ bool operator()(i64 i) const { return state[i] == 0; }
+};
+
 struct IsPlaced {
     const unsigned char* state;
     __device__ bool operator()(i64 i) const { return state[i] == 1; }
@@ -1317,8 +1430,9 @@ struct LevelResult {
 template <class T>
 class LevelRefiner {
 public:
-    LevelRefiner(Context& c, const DGraph& g, int k, double eps, int* labels, u64* loads, u64 total, bool log)
-        : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log) {}
+    LevelRefiner(Context& c, const DGraph& g, int k, double eps, int* labels, u64* loads, u64 total, bool log,
+                 bool verify)
+        : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log), verify(verify) {}
 
     LevelResult run(bool has_known, u64 known);
 
@@ -1331,6 +1445,9 @@ private:
     u64* loads;
     u64 total;
     bool log;
+    bool verify;
+    T* check_A = nullptr;       // verify: independent rebuild of the cache
+    T* check_totals = nullptr;
 
     u64 C = 0;
     i64 n = 0;
@@ -1357,6 +1474,9 @@ private:
     // Rebuilds the cache and row totals from the labels; with directed_cut
     // also sums the directed cut (device counter, cleared by the caller).
     void build(u64* directed_cut = nullptr, const u64* gate = nullptr, u64 threshold = 0) {
+        build_into(A, totals, directed_cut, gate, threshold);
+    }
+    void build_into(T* A, T* totals, u64* directed_cut, const u64* gate, u64 threshold) {
         constexpr int W = 8;
         const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * (32 / W) * k * sizeof(T);
@@ -1434,6 +1554,23 @@ private:
             launch(k_proposals<T, decltype(width)::value, decltype(vec)::value>, grid, kThreads, 0, s(), q, a, t);
         });
     }
+    // GP_FLAG_VERIFY after every batch (incremental.cuh:846-853, 870-877):
+    // the incremental cut equals a CSR scan and the cache equals an
+    // independent rebuild.
+    void check_state(const char* cut_message) {
+        if (!verify) return;
+        if (device_cut(ctx, g, labels) != cut) fail(GP_INTERNAL, cut_message);
+        if (!check_A) {
+            check_A = ctx.persist.alloc<T>(static_cast<size_t>(n) * k);
+            check_totals = ctx.persist.alloc<T>(n);
+        }
+        build_into(check_A, check_totals, nullptr, nullptr, 0);
+        ctx.clear_scalars(1);
+        launch(k_compare_cache<T>, grid_for(n * k, kThreads), kThreads, 0, s(), static_cast<i64>(n) * k,
+               static_cast<const T*>(A), static_cast<const T*>(check_A), n, static_cast<const T*>(totals),
+               static_cast<const T*>(check_totals), ctx.dev_scalars);
+        if (ctx.read_scalars(1)[0]) fail(GP_INTERNAL, "affinity cache differs from independent CSR rebuild");
+    }
     void account(long long delta) {
         if (delta >= 0) {
             if (static_cast<u64>(delta) > cut) fail(GP_INTERNAL, "incremental cut underflow");
@@ -1467,6 +1604,7 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     if (count) {
         account(delta);
         ++revision;
+        check_state("incremental cut differs from CSR scan");
     }
     return count;
 }
@@ -1536,7 +1674,21 @@ bool LevelRefiner<T>::repair() {
                 u64* rkeys = A_.alloc<u64>(acount);
                 u64* rkeys_alt = A_.alloc<u64>(acount);
                 u64* rprefix = A_.alloc<u64>(acount);
-                for (int attempt = 0; attempt < k; ++attempt) {
+                u32* open = A_.alloc<u32>(acount);
+                u32* open_count = reinterpret_cast<u32*>(counters + 5);
+                // Small sets of open donors finish all their attempts in one block.
+                auto finish_in_block = [&](int first_attempt) {
+                    launch(k_attempts<T>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
+                           static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
+                           static_cast<const T*>(A), static_cast<const int*>(labels), g.vw, k,
+                           static_cast<const int*>(targets), static_cast<const u64*>(slack), requests, tried, state,
+                           targets, flags);
+                };
+                if (acount <= kAttemptCap) {
+                    select_if(A_, s(), acount, IsOpen{state}, WriteIdx{open}, open_count);
+                    finish_in_block(0);
+                }
+                for (int attempt = 0; attempt < k && acount > kAttemptCap; ++attempt) {
                     GP_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(u64), s()));
                     with_groups([&](auto width, auto vec) {
                         constexpr int W = decltype(width)::value;
@@ -1560,6 +1712,12 @@ bool LevelRefiner<T>::repair() {
                     launch(k_admit, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, kk, active, rprefix, base_t,
                            g.vw, slack, requests, added, tried, state, targets, flags);
                     launch(k_merge_requests, 1, 128, 0, s(), k, requests, added);
+                    // At most rcount donors remain open.
+                    if (rcount <= kAttemptCap && attempt + 1 < k) {
+                        select_if(A_, s(), acount, IsOpen{state}, WriteIdx{open}, open_count);
+                        finish_in_block(attempt + 1);
+                        break;
+                    }
                 }
                 // Movers = placed donors, in repair order.
                 select_if(A_, s(), acount, IsPlaced{state}, WriteActiveVertex{active, movers}, donor_count);
@@ -1574,6 +1732,7 @@ bool LevelRefiner<T>::repair() {
                     max_load_host = ctx.host_scalars[1];
                     account(delta);
                     ++revision;
+                    check_state("GPU rebalance cut mismatch");
                 }
             }
         }
@@ -1683,6 +1842,7 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         max_load_host = ctx.host_scalars[1];
         account(delta);
         ++revision;
+        check_state("incremental cut differs from CSR scan");
         if (delta <= 0) fail(GP_INTERNAL, "non-improving boundary group batch");
         if (max_load_host > C || cut >= best_cut) fail(GP_INTERNAL, "capacity exchange violated cut/capacity");
         best_cut = cut;
@@ -1818,7 +1978,7 @@ u64 device_cut(Context& ctx, const DGraph& g, const int* labels) {
 
 // refine_hierarchy_impl (src/refine.cu:483-730).
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
-                        int* labels, bool log) {
+                        int* labels, bool log, bool verify) {
     cudaStream_t s = ctx.stream;
     const size_t L = h.levels.size();
     std::vector<int*> level_labels(L);
@@ -1836,8 +1996,8 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
     for (int p = 0; p < k; ++p) { total += ctx.host_scalars[p]; maxload = std::max<u64>(maxload, ctx.host_scalars[p]); }
     auto refine = [&](const DGraph& g, int* lab, bool has_known, u64 known) {
         if (g.incident_bound <= 0xffffffffULL)
-            return LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log).run(has_known, known);
-        return LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log).run(has_known, known);
+            return LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
+        return LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
     };
     LevelResult res = refine(coarsest, level_labels[L - 1], false, 0);
     u64 last_cut = res.cut;
@@ -1850,6 +2010,21 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
         const size_t f = c - 1;
         const DGraph& fg = h.levels[f];
         launch(k_project, blocks_for(fg.n, 256), 256, 0, s, fg.n, h.maps[f], level_labels[c], level_labels[f]);
+        if (verify) {  // projection keeps the cut and the part weights (src/refine.cu:636-656)
+            ArenaScope vs(ctx.scratch);
+            u64* fine_loads = ctx.scratch.alloc<u64>(k);
+            GP_CUDA(cudaMemsetAsync(fine_loads, 0, sizeof(u64) * k, s));
+            launch(k_loads, std::min(blocks_for(fg.n, 256), 148 * 4), 256, sizeof(u64) * k, s, fg.n, k,
+                   static_cast<const int*>(level_labels[f]), fg.vw, fine_loads);
+            const u64 fine_cut = device_cut(ctx, fg, level_labels[f]);
+            const u64 coarse_cut = device_cut(ctx, h.levels[c], level_labels[c]);
+            std::vector<u64> a(k), b(k);
+            GP_CUDA(cudaMemcpyAsync(a.data(), fine_loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+            GP_CUDA(cudaMemcpyAsync(b.data(), loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+            GP_CUDA(cudaStreamSynchronize(s));
+            if (fine_cut != coarse_cut || fine_cut != last_cut || a != b)
+                fail(GP_INTERNAL, "GPU projection failed cut or part-weight preservation");
+        }
         GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
         GP_CUDA(cudaStreamSynchronize(s));
         maxload = 0;
@@ -1870,6 +2045,7 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
     maxload = 0;
     for (int p = 0; p < k; ++p) maxload = std::max<u64>(maxload, ctx.host_scalars[p]);
     if (maxload > cap) fail(GP_INTERNAL, "final original partition violates capacity");
+    if (verify && device_cut(ctx, h.levels[0], labels) != last_cut) fail(GP_INTERNAL, "final cut differs from CSR scan");
     out.cut = last_cut;
     out.max_load = maxload;
     return out;
