@@ -62,6 +62,12 @@ class _Stats(_C.Structure):
                 ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64)]
 
 
+class _Request(_C.Structure):
+    _fields_ = [("graph", _Csr), ("k", _C.c_int32), ("epsilon", _C.c_double), ("seed", _C.c_uint32),
+                ("flags", _C.c_uint32), ("labels_out", _C.c_void_p), ("stats", _Stats), ("status", _C.c_int),
+                ("queue_seconds", _C.c_double), ("run_seconds", _C.c_double)]
+
+
 _lib_handle = None
 
 
@@ -296,6 +302,25 @@ class Context:
                                       _C.c_uint32(seed), _C.c_uint32(flags), _C.c_void_p(labels_ptr), _C.byref(stats)))
         return Stats._from(stats)
 
+    def partition_batch(self, jobs, concurrency: int = 8, flags: int = FLAG_QUIET):
+        """gp_partition_batch over (graph, k, epsilon, seed) tuples; returns a
+        list of (labels, Stats, run_seconds) in input order.  Raises on the
+        first failed request."""
+        jobs = list(jobs)
+        requests = (_Request * max(1, len(jobs)))()
+        keep = []
+        outs = []
+        for r, (graph, k, eps, seed) in zip(requests, jobs):
+            g = graph.as_c()
+            labels = _np.empty(graph.n, _np.int32)
+            keep.append((graph, g))
+            outs.append(labels)
+            r.graph = g
+            r.k, r.epsilon, r.seed, r.flags = k, eps, seed, flags
+            r.labels_out = labels.ctypes.data_as(_C.c_void_p)
+        _check(self._lib.gp_partition_batch(self._handle, requests, _C.c_int32(len(jobs)), _C.c_int32(concurrency)))
+        return [(outs[i], Stats._from(requests[i].stats), requests[i].run_seconds) for i in range(len(jobs))]
+
     def evaluate_device(self, offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
                         edge_weights_ptr, labels_ptr: int, k: int, cut_ptr: int, loads_ptr: int,
                         stream_ptr=None) -> None:
@@ -362,6 +387,63 @@ def evaluate_device_static(offsets_ptr: int, neighbors_ptr: int, n: int, m: int,
     _check(library().gp_evaluate_device_static(_C.byref(g), _C.c_void_p(labels_ptr), _C.c_int32(k),
                                                _C.c_void_p(cut_ptr), _C.c_void_p(loads_ptr),
                                                _C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+class Server:
+    """gp_server_*: worker contexts taking requests as they arrive, admitted
+    by estimated device footprint; resident graphs via add_graph."""
+
+    def __init__(self, device: int = 0, workers: int = 8, hbm_budget_bytes: int = 0):
+        self._lib = library()
+        self._handle = _C.c_void_p()
+        self._pending = {}
+        _check(self._lib.gp_server_create(_C.c_int(device), _C.c_int32(workers), _C.c_uint64(hbm_budget_bytes),
+                                          _C.byref(self._handle)))
+        self._graphs = []
+
+    def add_graph(self, graph: Graph) -> int:
+        gid = _C.c_int32()
+        g = graph.as_c()
+        _check(self._lib.gp_server_add_graph(self._handle, _C.byref(g), _C.byref(gid)))
+        self._graphs.append(graph)
+        return gid.value
+
+    def submit(self, graph: Graph | int, k: int, epsilon: float = 1.03, seed: int = 0,
+               flags: int = FLAG_QUIET) -> int:
+        """Queue a request for a host graph or a resident graph id; returns a ticket."""
+        req = _Request()
+        resident = isinstance(graph, int)
+        host = self._graphs[graph] if resident else graph
+        g = host.as_c()
+        if not resident:
+            req.graph = g
+        labels = _np.empty(host.n, _np.int32)
+        req.k, req.epsilon, req.seed, req.flags = k, epsilon, seed, flags
+        req.labels_out = labels.ctypes.data_as(_C.c_void_p)
+        ticket = _C.c_uint64()
+        _check(self._lib.gp_server_submit(self._handle, _C.byref(req), _C.c_int32(graph if resident else -1),
+                                          _C.byref(ticket)))
+        self._pending[ticket.value] = (req, labels, host, g)
+        return ticket.value
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        """Returns (labels, Stats, queue_seconds, run_seconds); raises on failure."""
+        _check(self._lib.gp_server_wait(self._handle, _C.c_uint64(ticket), _C.c_double(timeout)))
+        req, labels, _, _ = self._pending.pop(ticket)
+        if req.status != 0:
+            raise GpartError(req.status, "request failed")
+        return labels, Stats._from(req.stats), req.queue_seconds, req.run_seconds
+
+    def close(self) -> None:
+        if self._handle:
+            self._lib.gp_server_destroy(self._handle)
+            self._handle = _C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def partition(graph: Graph, k: int, epsilon: float = 1.03, seed: int = 0, flags: int = FLAG_QUIET):

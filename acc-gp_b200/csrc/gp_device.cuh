@@ -206,6 +206,30 @@ __device__ __forceinline__ void block_atomic_max(unsigned long long* out, unsign
     if (threadIdx.x == 0 && v) atomicMax(out, v);
 }
 
+// A block's sum of one value per warp, added to a global counter without a
+// barrier at the end of the kernel: warps add into shared memory as they
+// finish, and the block's last warp adds the block's sum.  Warps of uneven
+// work then never wait for each other.  init() must be called by every
+// thread at the start of the kernel.
+struct WarpSum {
+    unsigned long long sum;
+    unsigned arrived;
+    __device__ __forceinline__ void init() {
+        if (threadIdx.x == 0) { sum = 0; arrived = 0; }
+        __syncthreads();
+    }
+    // value: the warp's total, taken from lane 0.
+    __device__ __forceinline__ void finish(unsigned long long value, unsigned long long* out) {
+        if ((threadIdx.x & 31) != 0) return;
+        if (value) atomicAdd(&sum, value);
+        __threadfence_block();
+        if (atomicAdd(&arrived, 1u) == (blockDim.x >> 5) - 1) {
+            const unsigned long long total = atomicAdd(&sum, 0ULL);
+            if (total) atomicAdd(out, total);
+        }
+    }
+};
+
 // Block-aggregated append: every `active` thread writes v to its own slot of
 // queue; one atomic on *count per block.  All threads of the block call it.
 template <class V>

@@ -14,4 +14,12 @@ const char* last_error();
 gp_status capacity_of(uint64_t total, int k, double eps, uint64_t* out);
 gp_status validate_host_csr(const gp_csr* g, bool need_positive_vw);
 
+// Worker contexts of gp_partition_batch, owned by the calling context
+// (gp_batch.cpp); accessors defined in gp_partition.cu.
+struct WorkerPool;
+WorkerPool*& worker_pool(gp_context* ctx);
+void destroy_worker_pool(WorkerPool* pool);
+int context_device(const gp_context* ctx);
+void copy_options(const gp_context* from, gp_context* to);
+
 }  // namespace gp

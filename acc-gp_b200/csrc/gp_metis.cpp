@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -76,8 +77,15 @@ gp_status metis_initial_partition(const HostCsr& g, int parts, double eps, uint3
     options[kNumbering] = 0;
     real_t upper = static_cast<real_t>(eps);
     if (upper <= 1.0f) upper = std::nextafter(1.0f, INFINITY);
-    const int status = METIS_PartGraphKway(&nn, &ncon, xadj.data(), adj.data(), vwgt.data(), nullptr, adjw.data(),
-                                           &k, nullptr, &upper, options, &objective, part.data());
+    int status;
+    {
+        // METIS seeds one process-wide random generator per call, so calls
+        // from concurrent contexts are serialised to stay reproducible.
+        static std::mutex metis_mutex;
+        std::lock_guard<std::mutex> lock(metis_mutex);
+        status = METIS_PartGraphKway(&nn, &ncon, xadj.data(), adj.data(), vwgt.data(), nullptr, adjw.data(), &k,
+                                     nullptr, &upper, options, &objective, part.data());
+    }
     if (status != kMetisOk) { error = "METIS_PartGraphKway failed: " + std::to_string(status); return GP_INTERNAL; }
     labels.resize(static_cast<size_t>(n));
     for (int64_t v = 0; v < n; ++v) {

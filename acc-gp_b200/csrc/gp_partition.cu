@@ -19,9 +19,21 @@ struct gp_context {
     gp::CoarsenOptions defaults;  // overridable per context, see gp_set_option
     bool seed_matching = true, fast_path = true;
     int cluster_size_factor = 0, fine_factor = 64, growth = 8, heavy_limit = 64;
+    gp::WorkerPool* pool = nullptr;  // batch workers, created on first use
 };
 
 namespace gp {
+
+WorkerPool*& worker_pool(gp_context* ctx) { return ctx->pool; }
+int context_device(const gp_context* ctx) { return ctx->ctx.device; }
+void copy_options(const gp_context* from, gp_context* to) {
+    to->seed_matching = from->seed_matching;
+    to->fast_path = from->fast_path;
+    to->cluster_size_factor = from->cluster_size_factor;
+    to->fine_factor = from->fine_factor;
+    to->growth = from->growth;
+    to->heavy_limit = from->heavy_limit;
+}
 
 thread_local KernelProfiler* g_profiler = nullptr;
 
@@ -325,6 +337,8 @@ gp_status gp_context_create(int device, gp_context** out) {
 
 void gp_context_destroy(gp_context* h) {
     if (!h) return;
+    destroy_worker_pool(h->pool);
+    h->pool = nullptr;
     Context& c = h->ctx;
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);

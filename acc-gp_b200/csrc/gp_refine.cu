@@ -36,6 +36,8 @@ __global__ void k_cut_chunks(DGraph g, const int* labels, u64* out) {
     block_atomic_add(out, local);
 }
 __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, u64* out) {
+    __shared__ WarpSum cut_sum;
+    cut_sum.init();
     const int lane = threadIdx.x & 31;
     u64 local = 0;
     for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
@@ -45,7 +47,7 @@ __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, cons
         for (int e = off[v] + lane; e < off[v + 1]; e += 32)
             if (labels[nbr[e]] != p) local += edge_w(ew, e);
     }
-    block_atomic_add(out, local);
+    cut_sum.finish(warp_sum(local), out);
 }
 
 __global__ void k_project(i64 n, const int* map, const int* coarse, int* fine) {
@@ -111,7 +113,9 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
                                                     const int* labels, int k, C* A, C* totals, u64* directed_cut,
                                                     const u64* gate, u64 threshold) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ WarpSum cut_sum;
     if (gate && *gate <= threshold) return;  // incremental update chosen
+    cut_sum.init();
     constexpr int N = Vectorized ? AffinityVec<C>::N : 1;
     constexpr int G = 32 / W;
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
@@ -126,7 +130,11 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         const bool valid = v < n;
         const int begin = valid ? off[v] : 0, end = valid ? off[v + 1] : 0;
         const int deg = end - begin;
-        for (int p = sub; p < k; p += W) hist[p] = 0;
+        if constexpr (Vectorized) {
+            for (int p0 = sub * N; p0 < k; p0 += W * N) *reinterpret_cast<typename AffinityVec<C>::V*>(hist + p0) = {};
+        } else {
+            for (int p = sub; p < k; p += W) hist[p] = 0;
+        }
         __syncwarp();
         if (deg <= kBuildShort) {
             for (int e = begin + sub; e < end; e += W) {
@@ -169,7 +177,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         }
         __syncwarp();
     }
-    if (directed_cut) block_atomic_add(directed_cut, cut);
+    if (directed_cut) cut_sum.finish(warp_sum(cut), directed_cut);
 }
 
 // GP_FLAG_VERIFY: the incremental cache against an independent rebuild.
@@ -446,8 +454,10 @@ template <class C>
 __global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
                          const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
                          C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold) {
+    __shared__ WarpSum delta_sum;
     const int lane = threadIdx.x & 31;
     if (gate && *gate > threshold) return;  // rebuild chosen
+    delta_sum.init();
     if (live_count) count = static_cast<i64>(*live_count);
     long long total = 0;
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
@@ -474,7 +484,7 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
             atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
         }
     }
-    block_atomic_add(delta, lane == 0 ? total : 0LL);
+    delta_sum.finish(static_cast<u64>(total), reinterpret_cast<u64*>(delta));
 }
 
 // Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,

@@ -323,6 +323,68 @@ def launch_list(args):
     ctx.close()
 
 
+def batch_jobs(gp, count, seed):
+    """The batched workload: `count` graphs, vertex counts log-uniform in
+    [1e3, 1e6]; even indices R-MAT (edge factor 8..16, a=.57 b=.19 c=.19,
+    2^round(log2 n) vertices), odd indices 2D or 3D grids of the nearest
+    shape; k uniform in {4,...,128}, halved while the capacity
+    floor(n*1.03/k) cannot hold the graph; epsilon 1.03.  Seeded synthetic
+    data."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(count):
+        n = int(10 ** rng.uniform(3, 6))
+        k = int(rng.choice([4, 8, 16, 32, 64, 128]))
+        if i % 2 == 0:
+            scale = max(10, int(round(np.log2(n))))
+            g = gp.rmat(scale, int(rng.integers(8, 17)), 0.57, 0.19, 0.19, int(rng.integers(1 << 30)))
+        elif rng.random() < 0.5:
+            w = max(2, int(round(n ** 0.5)))
+            g = gp.grid2d(w, max(2, n // w))
+        else:
+            c = max(2, int(round(n ** (1 / 3))))
+            g = gp.mesh3d(c, c, max(2, n // (c * c)))
+        while k > 2 and (g.n * 103) // (100 * k) * k < g.n:  # floor(n*1.03/k)*k must hold n
+            k //= 2
+        jobs.append((g, k, 1.03, 0))
+    return jobs
+
+
+def run_batch(args):
+    """Batched form: the same graphs partitioned one after another and as one
+    gp_partition_batch call; every batched result is checked against the
+    serial one.  Prints one JSON line (graphs/s)."""
+    import torch
+    gp = load_package()
+    t0 = time.perf_counter()
+    jobs = batch_jobs(gp, args.batch_graphs, 0)
+    gen_s = time.perf_counter() - t0
+    ctx = gp.Context(0)
+    warm = jobs[: min(8, len(jobs))]
+    ctx.partition_batch(warm, concurrency=args.concurrency)
+    for g, k, eps, seed in warm:
+        ctx.partition(g, k, eps, seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    serial = [ctx.partition(g, k, eps, seed) for g, k, eps, seed in jobs]
+    serial_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    batched = ctx.partition_batch(jobs, concurrency=args.concurrency)
+    batch_s = time.perf_counter() - t0
+    identical = all((a[0] == b[0]).all() and a[1].edge_cut == b[1].edge_cut for a, b in zip(serial, batched))
+    ok = all(gp.verify(g, b[0], k, eps)["capacity_ok"] for (g, k, eps, _), b in zip(jobs, batched))
+    print(json.dumps({
+        "metric": "batched graphs/s", "value": len(jobs) / batch_s, "unit": "graphs/s", "n_gpus": 1,
+        "serial_value": len(jobs) / serial_s, "speedup_vs_serial": serial_s / batch_s,
+        "graphs": len(jobs), "concurrency": args.concurrency, "identical_to_serial": identical,
+        "verified": ok, "total_vertices": int(sum(g.n for g, _, _, _ in jobs)),
+        "total_entries": int(sum(g.m for g, _, _, _ in jobs)), "generation_s": gen_s,
+        "data": "synthetic", "config": {"workload": "batch512_uneven", "k": "uniform {4..128}", "epsilon": 1.03},
+    }), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,11 +394,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
+    ap.add_argument("--workload", choices=["rmat22", "batch"], default="rmat22",
+                    help="batch: the uneven 512-graph set, serial vs gp_partition_batch")
+    ap.add_argument("--batch-graphs", type=int, default=512)
+    ap.add_argument("--concurrency", type=int, default=16)
     ap.add_argument("--scale", type=int, default=22,
                     help="R-MAT scale of the --launch-list graph (smaller cases for ncu captures)")
     args = ap.parse_args()
     if args.launch_list:
         launch_list(args)
+    elif args.workload == "batch":
+        run_batch(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -145,6 +145,57 @@ gp_status gp_evaluate_device_static(const gp_csr* graph, const int32_t* labels,
                                     int32_t k, uint64_t* cut_out,
                                     uint64_t* loads_out, void* stream);
 
+/* ---- many graphs on one GPU ---- */
+
+/* One partition request of a batch or a server.  `graph` is a host CSR
+ * (for a server request naming a resident graph it is ignored); labels_out
+ * is a host buffer of n int32.  The library fills stats, status and the two
+ * times: queue_seconds (submit -> start, servers only) and run_seconds
+ * (start -> labels in labels_out). */
+typedef struct gp_request {
+    gp_csr graph;
+    int32_t k;
+    double epsilon;
+    uint32_t seed;
+    uint32_t flags;
+    int32_t* labels_out;
+    gp_stats stats;
+    gp_status status;
+    double queue_seconds;
+    double run_seconds;
+} gp_request;
+
+/* Partition `count` independent graphs of any sizes on the context's GPU,
+ * up to `concurrency` at a time (1..64; each in-flight graph has its own
+ * stream and device arena, kept by the context for later batches), largest
+ * first.  No counterpart in the reference, which partitions one graph per
+ * process (app/partition_main.cu); the batched form of that path.  Every
+ * result is identical to gp_partition of the same request alone.  Returns
+ * GP_OK when every request succeeded, else the status of the first failed
+ * request (per-request status in requests[i].status). */
+gp_status gp_partition_batch(gp_context* ctx, gp_request* requests, int32_t count, int32_t concurrency);
+
+/* A partition server: `workers` threads, each with its own context on
+ * `device`, take requests as they arrive.  A request is admitted when its
+ * estimated device footprint fits in what is left of hbm_budget_bytes
+ * (0: no limit) among the requests running; smaller requests may pass a
+ * waiting larger one.  Graphs added with gp_server_add_graph stay resident
+ * on the device and are partitioned without an upload.  No counterpart in
+ * the reference. */
+typedef struct gp_server gp_server;
+gp_status gp_server_create(int device, int32_t workers, uint64_t hbm_budget_bytes, gp_server** out);
+/* Uploads a host CSR once; requests name it by *graph_id. */
+gp_status gp_server_add_graph(gp_server* server, const gp_csr* graph, int32_t* graph_id);
+/* Queues a request (graph_id -1: request->graph is a host CSR).  The request
+ * and its buffers must stay valid until gp_server_wait returns for it. */
+gp_status gp_server_submit(gp_server* server, gp_request* request, int32_t graph_id, uint64_t* ticket);
+/* Waits up to timeout_seconds (< 0: no limit) for a request; returns
+ * GP_DEVICE_TIMEOUT if it is still running, else GP_OK with the request's
+ * own status in request->status. */
+gp_status gp_server_wait(gp_server* server, uint64_t ticket, double timeout_seconds);
+/* Finishes every queued request, then stops the workers. */
+void gp_server_destroy(gp_server* server);
+
 /* Kernel timing for measurement: between begin and end, every launch of a
  * kernel whose name contains `kernel_substring` is bracketed by CUDA events
  * on the stream it runs on; end returns the launch count, the summed device

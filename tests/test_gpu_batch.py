@@ -1,0 +1,81 @@
+"""Many graphs on one GPU: gp_partition_batch and the partition server.
+
+Every result must equal the same request partitioned alone (the same
+deterministic single-graph path runs on each worker context), and the
+verifier must accept it."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_graphs(gp):
+    """Uneven sizes and kinds: grids, meshes, R-MAT (one weighted)."""
+    return [
+        (gp.grid2d(40, 30), 4, 1.03, 0),
+        (gp.rmat(14, 8, 0.57, 0.19, 0.19, 1), 64, 1.03, 0),
+        (gp.mesh3d(12, 10, 9), 16, 1.05, 3),
+        (gp.rmat(16, 16, 0.57, 0.19, 0.19, 2), 128, 1.03, 0),
+        (gp.grid2d(256, 256), 8, 1.03, 0),
+        (gp.with_weights(gp.rmat(13, 12, 0.57, 0.19, 0.19, 4), 5, (1, 16), (1, 64)), 37, 1.01, 9),
+        (gp.rmat(12, 16, 0.57, 0.19, 0.19, 7), 2, 1.03, 1),
+        (gp.mesh3d(30, 30, 30), 32, 1.03, 0),
+        (gp.grid2d(7, 500), 8, 1.03, 2),
+        (gp.rmat(17, 10, 0.57, 0.19, 0.19, 8), 64, 1.03, 0),
+    ]
+
+
+def test_batch_equals_single_calls(gp, ctx):
+    jobs = mixed_graphs(gp)
+    alone = [ctx.partition(g, k, eps, seed) for g, k, eps, seed in jobs]
+    batched = ctx.partition_batch(jobs, concurrency=6)
+    for (g, k, eps, _), (labels, st), (blabels, bst, run_s) in zip(jobs, alone, batched):
+        np.testing.assert_array_equal(blabels, labels)
+        assert bst.edge_cut == st.edge_cut and run_s > 0
+        verdict = gp.verify(g, blabels, k, eps)
+        assert verdict["capacity_ok"] and verdict["cut"] == bst.edge_cut
+
+
+def test_batch_reports_failed_request(gp, ctx):
+    jobs = [(gp.grid2d(20, 20), 4, 1.03, 0), (gp.grid2d(3, 3), 16, 2.0, 0)]
+    with pytest.raises(gp.GpartError) as e:
+        ctx.partition_batch(jobs, concurrency=2)
+    assert "request 1" in str(e.value)
+
+
+def test_server_results_same_alone_and_in_mix(gp, ctx):
+    jobs = mixed_graphs(gp)
+    alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
+    with gp.Server(0, workers=4) as server:
+        resident = server.add_graph(jobs[3][0])
+        tickets = []
+
+        def arrive():
+            rng = np.random.default_rng(0)
+            for i, (g, k, eps, seed) in enumerate(jobs):
+                graph = resident if i == 3 else g
+                tickets.append((i, server.submit(graph, k, eps, seed)))
+                time.sleep(float(rng.exponential(0.004)))
+
+        producer = threading.Thread(target=arrive)
+        producer.start()
+        producer.join()
+        for i, ticket in tickets:
+            labels, st, queued, run = server.wait(ticket)
+            np.testing.assert_array_equal(labels, alone[i])
+            assert run > 0 and queued >= 0
+
+
+def test_server_footprint_budget_still_completes(gp, ctx):
+    """With a budget smaller than any request, requests run one at a time
+    (an idle server always admits the next one) and all complete."""
+    jobs = mixed_graphs(gp)[:4]
+    alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
+    with gp.Server(0, workers=3, hbm_budget_bytes=1) as server:
+        tickets = [server.submit(g, k, eps, seed) for g, k, eps, seed in jobs]
+        for t, expect in zip(tickets, alone):
+            labels, _, _, _ = server.wait(t, timeout=300.0)
+            np.testing.assert_array_equal(labels, expect)

@@ -131,3 +131,39 @@ def test_evaluate_device_matches_verifier(gp, ctx):
     verdict = gp.verify(g, labels, k, 2.0)
     assert int(cut.item()) == verdict["cut"]
     assert [int(x) for x in loads.cpu()] == verdict["loads"]
+
+
+@pytest.mark.parametrize("case", ["rmat", "weighted_mesh"])
+def test_verify_flag_checks_pass_and_change_nothing(gp, ctx, case):
+    """GP_FLAG_VERIFY (the reference's --verify) runs every strict check and
+    leaves the result unchanged."""
+    if case == "rmat":
+        g, k = gp.rmat(16, 16, 0.57, 0.19, 0.19, 3), 64
+    else:
+        g, k = gp.with_weights(gp.mesh3d(20, 20, 20), 9, (1, 4), (1, 16)), 32
+    plain, sp = ctx.partition(g, k, 1.03, 0)
+    checked, sc = ctx.partition(g, k, 1.03, 0, gp.FLAG_QUIET | gp.FLAG_VERIFY)
+    np.testing.assert_array_equal(plain, checked)
+    assert sc.edge_cut == sp.edge_cut
+
+
+def test_verify_flag_rejects_one_way_edges(gp, ctx):
+    g = gp.grid2d(20, 20)
+    off, nbr = g.offsets.copy(), g.neighbors.copy()
+    # Redirect one directed entry of vertex 0 to another valid vertex: the
+    # reverse entry is missing, which only the strict check detects.
+    nbr[off[0]] = 399
+    bad = gp.Graph(off, nbr, None)
+    with pytest.raises(gp.GpartError) as e:
+        ctx.partition(bad, 4, 1.03, 0, gp.FLAG_QUIET | gp.FLAG_VERIFY)
+    assert e.value.status == 1 and "bidirectional" in str(e.value)
+
+
+def test_verify_flag_rejects_unequal_reverse_weights(gp, ctx):
+    g = gp.with_weights(gp.grid2d(16, 16), 1, (1, 1), (1, 9))
+    ew = g.edge_weights.copy()
+    ew[g.offsets[5]] += 1
+    bad = gp.Graph(g.offsets, g.neighbors, g.vertex_weights, ew)
+    with pytest.raises(gp.GpartError) as e:
+        ctx.partition(bad, 4, 1.03, 0, gp.FLAG_QUIET | gp.FLAG_VERIFY)
+    assert e.value.status == 1 and "reverse edge weights differ" in str(e.value)
