@@ -1005,13 +1005,14 @@ __global__ void k_copy_chunks(DGraph g, const int* raw_off, const int* raw_t, co
 
 __global__ void k_heavy_counts(i64 n, const int* off, u64* sc) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    u64 rows = 0, chunks = 0;
+    u64 rows = 0, chunks = 0, entries = 0;
     if (v < n) {
         const int d = off[v + 1] - off[v];
-        if (d > kHeavyRow) { rows = 1; chunks = (d + kChunk - 1) / kChunk; }
+        if (d > kHeavyRow) { rows = 1; chunks = (d + kChunk - 1) / kChunk; entries = d; }
     }
     block_atomic_add(sc, rows);
     block_atomic_add(sc + 1, chunks);
+    block_atomic_add(sc + 2, entries);
 }
 struct IsHeavyRow {
     const int* off;
@@ -1469,12 +1470,14 @@ void build_chunks(Context& ctx, DGraph& g) {
     g.heavy = nullptr;
     g.heavy_count = 0;
     g.chunks = 0;
+    g.heavy_entries = 0;
     if (g.n <= 0) return;
-    ctx.clear_scalars(2);
+    ctx.clear_scalars(3);
     launch(k_heavy_counts, blocks_for(g.n, kThreads), kThreads, 0, s, g.n, g.off, ctx.dev_scalars);
-    const u64* sc = ctx.read_scalars(2);
+    const u64* sc = ctx.read_scalars(3);
     g.heavy_count = static_cast<i64>(sc[0]);
     g.chunks = static_cast<i64>(sc[1]);
+    g.heavy_entries = static_cast<i64>(sc[2]);
     if (!g.heavy_count) return;
     g.heavy = ctx.persist.alloc<int>(g.heavy_count);
     g.chunk_row = ctx.persist.alloc<int>(g.chunks);

@@ -46,6 +46,9 @@ struct KernelProfiler {
     size_t used = 0;
     bool last_timed = false;
     double bytes = 0;
+    // Kernels whose work is decided on the device add their algorithmic
+    // bytes here when they run (see work_counter).
+    unsigned long long* device_bytes = nullptr;
     bool matches(const void* kernel);
     void before(cudaStream_t s);
     void after(cudaStream_t s);
@@ -55,6 +58,13 @@ extern thread_local KernelProfiler* g_profiler;
 
 inline void account_bytes(double bytes) {
     if (g_profiler && g_profiler->last_timed) g_profiler->bytes += bytes;
+}
+// Device counter for the algorithmic bytes of `kernel` when it is profiled,
+// else nullptr; the kernel adds its bytes only if it does its work.
+template <class K>
+inline unsigned long long* work_counter(K kernel) {
+    return g_profiler && g_profiler->device_bytes && g_profiler->matches(reinterpret_cast<const void*>(kernel))
+               ? g_profiler->device_bytes : nullptr;
 }
 
 template <class... Params, class... Args>

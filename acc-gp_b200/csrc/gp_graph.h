@@ -35,6 +35,7 @@ struct DGraph {
     int* chunk_hidx = nullptr;  // index of the chunk's row in `heavy`
     int* chunk_begin = nullptr;
     i64 chunks = 0;
+    i64 heavy_entries = 0;  // CSR entries in heavy rows
 };
 
 // Chunk-parallel loop body helpers: the chunk's edge range.

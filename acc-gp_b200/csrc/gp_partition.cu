@@ -5,6 +5,8 @@
 #include "gp_primitives.cuh"
 
 #include <algorithm>
+#include <cstdlib>
+#include <cxxabi.h>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -42,7 +44,16 @@ bool KernelProfiler::matches(const void* kernel) {
         if (entry.first == kernel) return entry.second;
     const char* name = nullptr;
     bool hit = false;
-    if (cudaFuncGetName(&name, kernel) == cudaSuccess && name) hit = std::strstr(name, pattern.c_str()) != nullptr;
+    if (cudaFuncGetName(&name, kernel) == cudaSuccess && name) {
+        // Match the pattern against the symbol and its demangled form.
+        hit = std::strstr(name, pattern.c_str()) != nullptr;
+        int status = 0;
+        char* readable = abi::__cxa_demangle(name, nullptr, nullptr, &status);
+        if (readable) {
+            hit = hit || std::strstr(readable, pattern.c_str()) != nullptr;
+            std::free(readable);
+        }
+    }
     cache.emplace_back(kernel, hit);
     return hit;
 }
@@ -340,6 +351,10 @@ void gp_context_destroy(gp_context* h) {
     destroy_worker_pool(h->pool);
     h->pool = nullptr;
     Context& c = h->ctx;
+    if (h->profiler.device_bytes) {
+        cudaSetDevice(c.device);
+        cudaFree(h->profiler.device_bytes);
+    }
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     c.persist.reset_device();
@@ -383,8 +398,13 @@ gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring) {
     ctx->profiler.used = 0;
     ctx->profiler.bytes = 0;
     ctx->profiler.last_timed = false;
-    g_profiler = &ctx->profiler;
-    return GP_OK;
+    return guarded([&]() -> gp_status {
+        GP_CUDA(cudaSetDevice(ctx->ctx.device));
+        if (!ctx->profiler.device_bytes) GP_CUDA(cudaMalloc(&ctx->profiler.device_bytes, sizeof(unsigned long long)));
+        GP_CUDA(cudaMemset(ctx->profiler.device_bytes, 0, sizeof(unsigned long long)));
+        g_profiler = &ctx->profiler;
+        return GP_OK;
+    });
 }
 
 gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms, double* algorithmic_bytes) {
@@ -401,7 +421,10 @@ gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms, 
         }
         if (launches) *launches = p.used;
         if (total_ms) *total_ms = ms;
-        if (algorithmic_bytes) *algorithmic_bytes = p.bytes;
+        unsigned long long device_bytes = 0;
+        if (p.device_bytes)
+            GP_CUDA(cudaMemcpy(&device_bytes, p.device_bytes, sizeof(device_bytes), cudaMemcpyDeviceToHost));
+        if (algorithmic_bytes) *algorithmic_bytes = p.bytes + static_cast<double>(device_bytes);
         p.used = 0;
         p.bytes = 0;
         return GP_OK;

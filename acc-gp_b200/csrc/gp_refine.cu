@@ -101,6 +101,32 @@ template <class C> struct AffinityVec;
 template <> struct AffinityVec<u32> { using V = uint4; static constexpr int N = 4; };
 template <> struct AffinityVec<u64> { using V = ulonglong2; static constexpr int N = 2; };
 
+// Adds the entries [begin, end) of row v to a shared histogram by part,
+// `stride` lanes apart starting at `first`, four entries per lane at a time
+// so that four neighbour and four label loads are in flight together.
+template <class C>
+__device__ __forceinline__ void accumulate_row(const int* nbr, const u32* ew, const int* labels, int v, int first,
+                                               int end, int stride, C* hist) {
+    constexpr int kUnroll = 4;
+    for (int e0 = first; e0 < end; e0 += kUnroll * stride) {
+        int u[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            const int e = e0 + j * stride;
+            u[j] = e < end ? nbr[e] : v;
+        }
+        int part[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) part[j] = u[j] != v ? labels[u[j]] : -1;
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            // part >= 0 only for entries inside the row
+            const C w = part[j] >= 0 ? static_cast<C>(edge_w(ew, e0 + j * stride)) : C(0);
+            if (part[j] >= 0) atomicAdd(hist + part[j], w);
+        }
+    }
+}
+
 // incremental_build_affinity (incremental.cuh:61-140), dense layout.  A warp
 // builds 32/W rows at a time, W lanes per row, each row's k-wide histogram in
 // shared memory; rows longer than kBuildShort entries are accumulated by the
@@ -111,10 +137,11 @@ constexpr int kBuildShort = 64;
 template <class C, int W, bool Vectorized>
 __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const int* nbr, const u32* ew,
                                                     const int* labels, int k, C* A, C* totals, u64* directed_cut,
-                                                    const u64* gate, u64 threshold) {
+                                                    const u64* gate, u64 threshold, u64* work, u64 work_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ WarpSum cut_sum;
     if (gate && *gate <= threshold) return;  // incremental update chosen
+    if (work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(work, work_bytes);
     cut_sum.init();
     constexpr int N = Vectorized ? AffinityVec<C>::N : 1;
     constexpr int G = 32 / W;
@@ -137,10 +164,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         }
         __syncwarp();
         if (deg <= kBuildShort) {
-            for (int e = begin + sub; e < end; e += W) {
-                const int u = nbr[e];
-                if (u != v) atomicAdd(hist + labels[u], static_cast<C>(edge_w(ew, e)));
-            }
+            accumulate_row(nbr, ew, labels, static_cast<int>(v), begin + sub, end, W, hist);
         }
         for (unsigned rest = __ballot_sync(0xffffffffu, deg > kBuildShort && deg <= kHeavyRow) & leaders; rest;
              rest &= rest - 1) {
@@ -148,10 +172,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
             const int vv = static_cast<int>(base) + leader / W;
             const int b = __shfl_sync(0xffffffffu, begin, leader), e_end = __shfl_sync(0xffffffffu, end, leader);
             C* h = warp_hist + (leader / W) * k;
-            for (int e = b + lane; e < e_end; e += 32) {
-                const int u = nbr[e];
-                if (u != vv) atomicAdd(h + labels[u], static_cast<C>(edge_w(ew, e)));
-            }
+            accumulate_row(nbr, ew, labels, vv, b + lane, e_end, 32, h);
         }
         __syncwarp();
         C total = 0;
@@ -370,16 +391,21 @@ __global__ void k_filter(LpParams q) {
         if (q.off[v + 1] - q.off[v] > kHeavyRow) continue;  // k_filter_chunks / k_filter_finish
         const int s = q.labels[v], t = q.targets[v];
         const long long gain = q.gains[v];
+        const int end = q.off[v + 1];
         long long corr = 0;
-        for (int e = q.off[v] + lane; e < q.off[v + 1]; e += 32) {
-            const int u = q.nbr[e];
-            if (u == v) continue;
-            const int tu = q.targets[u];
-            if (tu < 0) continue;
-            const long long gu = q.gains[u];
-            if (!(gu > gain || (gu == gain && u < v))) continue;
-            const int lu = q.labels[u];
-            corr += static_cast<long long>(edge_w(q.ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+        // Two entries per lane at a time; the neighbour's target, gain and
+        // label are gathered together.
+        for (int e0 = q.off[v] + lane; e0 < end; e0 += 64) {
+            const int e1 = e0 + 32;
+            const int u0 = q.nbr[e0], u1 = e1 < end ? q.nbr[e1] : v;
+            const int t0 = q.targets[u0], l0 = q.labels[u0];
+            const long long g0 = q.gains[u0];
+            const int t1 = u1 != v ? q.targets[u1] : -1, l1 = u1 != v ? q.labels[u1] : 0;
+            const long long g1 = u1 != v ? q.gains[u1] : 0;
+            if (u0 != v && t0 >= 0 && (g0 > gain || (g0 == gain && u0 < v)))
+                corr += static_cast<long long>(edge_w(q.ew, e0)) * ((t0 == t) - (t0 == s) - (l0 == t) + (l0 == s));
+            if (u1 != v && t1 >= 0 && (g1 > gain || (g1 == gain && u1 < v)))
+                corr += static_cast<long long>(edge_w(q.ew, e1)) * ((t1 == t) - (t1 == s) - (l1 == t) + (l1 == s));
         }
         corr = warp_sum(corr);
         if (lane == 0) {
@@ -465,17 +491,30 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
         const int v = movers[i];
         if (off[v + 1] - off[v] > kHeavyRow) continue;  // k_update_chunks
         const int s = labels[v], t = targets[v];
+        const int end = off[v + 1];
         long long gain = 0;
-        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
-            const int u = nbr[e];
-            if (u == v) continue;
-            const int old = labels[u];
-            const bool moves = flags[u] != 0;
-            const int nw = moves ? targets[u] : old;
-            const u32 w = edge_w(ew, e);
-            atomicAdd(A + static_cast<i64>(u) * k + s, static_cast<C>(0) - static_cast<C>(w));
-            atomicAdd(A + static_cast<i64>(u) * k + t, static_cast<C>(w));
-            if (!moves || u > v) gain += static_cast<long long>(w) * ((s != old) - (t != nw));
+        // Two entries per lane at a time: their gathers are in flight together.
+        for (int e0 = off[v] + lane; e0 < end; e0 += 64) {
+            const int e1 = e0 + 32;
+            const int u0 = nbr[e0], u1 = e1 < end ? nbr[e1] : v;
+            const int old0 = labels[u0], f0 = flags[u0], t0 = targets[u0];
+            const int old1 = u1 != v ? labels[u1] : 0, f1 = u1 != v ? flags[u1] : 0, t1 = u1 != v ? targets[u1] : 0;
+            if (u0 != v) {
+                const u32 w = edge_w(ew, e0);
+                const bool moves = f0 != 0;
+                const int nw = moves ? t0 : old0;
+                atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
+                if (!moves || u0 > v) gain += static_cast<long long>(w) * ((s != old0) - (t != nw));
+            }
+            if (u1 != v) {
+                const u32 w = edge_w(ew, e1);
+                const bool moves = f1 != 0;
+                const int nw = moves ? t1 : old1;
+                atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
+                if (!moves || u1 > v) gain += static_cast<long long>(w) * ((s != old1) - (t != nw));
+            }
         }
         gain = warp_sum(gain);
         total += gain;
@@ -1491,12 +1530,18 @@ private:
         const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * (32 / W) * k * sizeof(T);
         const int grid = grid_for(n * W, kThreads);
+        // Algorithmic bytes: offsets, the light rows' neighbours (weights)
+        // and label gathers, every row of the cache and its total written,
+        // each row's own label.
+        const u64 light = static_cast<u64>(g.m - g.heavy_entries);
+        const u64 bytes = 4ULL * (n + 1) + light * (8ULL + (g.ew ? 4ULL : 0ULL)) +
+                          static_cast<u64>(n) * (static_cast<u64>(k) + 1) * sizeof(T) + 4ULL * n;
         if (vec)
             launch(k_build<T, W, true>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes);
         else
             launch(k_build<T, W, false>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes);
         if (g.chunks) {
             launch(k_build_chunks<T>, static_cast<int>(g.chunks), 256, sizeof(T) * k, s(), g,
                    static_cast<const int*>(labels), k, A, totals, gate, threshold);
@@ -1901,7 +1946,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     // An entry-by-entry update touches two random cache counters per entry
     // (about 128 bytes of DRAM traffic); a rebuild writes the whole cache and
     // reads the CSR once.
-    rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) / 128;
+    rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) / 100;
     GP_CUDA(cudaMemsetAsync(counters + 7, 0, sizeof(u64), s()));
     build(has_known ? nullptr : counters + 7);
     launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);

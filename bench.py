@@ -36,13 +36,15 @@ WORKLOAD = dict(workload="rmat22_k64", graph="R-MAT scale 22, edge factor 16, a=
                 k=64, epsilon=1.03, seed=0, vertices=4194304)
 METRIC = "partition ms & batched graphs/s at k=64 ε=1.03; cut vs ref; HBM GB/s"
 # Kernel whose roofline fraction is reported: the largest share of device
-# time in the ncu launch list of this workload (profiles/).  Its launch site
-# reports the algorithmic bytes of every launch (keys and values read once
-# and written once per pass, plus the tile histogram).
-DOMINANT_KERNEL = "k_radix_downsweep"
+# time in the ncu launch list of this workload (profiles/), the affinity-cache
+# build of the refinement.  It reports its algorithmic bytes from the device
+# when it runs (a build the update path made unnecessary adds nothing):
+# offsets, light-row neighbours and label gathers, the k-wide cache rows and
+# totals written, each row's own label.
+DOMINANT_KERNEL = "k_build<"
 # ncu DRAM bytes (read + write) per algorithmic byte of that kernel, from the
 # capture summarised in this file ("traffic_per_algorithmic_byte: x").
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_radix_downsweep_rmat.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_build_rmat20_k64.md")
 
 
 def load_package():
@@ -216,7 +218,7 @@ def run_ours(args):
         alg = dom_bytes / dom_launches
         achieved = alg / (per_launch_ms * 1e-3) / 1e9
         ratio = traffic_ratio()
-        roof = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
+        roof = {"bound": "hbm", "kernel": DOMINANT_KERNEL.rstrip("<"), "achieved": achieved, "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": alg * ratio if ratio else None,
                 "algorithmic_bytes_per_launch": alg, "launches": dom_launches, "avg_launch_ms": per_launch_ms,
@@ -385,6 +387,71 @@ def run_batch(args):
     ctx.close()
 
 
+def run_serving(args):
+    """Serving form: a Poisson stream of requests (mean args.rate per second)
+    against a gp_server whose graphs are resident on the device.  The graph
+    pool spans vertex counts log-uniform in [1e4, 4e6] (R-MAT edge factor
+    12, a=.57 b=.19 c=.19, vertex weights U[1,16], edge weights U[1,64]);
+    each request draws a pool graph, k uniform in 2..128 (halved while the
+    capacity cannot hold the graph), epsilon in {1.01, 1.03, 1.05} and a
+    seed.  Reports p50/p99 latency (submit -> labels in host memory) and
+    throughput; a sample of results is checked against the same request
+    partitioned alone."""
+    import numpy as np
+    gp = load_package()
+    rng = np.random.default_rng(1)
+    pool = []
+    for i in range(args.pool_graphs):
+        scale = int(round(np.log2(10 ** rng.uniform(4, np.log10(4e6)))))
+        g = gp.with_weights(gp.rmat(scale, 12, 0.57, 0.19, 0.19, 100 + i), 7 + i, (1, 16), (1, 64))
+        pool.append(g)
+    requests = []
+    for _ in range(args.requests):
+        gi = int(rng.integers(len(pool)))
+        k = int(rng.integers(2, 129))
+        eps = float(rng.choice([1.01, 1.03, 1.05]))
+        total = int(pool[gi].vertex_weights.sum(dtype=np.uint64))
+        while k > 2 and int(total * eps) // k * k < total:
+            k //= 2
+        requests.append((gi, k, eps, int(rng.integers(1 << 30))))
+    gaps = rng.exponential(1.0 / args.rate, size=len(requests))
+    with gp.Server(0, workers=args.concurrency, hbm_budget_bytes=int(args.hbm_budget_gb * (1 << 30))) as server:
+        ids = [server.add_graph(g) for g in pool]
+        warm = [server.submit(ids[i], 8, 1.03, 0) for i in range(len(pool))]
+        for t in warm:
+            server.wait(t)
+        tickets = []
+        t0 = time.perf_counter()
+        due = t0
+        for (gi, k, eps, seed), gap in zip(requests, gaps):
+            due += gap
+            delay = due - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append((time.perf_counter(), server.submit(ids[gi], k, eps, seed)))
+        results = []
+        for (submitted, t), req in zip(tickets, requests):
+            labels, st, queued, run = server.wait(t)
+            results.append((labels, st, queued + run))
+        wall = time.perf_counter() - t0
+    lat = np.array([r[2] for r in results]) * 1e3
+    sample = list(range(0, len(requests), max(1, len(requests) // 12)))
+    same = True
+    with gp.Context(0) as ctx:
+        for i in sample:
+            gi, k, eps, seed = requests[i]
+            alone, _ = ctx.partition(pool[gi], k, eps, seed)
+            same &= bool((alone == results[i][0]).all())
+    print(json.dumps({
+        "metric": "serving latency and throughput", "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)), "throughput_req_s": len(requests) / wall,
+        "offered_rate_req_s": args.rate, "requests": len(requests), "workers": args.concurrency,
+        "pool_graphs": len(pool), "pool_vertices": [int(g.n) for g in pool],
+        "sample_identical_to_alone": same, "data": "synthetic",
+        "config": {"workload": "serving_poisson", "k": "uniform 2..128", "epsilon": [1.01, 1.03, 1.05]},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,8 +461,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
-    ap.add_argument("--workload", choices=["rmat22", "batch"], default="rmat22",
-                    help="batch: the uneven 512-graph set, serial vs gp_partition_batch")
+    ap.add_argument("--workload", choices=["rmat22", "batch", "serving"], default="rmat22",
+                    help="batch: the uneven 512-graph set, serial vs gp_partition_batch; "
+                         "serving: Poisson requests against a gp_server")
+    ap.add_argument("--requests", type=int, default=1000)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--pool-graphs", type=int, default=16)
+    ap.add_argument("--hbm-budget-gb", type=float, default=120.0)
     ap.add_argument("--batch-graphs", type=int, default=512)
     ap.add_argument("--concurrency", type=int, default=16)
     ap.add_argument("--scale", type=int, default=22,
@@ -405,6 +477,8 @@ def main():
         launch_list(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serving":
+        run_serving(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
