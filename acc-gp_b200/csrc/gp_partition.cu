@@ -167,7 +167,11 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     if (in->n > std::numeric_limits<int>::max() || in->m > std::numeric_limits<int>::max() || in->m < 0)
         fail(GP_INVALID_ARGUMENT, "graph exceeds supported 32-bit CSR limits; dataset excluded");
     if (!device_input) {
-        if (gp_status s = validate_host_csr(in, true); s != GP_OK) fail(s, last_error());
+        // O(1) shape checks here; monotone offsets, neighbour ranges and
+        // positive weights are checked on the device after the upload (the
+        // same messages), not by a serial scan of the host arrays.
+        if (!in->offsets || (in->m > 0 && !in->neighbors)) fail(GP_INVALID_ARGUMENT, "graph arrays must not be NULL");
+        if (in->offsets[0] != 0 || in->offsets[in->n] != in->m) fail(GP_INVALID_ARGUMENT, "invalid weighted CSR shape");
     }
     GP_CUDA(cudaSetDevice(ctx.device));
     cudaStream_t s = ctx.stream;
