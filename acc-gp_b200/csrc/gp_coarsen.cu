@@ -27,7 +27,9 @@ constexpr int kLargeDegree = kHeavyRow;   // rows above use a chunked global tab
 constexpr int kMediumHash = 512;          // SCLP_MEDIUM_HASH_SIZE
 constexpr int kLargeHash = 2 * kHeavyRow; // shared-memory table of the large class
 constexpr int kSegment = 4096;            // table slots summarised per block
-constexpr int kBlockSortRow = 4096;       // contraction: block bitonic sort limit
+constexpr int kBlockSortRow = 4096;       // contraction: one 256-thread block sorts rows up to this
+constexpr int kBigSortRow = 8192;         // one 1024-thread block (dynamic shared memory) up to this
+constexpr int kBigSortThreads = 1024;
 constexpr int kMediumWarps = 4;
 
 // ---------------------------------------------------------------- metadata
@@ -455,8 +457,10 @@ __global__ void k_affinity_heavy_insert(DGraph g, const u64* table_off, int* key
         }
     }
 }
+// Also empties the slots it read, so the tables start the next round clean
+// without clearing them all.
 __global__ void k_affinity_heavy_summary(const int* heavy, const int* seg_hidx, const int* seg_index,
-                                         const u64* table_off, const int* keys, const u64* vals, RoundParams p,
+                                         const u64* table_off, int* keys, u64* vals, RoundParams p,
                                          Summary* partial) {
     __shared__ Summary warp_part[8];
     const int sg = blockIdx.x, h = seg_hidx[sg], v = heavy[h];
@@ -466,7 +470,11 @@ __global__ void k_affinity_heavy_summary(const int* heavy, const int* seg_hidx, 
     Summary sm{0, 0, 0, 0};
     for (int i = threadIdx.x; i < kSegment; i += blockDim.x) {
         const int c = keys[base + i];
-        if (c >= 0) consider(p, sm, v, src, c, vals[base + i]);
+        if (c >= 0) {
+            consider(p, sm, v, src, c, vals[base + i]);
+            keys[base + i] = -1;
+            vals[base + i] = 0;
+        }
     }
     reduce_summary<32>(sm);
     if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sm;
@@ -758,14 +766,15 @@ __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int*
     }
 }
 
-// Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 larger.
+// Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 <= 8192, 4 larger;
+// sc[5] counts the records of class 4.
 __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u64* sc) {
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int r = c < nc ? raw[c] : 0;
-    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kBlockSortRow ? 2 : 3;
+    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kBlockSortRow ? 2 : r <= kBigSortRow ? 3 : 4;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) block_append(static_cast<int>(c), cls == k, lists + k * stride, sc + k);
-    block_atomic_add(sc + 4, cls == 3 ? static_cast<u64>(r) : 0ULL);
+    for (int k = 0; k < 5; ++k) block_append(static_cast<int>(c), cls == k, lists + k * stride, sc + k);
+    block_atomic_add(sc + 5, cls == 4 ? static_cast<u64>(r) : 0ULL);
 }
 
 // contraction_warp_sort / contraction_sort_row (contraction_rows.cuh:40-116):
@@ -861,43 +870,58 @@ __global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off,
 // memory (8-bit digits over the bits of nc; dropped intra-cluster entries
 // take the key nc and sort last), then one thread per run of equal keys sums
 // it and writes the unique run back at the row's start.
-__global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
-                                                         int* ucount, int nc, int bits) {
-    constexpr int kItems = kBlockSortRow / 256;
-    __shared__ int keys[kBlockSortRow];
-    __shared__ u32 vals[kBlockSortRow];
-    __shared__ u32 warp_count[8][kRadix];
-    __shared__ u32 local_base[kRadix];
-    __shared__ u32 scan_u[9];
-    __shared__ int scan_smem[9];
-    const int c = rows[blockIdx.x];
-    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+// Stable LSD passes over one row of `degree` raw entries, Items per thread;
+// leaves the sorted keys/values in shared memory.
+template <int Items>
+__device__ __forceinline__ void sort_row_in_smem(int* keys, u32* vals, u32 (*warp_count)[kRadix], u32* local_base,
+                                                 u32* scan_u, const int* raw_t, const u32* raw_w, int begin, int degree,
+                                                 int nc, int bits) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int k[kItems];
-    u32 v[kItems];
-    bool valid[kItems];
+    int k[Items];
+    u32 v[Items];
+    bool valid[Items];
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const int i = warp * (32 * kItems) + j * 32 + lane;
+    for (int j = 0; j < Items; ++j) {
+        const int i = warp * (32 * Items) + j * 32 + lane;
         valid[j] = i < degree;
         const int t = valid[j] ? raw_t[begin + i] : 0;
         k[j] = t == INT_MAX ? nc : t;
         v[j] = valid[j] ? raw_w[begin + i] : 0u;
     }
     for (int shift = 0; shift < bits; shift += kRadixBits) {
-        u32 pos[kItems];
-        rank_tile<kItems, int>(warp_count, local_base, scan_u, k, valid, shift, pos);
+        u32 pos[Items];
+        rank_tile<Items, int>(warp_count, local_base, scan_u, k, valid, shift, pos);
 #pragma unroll
-        for (int j = 0; j < kItems; ++j)
+        for (int j = 0; j < Items; ++j)
             if (valid[j]) { keys[pos[j]] = k[j]; vals[pos[j]] = v[j]; }
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < kItems; ++j) {
-            const int i = warp * (32 * kItems) + j * 32 + lane;
+        for (int j = 0; j < Items; ++j) {
+            const int i = warp * (32 * Items) + j * 32 + lane;
             if (valid[j]) { k[j] = keys[i]; v[j] = vals[i]; }
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
+                                                         int* ucount, int nc, int bits) {
+    __shared__ int keys[kBlockSortRow];
+    __shared__ u32 vals[kBlockSortRow];
+    __shared__ u32 warp_count[8][kRadix];
+    __shared__ u32 local_base[kRadix];
+    __shared__ u32 scan_u[33];
+    __shared__ int scan_smem[33];
+    const int c = rows[blockIdx.x];
+    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+    // Items per thread by row length (uniform per block).
+    if (degree <= 1024)
+        sort_row_in_smem<4>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
+    else if (degree <= 2048)
+        sort_row_in_smem<8>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
+    else
+        sort_row_in_smem<kBlockSortRow / 256>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree,
+                                              nc, bits);
     // keys/vals hold the sorted row; heads of runs and their exclusive scan.
     const int per = (degree + blockDim.x - 1) / blockDim.x;
     int local = 0;
@@ -920,7 +944,45 @@ __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const 
     if (threadIdx.x == 0) ucount[c] = total;
 }
 
-// Rows above 4096 raw entries: records (row rank, target) -> global radix
+// Rows of 4097..8192 raw entries: the same in-place sort by one block of
+// 1024 threads, 8 items each, in dynamic shared memory.
+__global__ void __launch_bounds__(kBigSortThreads) k_sort_rows_big(const int* rows, const int* raw_off, int* raw_t,
+                                                                   u32* raw_w, int* ucount, int nc, int bits) {
+    extern __shared__ __align__(16) unsigned char big_smem[];
+    int* keys = reinterpret_cast<int*>(big_smem);
+    u32* vals = reinterpret_cast<u32*>(keys + kBigSortRow);
+    u32 (*warp_count)[kRadix] = reinterpret_cast<u32 (*)[kRadix]>(vals + kBigSortRow);
+    u32* local_base = reinterpret_cast<u32*>(warp_count + kBigSortThreads / 32);
+    u32* scan_u = local_base + kRadix;
+    int* scan_i = reinterpret_cast<int*>(scan_u + 33);
+    const int c = rows[blockIdx.x];
+    const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
+    sort_row_in_smem<kBigSortRow / kBigSortThreads>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin,
+                                                    degree, nc, bits);
+    const int per = (degree + blockDim.x - 1) / blockDim.x;
+    int local = 0;
+    for (int q = 0; q < per; ++q) {
+        const int i = threadIdx.x * per + q;
+        if (i < degree) local += keys[i] != nc && (i == 0 || keys[i] != keys[i - 1]);
+    }
+    int total;
+    int run = block_exclusive_scan_wide<int>(local, total, scan_i);
+    for (int q = 0; q < per; ++q) {
+        const int i = threadIdx.x * per + q;
+        if (i < degree && keys[i] != nc && (i == 0 || keys[i] != keys[i - 1])) {
+            u64 sum = 0;
+            for (int j = i; j < degree && keys[j] == keys[i]; ++j) sum += vals[j];
+            raw_t[begin + run] = keys[i];
+            raw_w[begin + run] = static_cast<u32>(sum);
+            ++run;
+        }
+    }
+    if (threadIdx.x == 0) ucount[c] = total;
+}
+constexpr size_t kBigSortSmem = sizeof(int) * kBigSortRow * 2 + sizeof(u32) * (kBigSortThreads / 32) * kRadix +
+                                sizeof(u32) * (kRadix + 33) + sizeof(int) * 33;
+
+// Rows above 8192 raw entries: records (row rank, target) -> global radix
 // sort.  Flat over records; the row of a record is found by binary search.
 __global__ void k_large_records(i64 records, i64 count, const int* rows, const int* raw_off, const int* rec_off,
                                 const int* raw_t, const u32* raw_w, int tbits, u64* keys, u32* vals) {
@@ -1153,8 +1215,6 @@ void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 
             list_size[2], lists[2], static_cast<const u64*>(nullptr), static_cast<int*>(nullptr), static_cast<u64*>(nullptr), p);
     }
     if (g.heavy_count) {
-        GP_CUDA(cudaMemsetAsync(table_keys, 0xff, sizeof(int) * table_slots, ctx.stream));
-        GP_CUDA(cudaMemsetAsync(table_vals, 0, sizeof(u64) * table_slots, ctx.stream));
         launch(k_affinity_heavy_insert, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, table_off, table_keys,
                table_vals, p);
         launch(k_affinity_heavy_summary, static_cast<int>(segments), 256, 0, ctx.stream, g.heavy, seg_hidx, seg_index,
@@ -1232,6 +1292,9 @@ AggregateOut Aggregator::run() {
                 segments = static_cast<i64>(hs[1] & 0xffffffffULL);
                 table_keys = A.alloc<int>(table_slots);
                 table_vals = A.alloc<u64>(table_slots);
+                // Cleared once; every round's summary empties what it used.
+                GP_CUDA(cudaMemsetAsync(table_keys, 0xff, sizeof(int) * table_slots, s));
+                GP_CUDA(cudaMemsetAsync(table_vals, 0, sizeof(u64) * table_slots, s));
                 seg_hidx = A.alloc<int>(segments);
                 seg_index = A.alloc<int>(segments);
                 partial = A.alloc<Summary>(segments);
@@ -1391,13 +1454,13 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
                    static_cast<const int*>(base), raw_t, raw_w);
     }
     // Row classes by raw size.
-    int* lists = A.alloc<int>(static_cast<size_t>(nc) * 4);
-    ctx.clear_scalars(5);
+    int* lists = A.alloc<int>(static_cast<size_t>(nc) * 5);
+    ctx.clear_scalars(6);
     launch(k_row_classes, blocks_for(nc, kThreads), kThreads, 0, s, nc, raw, lists, nc, ctx.dev_scalars);
-    const u64* cls = ctx.read_scalars(5);
-    const i64 count[4] = {static_cast<i64>(cls[0]), static_cast<i64>(cls[1]), static_cast<i64>(cls[2]),
-                          static_cast<i64>(cls[3])};
-    const i64 large_records = static_cast<i64>(cls[4]);
+    const u64* cls = ctx.read_scalars(6);
+    const i64 count[5] = {static_cast<i64>(cls[0]), static_cast<i64>(cls[1]), static_cast<i64>(cls[2]),
+                          static_cast<i64>(cls[3]), static_cast<i64>(cls[4])};
+    const i64 large_records = static_cast<i64>(cls[5]);
     int* ucount = raw;  // raw sizes are no longer needed once the classes exist
     if (count[0])
         launch(k_sort_rows_warp<false>, blocks_for(count[0] * 32, kThreads), kThreads, 0, s, 
@@ -1409,19 +1472,29 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
                ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[3]) {
+        static bool configured = false;  // per process: the attribute belongs to the kernel
+        if (!configured) {
+            GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kBigSortSmem)));
+            configured = true;
+        }
+        launch(k_sort_rows_big, static_cast<int>(count[3]), kBigSortThreads, kBigSortSmem, s, lists + 3 * nc, raw_off,
+               raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
+    }
+    if (count[4]) {
         ArenaScope ls(A);
-        const int* large = lists + 3 * nc;
-        int* rec_off = A.alloc<int>(count[3]);
-        exclusive_scan<int>(A, s, count[3], LargeRowSize{large, raw_off}, rec_off,
+        const int* large = lists + 4 * nc;
+        int* rec_off = A.alloc<int>(count[4]);
+        exclusive_scan<int>(A, s, count[4], LargeRowSize{large, raw_off}, rec_off,
                             static_cast<int*>(nullptr));
         const int tbits = bit_length(static_cast<u64>(nc));
-        const int jbits = std::max(1, bit_length(static_cast<u64>(count[3] - 1)));
+        const int jbits = std::max(1, bit_length(static_cast<u64>(count[4] - 1)));
         u64* keys = A.alloc<u64>(large_records);
         u64* keys_alt = A.alloc<u64>(large_records);
         u32* vals = A.alloc<u32>(large_records);
         u32* vals_alt = A.alloc<u32>(large_records);
         launch(k_large_records, std::min(blocks_for(large_records, kThreads), 148 * 16), kThreads, 0, s,
-               large_records, count[3], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
+               large_records, count[4], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
                vals);
         radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, 0, tbits + jbits);
         u32* hpos = A.alloc<u32>(large_records);
@@ -1429,7 +1502,7 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         exclusive_scan<u32>(A, s, large_records, RecordHead{keys, (1ULL << tbits) - 1}, hpos, heads_total);
         launch(k_large_write, blocks_for(large_records, kThreads), kThreads, 0, s, 
             large_records, keys, vals, hpos, tbits, large, rec_off, raw_off, raw_t, raw_w);
-        launch(k_large_counts, blocks_for(count[3], kThreads), kThreads, 0, s, count[3], large, rec_off, hpos,
+        launch(k_large_counts, blocks_for(count[4], kThreads), kThreads, 0, s, count[4], large, rec_off, hpos,
                                                                                  heads_total, large_records, ucount);
     }
     // Final offsets, then the compact copy into the level's own storage.

@@ -39,6 +39,35 @@ __device__ __forceinline__ T block_exclusive_scan(T value, T& total, T* smem /* 
     return result;
 }
 
+// Block-wide exclusive scan for any block of up to 1024 threads (a multiple
+// of 32); smem holds at least 33 values.
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan_wide(T value, T& total, T* smem) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    T inc = value;
+    for (int d = 1; d < 32; d <<= 1) {
+        const T o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += o;
+    }
+    if (lane == 31) smem[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const T s = lane < warps ? smem[lane] : T(0);
+        T si = s;
+        for (int d = 1; d < 32; d <<= 1) {
+            const T o = __shfl_up_sync(0xffffffffu, si, d);
+            if (lane >= d) si += o;
+        }
+        if (lane < warps) smem[lane] = si - s;
+        if (lane == 31) smem[32] = si;
+    }
+    __syncthreads();
+    const T result = smem[warp] + inc - value;
+    total = smem[32];
+    __syncthreads();
+    return result;
+}
+
 template <class T, class In>
 __global__ void k_tile_sums(i64 n, In in, T* sums) {
     __shared__ T smem[9];
@@ -279,7 +308,8 @@ __device__ __forceinline__ void tile_positions(SortTileSmem& sm, const u64 (&k)[
 // The same ranking for a tile of Items items per thread held in registers in
 // the warp-striped layout (item j of lane l of warp w is tile index
 // w*32*Items + j*32 + l), keys of any integer type.  warp_count is
-// [blockDim/32][kRadix], local_base [kRadix]; blockDim.x must be kRadix.
+// [blockDim/32][kRadix], local_base [kRadix], scan >= 33 values; blockDim.x
+// is a multiple of 32 from kRadix to 1024.
 template <int Items, class K>
 __device__ __forceinline__ void rank_tile(u32 (*warp_count)[kRadix], u32* local_base, u32* scan, const K (&k)[Items],
                                           const bool (&valid)[Items], int shift, u32 (&pos)[Items]) {
@@ -301,15 +331,17 @@ __device__ __forceinline__ void rank_tile(u32 (*warp_count)[kRadix], u32* local_
         __syncwarp();
     }
     __syncthreads();
-    const int d = threadIdx.x;
+    const int d = threadIdx.x;  // threads below kRadix own one digit each
     u32 run = 0;
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-        const u32 c = warp_count[w][d];
-        warp_count[w][d] = run;
-        run += c;
-    }
+    if (d < kRadix)
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            const u32 c = warp_count[w][d];
+            warp_count[w][d] = run;
+            run += c;
+        }
     u32 total;
-    local_base[d] = block_exclusive_scan<u32>(run, total, scan);
+    const u32 base = block_exclusive_scan_wide<u32>(run, total, scan);
+    if (d < kRadix) local_base[d] = base;
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < Items; ++j) {

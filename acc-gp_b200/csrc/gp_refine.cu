@@ -924,23 +924,38 @@ __global__ void k_req_heads(i64 count, const u64* keys, const u64* prefix, u64* 
 // reserve_receiver_prefixes' ticket rule (rebalance_graph.cuh:127-153) in
 // (part, repair order) order: a donor is admitted when its whole weighted
 // range [begin, begin+w) lies inside the part's immutable room.
+// The weight requested per part is summed per warp (requests arrive sorted
+// by part, so a warp holds one or two parts) and per block in shared memory
+// before one global atomic per part and block.
 __global__ void k_admit(i64 count, const u32* reqs, const u64* keys, const u32* active, const u64* prefix,
                         const u64* base, const u32* vw, const u64* slack, const u64* requests, u64* added,
-                        u64* tried, unsigned char* state, int* targets, int* flags) {
+                        u64* tried, unsigned char* state, int* targets, int* flags, int k) {
+    __shared__ u64 block_added[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) block_added[p] = 0;
+    __syncthreads();
     const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    const u32 i = reqs[j];
-    const int t = static_cast<int>(keys[j]);
-    const int v = static_cast<int>(active[i]);
-    const u64 w = vw[v];
-    tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
-    const u64 begin = requests[t] + prefix[j] - base[t];
-    atomicAdd(added + t, w);
-    if (begin <= slack[t] && w <= slack[t] - begin) {
-        targets[v] = t;
-        flags[v] = 1;
-        state[i] = 1;
+    const bool valid = j < count;
+    const int t = valid ? static_cast<int>(keys[j]) : -1;
+    u64 w = 0;
+    if (valid) {
+        const u32 i = reqs[j];
+        const int v = static_cast<int>(active[i]);
+        w = vw[v];
+        tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
+        const u64 begin = requests[t] + prefix[j] - base[t];
+        if (begin <= slack[t] && w <= slack[t] - begin) {
+            targets[v] = t;
+            flags[v] = 1;
+            state[i] = 1;
+        }
     }
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    u64 sum = 0;
+    for (unsigned rest = peers; rest; rest &= rest - 1) sum += __shfl_sync(peers, w, __ffs(rest) - 1);
+    if (t >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(block_added + t, sum);
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (block_added[p]) atomicAdd(added + p, block_added[p]);
 }
 __global__ void k_merge_requests(int k, u64* requests, u64* added) {
     for (int p = threadIdx.x; p < k; p += blockDim.x) { requests[p] += added[p]; added[p] = 0; }
@@ -1765,7 +1780,7 @@ bool LevelRefiner<T>::repair() {
                     exclusive_scan<u64>(A_, s(), rcount, ReqWeight{r, active, g.vw}, rprefix, static_cast<u64*>(nullptr));
                     launch(k_req_heads, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, kk, rprefix, base_t);
                     launch(k_admit, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, kk, active, rprefix, base_t,
-                           g.vw, slack, requests, added, tried, state, targets, flags);
+                           g.vw, slack, requests, added, tried, state, targets, flags, k);
                     launch(k_merge_requests, 1, 128, 0, s(), k, requests, added);
                     // At most rcount donors remain open.
                     if (rcount <= kAttemptCap && attempt + 1 < k) {
