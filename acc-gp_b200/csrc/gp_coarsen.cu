@@ -780,6 +780,45 @@ __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u6
 // contraction_warp_sort / contraction_sort_row (contraction_rows.cuh:40-116):
 // striped bitonic network over Items*32 keys, then a segmented warp scan
 // that sums equal keys; writes the unique sorted run back at `begin`.
+// Writes the unique keys of a sorted warp row (striped: item it of lane l is
+// position it*32 + l; INT_MAX marks dropped or absent entries) back at
+// `begin`, summing the weights of equal keys.
+template <int Items>
+__device__ __forceinline__ void warp_emit_row(const int (&keys)[Items], const u32 (&vals)[Items], int begin,
+                                              int* keys_io, u32* w_io, int lane, int* count_out) {
+    int count = 0;
+    int carry_key = INT_MAX;
+    u32 carry_sum = 0;
+#pragma unroll
+    for (int it = 0; it < Items; ++it) {
+        const int key = keys[it];
+        u32 sum = vals[it];
+        if (!lane && key == carry_key) sum += carry_sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int ok = __shfl_up_sync(0xffffffffu, key, d);
+            const u32 os = __shfl_up_sync(0xffffffffu, sum, d);
+            if (lane >= d && key == ok) sum += os;
+        }
+        const int next_stripe = it + 1 < Items ? keys[it + 1] : INT_MAX;
+        const int following = __shfl_down_sync(0xffffffffu, key, 1);
+        const int following_stripe = __shfl_sync(0xffffffffu, next_stripe, 0);
+        const int next_key = lane < 31 ? following : following_stripe;
+        const bool emit = key != INT_MAX && key != next_key;
+        const unsigned mask = __ballot_sync(0xffffffffu, emit);
+        if (emit) {
+            const int out = begin + count + __popc(mask & ((1u << lane) - 1u));
+            keys_io[out] = key;
+            w_io[out] = sum;
+        }
+        count += __popc(mask);
+        carry_key = __shfl_sync(0xffffffffu, key, 31);
+        carry_sum = __shfl_sync(0xffffffffu, sum, 31);
+    }
+    *count_out = count;
+}
+
+
 template <int Items>
 __device__ void warp_sort_row(int begin, int degree, int* keys_io, u32* w_io, int lane, int* count_out) {
     int keys[Items];
@@ -815,40 +854,82 @@ __device__ void warp_sort_row(int begin, int degree, int* keys_io, u32* w_io, in
             for (int it = 0; it < Items; ++it) { keys[it] = nk[it]; vals[it] = nv[it]; }
         }
     }
-    int count = 0;
-    int carry_key = INT_MAX;
-    u32 carry_sum = 0;
+    warp_emit_row<Items>(keys, vals, begin, keys_io, w_io, lane, count_out);
+}
+
+// Rows of 129..512 raw entries: stable LSD radix sort of the warp's row in
+// its shared-memory slice (8-bit digits over `bits` bits; dropped entries
+// carry the key nc), then the same run reduction as the network sort.
+template <int Items>
+__device__ void warp_radix_row(int begin, int degree, int* keys_io, u32* w_io, int lane, int* count_out, int nc,
+                               int bits, int* skeys, u32* svals, u32* counts) {
+    int k[Items];
+    u32 v[Items];
 #pragma unroll
-    for (int it = 0; it < Items; ++it) {
-        const int key = keys[it];
-        u32 sum = vals[it];
-        if (!lane && key == carry_key) sum += carry_sum;
+    for (int j = 0; j < Items; ++j) {
+        const int pos = j * 32 + lane;
+        const int t = pos < degree ? keys_io[begin + pos] : INT_MAX;
+        k[j] = t == INT_MAX ? nc : t;
+        v[j] = pos < degree ? w_io[begin + pos] : 0u;
+    }
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        for (int d = lane; d < kRadix; d += 32) counts[d] = 0;
+        __syncwarp();
+        u32 rank[Items];
+#pragma unroll
+        for (int j = 0; j < Items; ++j) {
+            const bool valid = j * 32 + lane < degree;
+            const int digit = (k[j] >> shift) & (kRadix - 1);
+            const unsigned active = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                const unsigned peers = __match_any_sync(active, digit);
+                const unsigned below = peers & ((1u << lane) - 1u);
+                rank[j] = counts[digit] + __popc(below);
+                __syncwarp(active);
+                if (below == 0) counts[digit] += __popc(peers);
+            }
+            __syncwarp();
+        }
+        // Exclusive scan of the digit counts, eight consecutive digits a lane.
+        u32 c8[kRadix / 32], sum = 0;
+#pragma unroll
+        for (int q = 0; q < kRadix / 32; ++q) { c8[q] = counts[lane * (kRadix / 32) + q]; sum += c8[q]; }
+        u32 incl = sum;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const int ok = __shfl_up_sync(0xffffffffu, key, d);
-            const u32 os = __shfl_up_sync(0xffffffffu, sum, d);
-            if (lane >= d && key == ok) sum += os;
+            const u32 o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += o;
         }
-        const int next_stripe = it + 1 < Items ? keys[it + 1] : INT_MAX;
-        const int following = __shfl_down_sync(0xffffffffu, key, 1);
-        const int following_stripe = __shfl_sync(0xffffffffu, next_stripe, 0);
-        const int next_key = lane < 31 ? following : following_stripe;
-        const bool emit = key != INT_MAX && key != next_key;
-        const unsigned mask = __ballot_sync(0xffffffffu, emit);
-        if (emit) {
-            const int out = begin + count + __popc(mask & ((1u << lane) - 1u));
-            keys_io[out] = key;
-            w_io[out] = sum;
-        }
-        count += __popc(mask);
-        carry_key = __shfl_sync(0xffffffffu, key, 31);
-        carry_sum = __shfl_sync(0xffffffffu, sum, 31);
+        u32 run = incl - sum;
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kRadix / 32; ++q) { counts[lane * (kRadix / 32) + q] = run; run += c8[q]; }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < Items; ++j)
+            if (j * 32 + lane < degree) {
+                const u32 p = counts[(k[j] >> shift) & (kRadix - 1)] + rank[j];
+                skeys[p] = k[j];
+                svals[p] = v[j];
+            }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < Items; ++j)
+            if (j * 32 + lane < degree) { k[j] = skeys[j * 32 + lane]; v[j] = svals[j * 32 + lane]; }
+        __syncwarp();
     }
-    *count_out = count;
+#pragma unroll
+    for (int j = 0; j < Items; ++j)
+        if (k[j] == nc) k[j] = INT_MAX;
+    warp_emit_row<Items>(k, v, begin, keys_io, w_io, lane, count_out);
 }
 
 template <bool Long>
-__global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off, int* raw_t, u32* raw_w, int* ucount) {
+__global__ void __launch_bounds__(256) k_sort_rows_warp(i64 count, const int* rows, const int* raw_off, int* raw_t,
+                                                        u32* raw_w, int* ucount, int nc, int bits) {
+    __shared__ int skeys[Long ? 8 : 1][512];
+    __shared__ u32 svals[Long ? 8 : 1][512];
+    __shared__ u32 counts[Long ? 8 : 1][kRadix];
     const i64 index = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (index >= count) return;
@@ -856,8 +937,11 @@ __global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off,
     const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
     int out = 0;
     if (Long) {
-        if (degree <= 256) warp_sort_row<8>(begin, degree, raw_t, raw_w, lane, &out);
-        else warp_sort_row<16>(begin, degree, raw_t, raw_w, lane, &out);
+        const int w = Long ? (threadIdx.x >> 5) : 0;
+        if (degree <= 256)
+            warp_radix_row<8>(begin, degree, raw_t, raw_w, lane, &out, nc, bits, skeys[w], svals[w], counts[w]);
+        else
+            warp_radix_row<16>(begin, degree, raw_t, raw_w, lane, &out, nc, bits, skeys[w], svals[w], counts[w]);
     } else {
         if (degree <= 32) warp_sort_row<1>(begin, degree, raw_t, raw_w, lane, &out);
         else if (degree <= 64) warp_sort_row<2>(begin, degree, raw_t, raw_w, lane, &out);
@@ -866,10 +950,6 @@ __global__ void k_sort_rows_warp(i64 count, const int* rows, const int* raw_off,
     if (lane == 0) ucount[c] = out;
 }
 
-// Rows of 513..4096 raw entries: stable LSD radix sort by target in shared
-// memory (8-bit digits over the bits of nc; dropped intra-cluster entries
-// take the key nc and sort last), then one thread per run of equal keys sums
-// it and writes the unique run back at the row's start.
 // Stable LSD passes over one row of `degree` raw entries, Items per thread;
 // leaves the sorted keys/values in shared memory.
 template <int Items>
@@ -904,6 +984,10 @@ __device__ __forceinline__ void sort_row_in_smem(int* keys, u32* vals, u32 (*war
     }
 }
 
+// Rows of 513..4096 raw entries: stable LSD radix sort by target in shared
+// memory (8-bit digits over the bits of nc; dropped intra-cluster entries
+// take the key nc and sort last), then one thread per run of equal keys sums
+// it and writes the unique run back at the row's start.
 __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
                                                          int* ucount, int nc, int bits) {
     __shared__ int keys[kBlockSortRow];
@@ -1463,11 +1547,11 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     const i64 large_records = static_cast<i64>(cls[5]);
     int* ucount = raw;  // raw sizes are no longer needed once the classes exist
     if (count[0])
-        launch(k_sort_rows_warp<false>, blocks_for(count[0] * 32, kThreads), kThreads, 0, s, 
-            count[0], lists, raw_off, raw_t, raw_w, ucount);
+        launch(k_sort_rows_warp<false>, blocks_for(count[0] * 32, kThreads), kThreads, 0, s, count[0], lists, raw_off,
+               raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[1])
-        launch(k_sort_rows_warp<true>, blocks_for(count[1] * 32, kThreads), kThreads, 0, s, 
-            count[1], lists + nc, raw_off, raw_t, raw_w, ucount);
+        launch(k_sort_rows_warp<true>, blocks_for(count[1] * 32, kThreads), kThreads, 0, s, count[1], lists + nc,
+               raw_off, raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[2])
         launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
                ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));

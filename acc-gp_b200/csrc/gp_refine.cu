@@ -308,10 +308,9 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
                 current = A[v * k + src];
                 act = current != static_cast<u64>(totals[v]);
             }
-            if (!act) {
-                q.targets[v] = -1;
-                q.gains[v] = LLONG_MIN;
-            }
+            // A gain is read only where the target is set, so only
+            // proposers write one.
+            if (!act) q.targets[v] = -1;
         }
         s_propose[threadIdx.x] = 0;
         __syncwarp();
@@ -369,13 +368,111 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
             if (owner >= 0 && sub == 0) {
                 const bool propose = target >= 0 && (best >= ocur || ocur - best < static_cast<u64>(q.filter * static_cast<double>(ocur)));
                 q.targets[vv] = propose ? target : -1;
-                q.gains[vv] = !propose ? LLONG_MIN
-                              : best >= ocur ? static_cast<long long>(best - ocur) : -static_cast<long long>(ocur - best);
+                if (propose)
+                    q.gains[vv] = best >= ocur ? static_cast<long long>(best - ocur) : -static_cast<long long>(ocur - best);
                 s_propose[(threadIdx.x & ~31) + owner] = propose;
             }
         }
         __syncwarp();
         block_append(static_cast<int>(v), s_propose[threadIdx.x] != 0, q.cand, q.counters + 0);
+    }
+}
+
+// ---------------------------------------------------------------- on-demand affinities
+
+// Levels whose rows are short next to k (a mesh at k = 128: six neighbours
+// against 128 cache words) keep no dense cache: a vertex's affinities are
+// recomputed from its adjacency where they are needed, one thread per
+// vertex.  The values are exactly the cache's, so every decision is the
+// same; only the data read differs (the reference likewise switches to a
+// sparse/on-demand affinity layout, incremental.cuh:675-741).
+constexpr int kOnDemandDegree = 32;
+
+// Distinct neighbour parts of a row with their connection, and the row's
+// total (self loops excluded, as in the cache).
+struct RowParts {
+    int count;
+    int part[kOnDemandDegree];
+    u64 conn[kOnDemandDegree];
+    u64 total;
+    __device__ __forceinline__ u64 of(int p) const {
+        for (int i = 0; i < count; ++i)
+            if (part[i] == p) return conn[i];
+        return 0;
+    }
+};
+__device__ __forceinline__ void row_parts(int v, const int* off, const int* nbr, const u32* ew, const int* labels,
+                                          RowParts& r) {
+    r.count = 0;
+    r.total = 0;
+    for (int e = off[v]; e < off[v + 1]; ++e) {
+        const int u = nbr[e];
+        if (u == v) continue;
+        const int p = labels[u];
+        const u64 w = edge_w(ew, e);
+        r.total += w;
+        int i = 0;
+        while (i < r.count && r.part[i] != p) ++i;
+        if (i == r.count) {
+            r.part[i] = p;
+            r.conn[i] = 0;
+            ++r.count;
+        }
+        r.conn[i] += w;
+    }
+}
+
+// k_proposals with on-demand affinities: the same target (largest
+// affinity, or affinity minus repair price; lowest part on ties), filter
+// and outputs.
+__global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q) {
+    __shared__ u64 s_slack[kMaxParts];
+    __shared__ double s_price[kMaxParts];
+    if (q.prices)
+        for (int p = threadIdx.x; p < q.k; p += blockDim.x) { s_slack[p] = q.capacity - q.loads[p]; s_price[p] = q.prices[p]; }
+    __syncthreads();
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < q.n;
+         block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 v = block_base + threadIdx.x;
+        bool propose = false;
+        if (v < q.n) {
+            if (q.locks[v]) {
+                q.locks[v] = 0;
+                q.targets[v] = -1;
+            } else {
+                const int src = q.labels[v];
+                RowParts r;
+                row_parts(static_cast<int>(v), q.off, q.nbr, q.ew, q.labels, r);
+                const u64 current = r.of(src);
+                int target = -1;
+                u64 best = 0;
+                if (current != r.total) {
+                    const u64 weight = q.prices ? q.vw[v] : 0;
+                    double best_score = -DBL_MAX;
+                    for (int i = 0; i < r.count; ++i) {
+                        const int p = r.part[i];
+                        if (p == src) continue;
+                        const u64 conn = r.conn[i];
+                        if (q.prices) {
+                            const double cost = weight > s_slack[p] ? __dmul_rn(s_price[p], static_cast<double>(weight - s_slack[p])) : 0.0;
+                            const double score = __dsub_rn(static_cast<double>(conn), cost);
+                            if (target < 0 || score > best_score || (score == best_score && p < target)) {
+                                target = p; best = conn; best_score = score;
+                            }
+                        } else if (target < 0 || conn > best || (conn == best && p < target)) {
+                            target = p;
+                            best = conn;
+                        }
+                    }
+                }
+                propose = target >= 0 &&
+                          (best >= current || current - best < static_cast<u64>(q.filter * static_cast<double>(current)));
+                q.targets[v] = propose ? target : -1;
+                if (propose)
+                    q.gains[v] = best >= current ? static_cast<long long>(best - current) : -static_cast<long long>(current - best);
+            }
+        }
+        block_append(static_cast<int>(v), propose, q.cand, q.counters + 0);
     }
 }
 
@@ -503,16 +600,20 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
                 const u32 w = edge_w(ew, e0);
                 const bool moves = f0 != 0;
                 const int nw = moves ? t0 : old0;
-                atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
+                if (A) {  // no cache with on-demand affinities
+                    atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                    atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
+                }
                 if (!moves || u0 > v) gain += static_cast<long long>(w) * ((s != old0) - (t != nw));
             }
             if (u1 != v) {
                 const u32 w = edge_w(ew, e1);
                 const bool moves = f1 != 0;
                 const int nw = moves ? t1 : old1;
-                atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
+                if (A) {
+                    atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                    atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
+                }
                 if (!moves || u1 > v) gain += static_cast<long long>(w) * ((s != old1) - (t != nw));
             }
         }
@@ -626,18 +727,36 @@ __device__ int gain_bucket(u64 best, u64 current, u64 relief) {
 }
 
 // initialize_receiver_slack (rebalance_select.cuh:79-104) by one thread.
-__global__ void k_slack(int k, const u64* loads, u64 capacity, u64* slack, u64* requests, u64* cdf) {
-    if (threadIdx.x) return;
-    u64 carry = 0, minimum = ~0ULL;
-    for (int p = 0; p < k; ++p) {
-        const u64 room = loads[p] < capacity ? capacity - loads[p] : 0;
+// One thread per part; the CDF is a saturating prefix sum over the parts.
+__device__ __forceinline__ u64 saturating_add(u64 a, u64 b) { return ~0ULL - a < b ? ~0ULL : a + b; }
+__global__ void __launch_bounds__(kMaxParts) k_slack(int k, const u64* loads, u64 capacity, u64* slack, u64* requests,
+                                                     u64* cdf) {
+    __shared__ u64 warp_total[kMaxParts / 32], warp_min[kMaxParts / 32];
+    const int p = threadIdx.x, lane = p & 31, warp = p >> 5;
+    const u64 room = p < k ? (loads[p] < capacity ? capacity - loads[p] : 0) : 0;
+    u64 inc = room, least = room ? room : ~0ULL;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const u64 o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc = saturating_add(inc, o);
+        const u64 m = __shfl_xor_sync(0xffffffffu, least, d);
+        least = m < least ? m : least;
+    }
+    if (lane == 31) warp_total[warp] = inc;
+    if (lane == 0) warp_min[warp] = least;
+    __syncthreads();
+    u64 before = 0;
+    for (int w = 0; w < warp; ++w) before = saturating_add(before, warp_total[w]);
+    if (p < k) {
         slack[p] = room;
         requests[p] = 0;
-        if (room) minimum = min(minimum, room);
-        carry = ~0ULL - carry < room ? ~0ULL : carry + room;
-        cdf[p] = carry;
+        cdf[p] = saturating_add(before, inc);
     }
-    cdf[k] = minimum;
+    if (p == 0) {
+        u64 m = ~0ULL;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = warp_min[w] < m ? warp_min[w] : m;
+        cdf[k] = m;
+    }
 }
 
 struct IsDonor {
@@ -780,6 +899,117 @@ __global__ void __launch_bounds__(kThreads) k_repair_dest(i64 count, const u32* 
             bucket_keys[i] = key;
         }
     }
+}
+
+// k_repair_dest with on-demand affinities, one thread per donor: the best
+// connected destination with room (largest affinity, then room, then lowest
+// part), else the same fallback tickets.
+__global__ void __launch_bounds__(kThreads) k_repair_dest_od(i64 count, const u32* donors, const int* off,
+                                                             const int* nbr, const u32* ew, const int* labels,
+                                                             const u32* vw, int k, const u64* loads, u64 capacity,
+                                                             const u64* cdf, int* targets, u64* bucket_keys) {
+    __shared__ u64 s_room[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_room[p] = loads[p] < capacity ? capacity - loads[p] : 0;
+    __syncthreads();
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = static_cast<int>(donors[i]);
+        const int src = labels[v];
+        const u64 w = vw[v];
+        RowParts r;
+        row_parts(v, off, nbr, ew, labels, r);
+        const u64 current = r.of(src);
+        int part = -1;
+        u64 conn = 0, best_room = 0;
+        if (current != r.total)
+            for (int j = 0; j < r.count; ++j) {
+                const int p = r.part[j];
+                const u64 room = s_room[p];
+                if (p == src || w > room) continue;
+                const u64 value = r.conn[j];
+                if (part < 0 || value > conn || (value == conn && (room > best_room || (room == best_room && p < part)))) {
+                    part = p; conn = value; best_room = room;
+                }
+            }
+        if (!conn) part = -1;
+        if (part < 0) {
+            conn = 0;
+            const u32 hash = mix32(static_cast<u32>(v));
+            if (loads[src] >= capacity && w <= cdf[k]) {
+                const u64 sum = cdf[k - 1];
+                if (sum) {
+                    const u64 t = static_cast<u64>(hash) % sum;
+                    int lo = 0, hi = k;
+                    while (lo < hi) { const int mid = (lo + hi) / 2; if (cdf[mid] <= t) lo = mid + 1; else hi = mid; }
+                    part = lo;
+                }
+            } else {
+                u64 total = 0;
+                for (int p = 0; p < k; ++p)
+                    if (p != src && w <= s_room[p]) total = ~0ULL - total < s_room[p] ? ~0ULL : total + s_room[p];
+                if (total) {
+                    u64 t = static_cast<u64>(hash) % total;
+                    for (int p = 0; p < k; ++p)
+                        if (p != src && w <= s_room[p]) {
+                            if (t < s_room[p]) { part = p; break; }
+                            t -= s_room[p];
+                        }
+                }
+            }
+        }
+        targets[v] = part;
+        u64 key = ~0ULL;
+        if (part >= 0) {
+            const u64 excess = loads[src] - capacity;
+            const u64 relief = w < excess ? w : excess;
+            key = static_cast<u64>(src) * kBalanceWidth + gain_bucket(conn, current, relief) * 16 + mix32(static_cast<u32>(v)) % 16;
+        }
+        bucket_keys[i] = key;
+    }
+}
+
+// Receiver choice of one donor with on-demand affinities (k_choose, attempt
+// > 0): among parts other than its own, not yet tried, whose remaining room
+// holds it, the largest affinity, then the largest room, then the lowest
+// part.  Parts without a neighbour have affinity 0.
+__device__ __forceinline__ int choose_od(int v, const int* off, const int* nbr, const u32* ew, const int* labels,
+                                         int k, u64 w, u64 t0, u64 t1, const u64* avail) {
+    RowParts r;
+    row_parts(v, off, nbr, ew, labels, r);
+    const int src = labels[v];
+    int target = -1;
+    u64 best = 0, room = 0;
+    for (int p = 0; p < k; ++p) {
+        if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+        const u64 a = avail[p];
+        if (a < w) continue;
+        const u64 c = r.of(p);
+        if (target < 0 || c > best || (c == best && a > room)) { target = p; best = c; room = a; }
+    }
+    return target;
+}
+
+__global__ void __launch_bounds__(kThreads) k_choose_od(i64 count, const u32* active, int attempt, const int* off,
+                                                        const int* nbr, const u32* ew, const int* labels,
+                                                        const u32* vw, int k, const int* proposal, const u64* slack,
+                                                        const u64* requests, const u64* tried, unsigned char* state,
+                                                        int* want, u64* requesters) {
+    __shared__ u64 s_avail[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_avail[p] = requests[p] < slack[p] ? slack[p] - requests[p] : 0;
+    __syncthreads();
+    u64 asked = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        if (state[i]) {
+            want[i] = -1;
+            continue;
+        }
+        const int v = static_cast<int>(active[i]);
+        const int target = attempt == 0 ? proposal[v]
+                                        : choose_od(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
+        want[i] = target;
+        if (target < 0) state[i] = 2;
+        else ++asked;
+    }
+    block_atomic_add(requesters, asked);
 }
 
 constexpr u64 kNoBucket = 0xffffffULL;  // donors without a destination sort last
@@ -969,12 +1199,13 @@ constexpr int kAttemptThreads = 1024;
 constexpr int kAttemptCap = 2048;  // open donors handled by one block
 template <class C>
 __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, const u32* count_ptr, int first_attempt,
-                                                              const u32* active, const C* A, const int* labels,
+                                                              const u32* active, const C* A, const int* off,
+                                                              const int* nbr, const u32* ew, const int* labels,
                                                               const u32* vw, int k, const int* proposal,
                                                               const u64* slack, u64* requests, u64* tried,
                                                               unsigned char* state, int* targets, int* flags) {
     constexpr int kWarps = kAttemptThreads / 32;
-    __shared__ u64 s_slack[kMaxParts], s_requests[kMaxParts], s_base[kMaxParts];
+    __shared__ u64 s_slack[kMaxParts], s_requests[kMaxParts], s_base[kMaxParts], s_avail[kMaxParts];
     __shared__ u64 s_warp[kWarps][kMaxParts];  // per-warp weight requested per part
     __shared__ int s_want[kAttemptCap];
     __shared__ int s_any;
@@ -984,6 +1215,8 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
     __syncthreads();
     for (int attempt = first_attempt; attempt < k; ++attempt) {
         if (threadIdx.x == 0) s_any = 0;
+        for (int p = threadIdx.x; p < k; p += blockDim.x)
+            s_avail[p] = s_requests[p] < s_slack[p] ? s_slack[p] - s_requests[p] : 0;
         __syncthreads();
         // Choice (k_choose).
         for (int j = threadIdx.x; j < count; j += blockDim.x) {
@@ -993,6 +1226,8 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                 const int v = static_cast<int>(active[i]);
                 if (attempt == 0) {
                     target = proposal[v];
+                } else if (!A) {  // on-demand affinities
+                    target = choose_od(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
                 } else {
                     const u64 w = vw[v];
                     const int src = labels[v];
@@ -1530,6 +1765,8 @@ private:
     long long* corr_acc = nullptr;  // per heavy row: priority-filter correction
     u64 cut = 0, revision = 0;
     u64 rebuild_entries = ~0ULL;  // mover entries above which apply() rebuilds the cache
+    i64 repair_iterations = 0, repair_donors = 0;  // for the per-level log line
+    bool on_demand = false;  // no dense cache: affinities recomputed from the rows
     u64 max_load_host = 0;
 
     cudaStream_t s() const { return ctx.stream; }
@@ -1538,6 +1775,7 @@ private:
     // Rebuilds the cache and row totals from the labels; with directed_cut
     // also sums the directed cut (device counter, cleared by the caller).
     void build(u64* directed_cut = nullptr, const u64* gate = nullptr, u64 threshold = 0) {
+        if (on_demand) return;
         build_into(A, totals, directed_cut, gate, threshold);
     }
     void build_into(T* A, T* totals, u64* directed_cut, const u64* gate, u64 threshold) {
@@ -1575,8 +1813,8 @@ private:
     void apply(const int* list, const u64* live, i64 host_count, bool lp, bool sample) {
         GP_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(u64), s()));
         GP_CUDA(cudaMemsetAsync(counters + 6, 0, 2 * sizeof(u64), s()));
-        const u64* gate = sample ? nullptr : counters + 6;
-        const u64 threshold = sample ? ~0ULL : rebuild_entries;
+        const u64* gate = sample || on_demand ? nullptr : counters + 6;
+        const u64 threshold = gate ? rebuild_entries : ~0ULL;
         if (gate)
             launch(k_mover_entries, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    counters + 6);
@@ -1618,6 +1856,10 @@ private:
     }
     void proposals(const LpParams& q) {
         const int grid = grid_for(n, kThreads);
+        if (on_demand) {
+            launch(k_proposals_od, grid, kThreads, 0, s(), q);
+            return;
+        }
         const T* a = A;
         const T* t = totals;
         with_groups([&](auto width, auto vec) {
@@ -1630,6 +1872,7 @@ private:
     void check_state(const char* cut_message) {
         if (!verify) return;
         if (device_cut(ctx, g, labels) != cut) fail(GP_INTERNAL, cut_message);
+        if (on_demand) return;  // no cache to compare
         if (!check_A) {
             check_A = ctx.persist.alloc<T>(static_cast<size_t>(n) * k);
             check_totals = ctx.persist.alloc<T>(n);
@@ -1699,11 +1942,13 @@ bool LevelRefiner<T>::repair() {
     int iterations = 0;
     while (true) {
         ArenaScope it(A_);
-        launch(k_slack, 1, 32, 0, s(), k, loads, C, slack, requests, cdf);
+        launch(k_slack, 1, kMaxParts, 0, s(), k, loads, C, slack, requests, cdf);
         select_if(A_, s(), n, IsDonor{rorder, labels, loads, C}, WriteOrdered{rorder, donors}, donor_count);
         GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
         GP_CUDA(cudaStreamSynchronize(s()));
         const i64 dcount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+        ++repair_iterations;
+        repair_donors += dcount;
         i64 placed = 0;
         long long delta = 0;
         if (dcount > 0) {
@@ -1711,12 +1956,18 @@ bool LevelRefiner<T>::repair() {
             u64* keys_alt = A_.alloc<u64>(dcount);
             u32* items = A_.alloc<u32>(dcount);
             u32* items_alt = A_.alloc<u32>(dcount);
-            with_groups([&](auto width, auto vec) {
-                constexpr int W = decltype(width)::value;
-                launch(k_repair_dest<T, W, decltype(vec)::value>, grid_for(dcount * W, kThreads), kThreads, 0, s(),
-                       dcount, donors, static_cast<const T*>(A), static_cast<const T*>(totals), labels, g.vw, k, loads,
-                       C, cdf, targets, keys);
-            });
+            if (on_demand)
+                launch(k_repair_dest_od, grid_for(dcount, kThreads), kThreads, 0, s(), dcount,
+                       static_cast<const u32*>(donors), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
+                       static_cast<const u32*>(g.ew), static_cast<const int*>(labels), static_cast<const u32*>(g.vw), k,
+                       static_cast<const u64*>(loads), C, static_cast<const u64*>(cdf), targets, keys);
+            else
+                with_groups([&](auto width, auto vec) {
+                    constexpr int W = decltype(width)::value;
+                    launch(k_repair_dest<T, W, decltype(vec)::value>, grid_for(dcount * W, kThreads), kThreads, 0, s(),
+                           dcount, donors, static_cast<const T*>(A), static_cast<const T*>(totals), labels, g.vw, k, loads,
+                           C, cdf, targets, keys);
+                });
             GP_CUDA(cudaMemcpyAsync(items, donors, sizeof(u32) * dcount, cudaMemcpyDeviceToDevice, s()));
             // Stable sort by bucket keeps the repair order inside a bucket;
             // bucket keys are below k*800 < 2^17, the sentinel sorts last.
@@ -1750,7 +2001,8 @@ bool LevelRefiner<T>::repair() {
                 auto finish_in_block = [&](int first_attempt) {
                     launch(k_attempts<T>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
                            static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
-                           static_cast<const T*>(A), static_cast<const int*>(labels), g.vw, k,
+                           static_cast<const T*>(A), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
+                           static_cast<const u32*>(g.ew), static_cast<const int*>(labels), g.vw, k,
                            static_cast<const int*>(targets), static_cast<const u64*>(slack), requests, tried, state,
                            targets, flags);
                 };
@@ -1760,12 +2012,21 @@ bool LevelRefiner<T>::repair() {
                 }
                 for (int attempt = 0; attempt < k && acount > kAttemptCap; ++attempt) {
                     GP_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(u64), s()));
-                    with_groups([&](auto width, auto vec) {
-                        constexpr int W = decltype(width)::value;
-                        launch(k_choose<T, W, decltype(vec)::value>, grid_for(acount * W, kThreads), kThreads, 0, s(),
-                               acount, active, attempt, static_cast<const T*>(A), labels, g.vw, k, targets, slack,
-                               requests, tried, state, want, counters + 5);
-                    });
+                    if (on_demand)
+                        launch(k_choose_od, grid_for(acount, kThreads), kThreads, 0, s(), acount,
+                               static_cast<const u32*>(active), attempt, static_cast<const int*>(g.off),
+                               static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
+                               static_cast<const int*>(labels), static_cast<const u32*>(g.vw), k,
+                               static_cast<const int*>(targets), static_cast<const u64*>(slack),
+                               static_cast<const u64*>(requests), static_cast<const u64*>(tried), state, want,
+                               counters + 5);
+                    else
+                        with_groups([&](auto width, auto vec) {
+                            constexpr int W = decltype(width)::value;
+                            launch(k_choose<T, W, decltype(vec)::value>, grid_for(acount * W, kThreads), kThreads, 0, s(),
+                                   acount, active, attempt, static_cast<const T*>(A), labels, g.vw, k, targets, slack,
+                                   requests, tried, state, want, counters + 5);
+                        });
                     select_if(A_, s(), acount, WantsPart{want}, WriteIdx{reqs}, donor_count);
                     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
                     GP_CUDA(cudaStreamSynchronize(s()));
@@ -1929,8 +2190,14 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
     C = cap;
     const bool priced = total > static_cast<u64>(n);
-    A = A_.alloc<T>(static_cast<size_t>(n) * k);
-    totals = A_.alloc<T>(n);
+    // Short rows next to k (levels large enough to skip the exchange step,
+    // which reads the cache): recompute affinities on demand.
+    on_demand = n > 65536 && g.maximum_degree <= static_cast<u64>(kOnDemandDegree) &&
+                3 * g.maximum_degree < static_cast<u64>(k);
+    if (!on_demand) {
+        A = A_.alloc<T>(static_cast<size_t>(n) * k);
+        totals = A_.alloc<T>(n);
+    }
     targets = A_.alloc<int>(n);
     gains = A_.alloc<long long>(n);
     locks = A_.alloc<unsigned char>(n);
@@ -1970,6 +2237,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     max_load_host = ctx.host_scalars[0];
     if (has_known) {
         cut = known;
+    } else if (on_demand) {
+        cut = device_cut(ctx, g, labels);
     } else {
         if (ctx.host_scalars[4] & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
         cut = ctx.host_scalars[4] / 2;
@@ -2027,8 +2296,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     }
     if (cut != best || cut > feasible_start || max_load_host > C) fail(GP_INTERNAL, "incremental refinement postcondition failed");
     if (log)
-        std::printf("refine_level vertices=%lld initial_cut=%llu final_cut=%llu rounds=%d\n", static_cast<long long>(n),
-                    static_cast<unsigned long long>(feasible_start), static_cast<unsigned long long>(cut), rounds);
+        std::printf("refine_level vertices=%lld initial_cut=%llu final_cut=%llu rounds=%d repair_iterations=%lld "
+                    "repair_donors=%lld\n", static_cast<long long>(n), static_cast<unsigned long long>(feasible_start),
+                    static_cast<unsigned long long>(cut), rounds, static_cast<long long>(repair_iterations),
+                    static_cast<long long>(repair_donors));
     res.cut = cut;
     res.refined = true;
     return res;

@@ -318,14 +318,21 @@ def run_reference(args):
 def launch_list(args):
     import torch
     gp = load_package()
-    g = gp.rmat(args.scale, 16, 0.57, 0.19, 0.19, 0)
+    if args.workload == "m3":  # weighted 7-point mesh, side^3 vertices, k=128
+        g, k = gp.mesh3d(args.side, args.side, args.side, weighted=True, seed=0), 128
+    else:
+        g, k = gp.rmat(args.scale, 16, 0.57, 0.19, 0.19, 0), WORKLOAD["k"]
     dev = torch.device("cuda", 0)
     off_d = torch.from_numpy(g.offsets).to(dev)
     nbr_d = torch.from_numpy(g.neighbors).to(dev)
+    vw_d = torch.from_numpy(g.vertex_weights).to(dev) if g.vertex_weights is not None else None
+    ew_d = torch.from_numpy(g.edge_weights).to(dev) if g.edge_weights is not None else None
     labels_d = torch.empty(g.n, dtype=torch.int32, device=dev)
     ctx = gp.Context(0)
     for _ in range(args.warmup + 1):
-        st = ctx.partition_device(off_d.data_ptr(), nbr_d.data_ptr(), g.n, g.m, None, None, WORKLOAD["k"],
+        st = ctx.partition_device(off_d.data_ptr(), nbr_d.data_ptr(), g.n, g.m,
+                                  vw_d.data_ptr() if vw_d is not None else None,
+                                  ew_d.data_ptr() if ew_d is not None else None, k,
                                   WORKLOAD["epsilon"], WORKLOAD["seed"], labels_d.data_ptr())
     torch.cuda.synchronize()
     print(json.dumps({"launch_list": True, "launches_per_partition": st.kernel_launches,
@@ -469,7 +476,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
-    ap.add_argument("--workload", choices=["rmat22", "batch", "serving"], default="rmat22",
+    ap.add_argument("--side", type=int, default=256, help="mesh side of --launch-list --workload m3")
+    ap.add_argument("--workload", choices=["rmat22", "batch", "serving", "m3"], default="rmat22",
                     help="batch: the uneven 512-graph set, serial vs gp_partition_batch; "
                          "serving: Poisson requests against a gp_server")
     ap.add_argument("--requests", type=int, default=1000)
