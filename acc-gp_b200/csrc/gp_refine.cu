@@ -388,43 +388,48 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
 // sparse/on-demand affinity layout, incremental.cuh:675-741).
 constexpr int kOnDemandDegree = 32;
 
-// Distinct neighbour parts of a row with their connection, and the row's
-// total (self loops excluded, as in the cache).
-struct RowParts {
-    int count;
-    int part[kOnDemandDegree];
-    u64 conn[kOnDemandDegree];
+// A row of at most D entries in registers: the part of every neighbour (-1
+// for a self loop or an absent entry) and the edge weight; all loads of the
+// row are issued together.
+template <int D>
+struct RowRegs {
+    int part[D];
+    u64 w[D];
     u64 total;
+    __device__ __forceinline__ void load(int v, const int* off, const int* nbr, const u32* ew, const int* labels) {
+        const int b = off[v], end = off[v + 1];
+        int u[D];
+#pragma unroll
+        for (int j = 0; j < D; ++j) u[j] = b + j < end ? nbr[b + j] : v;
+        total = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            const bool ok = u[j] != v;  // absent entries read as v
+            part[j] = ok ? labels[u[j]] : -1;
+            w[j] = ok ? edge_w(ew, b + j) : 0;
+            total += w[j];
+        }
+    }
+    // Connection to part p (0 without a neighbour in p).
     __device__ __forceinline__ u64 of(int p) const {
-        for (int i = 0; i < count; ++i)
-            if (part[i] == p) return conn[i];
-        return 0;
+        u64 c = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) c += part[j] == p ? w[j] : 0;
+        return c;
+    }
+    // Entry j holds the first occurrence of its part.
+    __device__ __forceinline__ bool first(int j) const {
+        if (part[j] < 0) return false;
+        for (int i = 0; i < j; ++i)
+            if (part[i] == part[j]) return false;
+        return true;
     }
 };
-__device__ __forceinline__ void row_parts(int v, const int* off, const int* nbr, const u32* ew, const int* labels,
-                                          RowParts& r) {
-    r.count = 0;
-    r.total = 0;
-    for (int e = off[v]; e < off[v + 1]; ++e) {
-        const int u = nbr[e];
-        if (u == v) continue;
-        const int p = labels[u];
-        const u64 w = edge_w(ew, e);
-        r.total += w;
-        int i = 0;
-        while (i < r.count && r.part[i] != p) ++i;
-        if (i == r.count) {
-            r.part[i] = p;
-            r.conn[i] = 0;
-            ++r.count;
-        }
-        r.conn[i] += w;
-    }
-}
 
 // k_proposals with on-demand affinities: the same target (largest
 // affinity, or affinity minus repair price; lowest part on ties), filter
 // and outputs.
+template <int D>
 __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q) {
     __shared__ u64 s_slack[kMaxParts];
     __shared__ double s_price[kMaxParts];
@@ -441,18 +446,19 @@ __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q) {
                 q.targets[v] = -1;
             } else {
                 const int src = q.labels[v];
-                RowParts r;
-                row_parts(static_cast<int>(v), q.off, q.nbr, q.ew, q.labels, r);
+                RowRegs<D> r;
+                r.load(static_cast<int>(v), q.off, q.nbr, q.ew, q.labels);
                 const u64 current = r.of(src);
                 int target = -1;
                 u64 best = 0;
                 if (current != r.total) {
                     const u64 weight = q.prices ? q.vw[v] : 0;
                     double best_score = -DBL_MAX;
-                    for (int i = 0; i < r.count; ++i) {
+#pragma unroll
+                    for (int i = 0; i < D; ++i) {
                         const int p = r.part[i];
-                        if (p == src) continue;
-                        const u64 conn = r.conn[i];
+                        if (p == src || !r.first(i)) continue;
+                        const u64 conn = r.of(p);
                         if (q.prices) {
                             const double cost = weight > s_slack[p] ? __dmul_rn(s_price[p], static_cast<double>(weight - s_slack[p])) : 0.0;
                             const double score = __dsub_rn(static_cast<double>(conn), cost);
@@ -516,6 +522,77 @@ __global__ void k_filter(LpParams q) {
             q.flags[v] = keep;
         }
     }
+}
+
+// k_filter for rows of at most D entries, one thread per candidate (the
+// on-demand levels: a warp per six-entry row would leave most lanes idle).
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_filter_od(LpParams q) {
+    const i64 count = static_cast<i64>(q.counters[0]);
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = q.cand[i];
+        const int s = q.labels[v], t = q.targets[v];
+        const long long gain = q.gains[v];
+        const int b = q.off[v], end = q.off[v + 1];
+        int u[D];
+#pragma unroll
+        for (int j = 0; j < D; ++j) u[j] = b + j < end ? q.nbr[b + j] : v;
+        long long corr = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            if (u[j] == v) continue;
+            const int tu = q.targets[u[j]];
+            if (tu < 0) continue;
+            const long long gu = q.gains[u[j]];
+            if (!(gu > gain || (gu == gain && u[j] < v))) continue;
+            const int lu = q.labels[u[j]];
+            corr += static_cast<long long>(edge_w(q.ew, b + j)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+        }
+        bool keep;
+        if (q.prices) {
+            const u64 w = q.vw[v];
+            const double adj = __dsub_rn(repair_cost(s, w, q.loads, q.capacity, q.prices),
+                                         repair_cost(t, w, q.loads, q.capacity, q.prices));
+            keep = __dadd_rn(static_cast<double>(gain + corr), adj) >= 0;
+        } else keep = gain + corr >= 0;
+        q.flags[v] = keep;
+    }
+}
+
+// k_update without a cache (on-demand levels), one thread per mover: the
+// exact cut change and the repair samples.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_update_od(i64 count, const int* movers, const u64* live_count,
+                                                        const int* off, const int* nbr, const u32* ew, const u32* vw,
+                                                        const int* labels, const int* targets, const int* flags,
+                                                        long long* delta, Sample* samples) {
+    __shared__ WarpSum delta_sum;
+    delta_sum.init();
+    if (live_count) count = static_cast<i64>(*live_count);
+    long long total = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = movers[i];
+        const int s = labels[v], t = targets[v];
+        const int b = off[v], end = off[v + 1];
+        int u[D];
+#pragma unroll
+        for (int j = 0; j < D; ++j) u[j] = b + j < end ? nbr[b + j] : v;
+        long long gain = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            if (u[j] == v) continue;
+            const int old = labels[u[j]];
+            const bool moves = flags[u[j]] != 0;
+            const int nw = moves ? targets[u[j]] : old;
+            if (!moves || u[j] > v) gain += static_cast<long long>(edge_w(ew, b + j)) * ((s != old) - (t != nw));
+        }
+        total += gain;
+        if (samples) {
+            atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
+            atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
+        }
+    }
+    delta_sum.finish(static_cast<u64>(warp_sum(total)), reinterpret_cast<u64*>(delta));
 }
 
 // Heavy candidates: partial corrections per chunk, then the decision
@@ -904,6 +981,7 @@ __global__ void __launch_bounds__(kThreads) k_repair_dest(i64 count, const u32* 
 // k_repair_dest with on-demand affinities, one thread per donor: the best
 // connected destination with room (largest affinity, then room, then lowest
 // part), else the same fallback tickets.
+template <int D>
 __global__ void __launch_bounds__(kThreads) k_repair_dest_od(i64 count, const u32* donors, const int* off,
                                                              const int* nbr, const u32* ew, const int* labels,
                                                              const u32* vw, int k, const u64* loads, u64 capacity,
@@ -915,17 +993,19 @@ __global__ void __launch_bounds__(kThreads) k_repair_dest_od(i64 count, const u3
         const int v = static_cast<int>(donors[i]);
         const int src = labels[v];
         const u64 w = vw[v];
-        RowParts r;
-        row_parts(v, off, nbr, ew, labels, r);
+        RowRegs<D> r;
+        r.load(v, off, nbr, ew, labels);
         const u64 current = r.of(src);
         int part = -1;
         u64 conn = 0, best_room = 0;
         if (current != r.total)
-            for (int j = 0; j < r.count; ++j) {
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
                 const int p = r.part[j];
+                if (p < 0 || p == src || !r.first(j)) continue;
                 const u64 room = s_room[p];
-                if (p == src || w > room) continue;
-                const u64 value = r.conn[j];
+                if (w > room) continue;
+                const u64 value = r.of(p);
                 if (part < 0 || value > conn || (value == conn && (room > best_room || (room == best_room && p < part)))) {
                     part = p; conn = value; best_room = room;
                 }
@@ -971,10 +1051,11 @@ __global__ void __launch_bounds__(kThreads) k_repair_dest_od(i64 count, const u3
 // > 0): among parts other than its own, not yet tried, whose remaining room
 // holds it, the largest affinity, then the largest room, then the lowest
 // part.  Parts without a neighbour have affinity 0.
+template <int D>
 __device__ __forceinline__ int choose_od(int v, const int* off, const int* nbr, const u32* ew, const int* labels,
                                          int k, u64 w, u64 t0, u64 t1, const u64* avail) {
-    RowParts r;
-    row_parts(v, off, nbr, ew, labels, r);
+    RowRegs<D> r;
+    r.load(v, off, nbr, ew, labels);
     const int src = labels[v];
     int target = -1;
     u64 best = 0, room = 0;
@@ -988,6 +1069,7 @@ __device__ __forceinline__ int choose_od(int v, const int* off, const int* nbr, 
     return target;
 }
 
+template <int D>
 __global__ void __launch_bounds__(kThreads) k_choose_od(i64 count, const u32* active, int attempt, const int* off,
                                                         const int* nbr, const u32* ew, const int* labels,
                                                         const u32* vw, int k, const int* proposal, const u64* slack,
@@ -1004,7 +1086,7 @@ __global__ void __launch_bounds__(kThreads) k_choose_od(i64 count, const u32* ac
         }
         const int v = static_cast<int>(active[i]);
         const int target = attempt == 0 ? proposal[v]
-                                        : choose_od(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
+                                        : choose_od<D>(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
         want[i] = target;
         if (target < 0) state[i] = 2;
         else ++asked;
@@ -1197,7 +1279,7 @@ __global__ void k_merge_requests(int k, u64* requests, u64* added) {
 // are admitted in repair order exactly as the device-wide path does.
 constexpr int kAttemptThreads = 1024;
 constexpr int kAttemptCap = 2048;  // open donors handled by one block
-template <class C>
+template <class C, int D>
 __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, const u32* count_ptr, int first_attempt,
                                                               const u32* active, const C* A, const int* off,
                                                               const int* nbr, const u32* ew, const int* labels,
@@ -1227,7 +1309,7 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                 if (attempt == 0) {
                     target = proposal[v];
                 } else if (!A) {  // on-demand affinities
-                    target = choose_od(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
+                    target = choose_od<D>(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
                 } else {
                     const u64 w = vw[v];
                     const int src = labels[v];
@@ -1818,9 +1900,18 @@ private:
         if (gate)
             launch(k_mover_entries, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    counters + 6);
-        launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
-               g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
-               sample ? samples : static_cast<Sample*>(nullptr), gate, threshold);
+        if (on_demand)
+            with_row_size([&](auto d) {
+                launch(k_update_od<decltype(d)::value>, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list,
+                       live, static_cast<const int*>(g.off), static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
+                       static_cast<const u32*>(g.vw), static_cast<const int*>(labels), static_cast<const int*>(targets),
+                       static_cast<const int*>(flags), reinterpret_cast<long long*>(counters + 2),
+                       sample ? samples : static_cast<Sample*>(nullptr));
+            });
+        else
+            launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
+                   g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
+                   sample ? samples : static_cast<Sample*>(nullptr), gate, threshold);
         if (g.chunks)
             launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
                    static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
@@ -1854,10 +1945,17 @@ private:
         else if (W == 8) go(std::integral_constant<int, 8>{});
         else go(std::integral_constant<int, 16>{});
     }
+    // Row-register size of the on-demand kernels for this level.
+    template <class F>
+    void with_row_size(F&& f) const {
+        if (g.maximum_degree <= 8) f(std::integral_constant<int, 8>{});
+        else if (g.maximum_degree <= 16) f(std::integral_constant<int, 16>{});
+        else f(std::integral_constant<int, kOnDemandDegree>{});
+    }
     void proposals(const LpParams& q) {
         const int grid = grid_for(n, kThreads);
         if (on_demand) {
-            launch(k_proposals_od, grid, kThreads, 0, s(), q);
+            with_row_size([&](auto d) { launch(k_proposals_od<decltype(d)::value>, grid, kThreads, 0, s(), q); });
             return;
         }
         const T* a = A;
@@ -1900,7 +1998,10 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
     LpParams q{n, k, C, filter, g.off, g.nbr, g.ew, g.vw, labels, loads, prices, targets, gains, locks, flags, cand, movers, counters};
     proposals(q);
-    launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
+    if (on_demand)
+        with_row_size([&](auto d) { launch(k_filter_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), q); });
+    else
+        launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
     if (g.chunks) {
         GP_CUDA(cudaMemsetAsync(corr_acc, 0, sizeof(long long) * g.heavy_count, s()));
         launch(k_filter_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, q, corr_acc);
@@ -1957,10 +2058,12 @@ bool LevelRefiner<T>::repair() {
             u32* items = A_.alloc<u32>(dcount);
             u32* items_alt = A_.alloc<u32>(dcount);
             if (on_demand)
-                launch(k_repair_dest_od, grid_for(dcount, kThreads), kThreads, 0, s(), dcount,
-                       static_cast<const u32*>(donors), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
-                       static_cast<const u32*>(g.ew), static_cast<const int*>(labels), static_cast<const u32*>(g.vw), k,
-                       static_cast<const u64*>(loads), C, static_cast<const u64*>(cdf), targets, keys);
+                with_row_size([&](auto d) {
+                    launch(k_repair_dest_od<decltype(d)::value>, grid_for(dcount, kThreads), kThreads, 0, s(), dcount,
+                           static_cast<const u32*>(donors), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
+                           static_cast<const u32*>(g.ew), static_cast<const int*>(labels), static_cast<const u32*>(g.vw),
+                           k, static_cast<const u64*>(loads), C, static_cast<const u64*>(cdf), targets, keys);
+                });
             else
                 with_groups([&](auto width, auto vec) {
                     constexpr int W = decltype(width)::value;
@@ -1999,12 +2102,14 @@ bool LevelRefiner<T>::repair() {
                 u32* open_count = reinterpret_cast<u32*>(counters + 5);
                 // Small sets of open donors finish all their attempts in one block.
                 auto finish_in_block = [&](int first_attempt) {
-                    launch(k_attempts<T>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
-                           static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
-                           static_cast<const T*>(A), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
-                           static_cast<const u32*>(g.ew), static_cast<const int*>(labels), g.vw, k,
-                           static_cast<const int*>(targets), static_cast<const u64*>(slack), requests, tried, state,
-                           targets, flags);
+                    with_row_size([&](auto d) {
+                        launch(k_attempts<T, decltype(d)::value>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
+                               static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
+                               static_cast<const T*>(A), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
+                               static_cast<const u32*>(g.ew), static_cast<const int*>(labels), g.vw, k,
+                               static_cast<const int*>(targets), static_cast<const u64*>(slack), requests, tried, state,
+                               targets, flags);
+                    });
                 };
                 if (acount <= kAttemptCap) {
                     select_if(A_, s(), acount, IsOpen{state}, WriteIdx{open}, open_count);
@@ -2013,13 +2118,15 @@ bool LevelRefiner<T>::repair() {
                 for (int attempt = 0; attempt < k && acount > kAttemptCap; ++attempt) {
                     GP_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(u64), s()));
                     if (on_demand)
-                        launch(k_choose_od, grid_for(acount, kThreads), kThreads, 0, s(), acount,
-                               static_cast<const u32*>(active), attempt, static_cast<const int*>(g.off),
-                               static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
-                               static_cast<const int*>(labels), static_cast<const u32*>(g.vw), k,
-                               static_cast<const int*>(targets), static_cast<const u64*>(slack),
-                               static_cast<const u64*>(requests), static_cast<const u64*>(tried), state, want,
-                               counters + 5);
+                        with_row_size([&](auto d) {
+                            launch(k_choose_od<decltype(d)::value>, grid_for(acount, kThreads), kThreads, 0, s(), acount,
+                                   static_cast<const u32*>(active), attempt, static_cast<const int*>(g.off),
+                                   static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
+                                   static_cast<const int*>(labels), static_cast<const u32*>(g.vw), k,
+                                   static_cast<const int*>(targets), static_cast<const u64*>(slack),
+                                   static_cast<const u64*>(requests), static_cast<const u64*>(tried), state, want,
+                                   counters + 5);
+                        });
                     else
                         with_groups([&](auto width, auto vec) {
                             constexpr int W = decltype(width)::value;
