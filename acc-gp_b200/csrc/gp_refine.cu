@@ -2404,9 +2404,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     if (cut != best || cut > feasible_start || max_load_host > C) fail(GP_INTERNAL, "incremental refinement postcondition failed");
     if (log)
         std::printf("refine_level vertices=%lld initial_cut=%llu final_cut=%llu rounds=%d repair_iterations=%lld "
-                    "repair_donors=%lld\n", static_cast<long long>(n), static_cast<unsigned long long>(feasible_start),
-                    static_cast<unsigned long long>(cut), rounds, static_cast<long long>(repair_iterations),
-                    static_cast<long long>(repair_donors));
+                    "repair_donors=%lld maximum_degree=%llu affinities=%s\n", static_cast<long long>(n),
+                    static_cast<unsigned long long>(feasible_start), static_cast<unsigned long long>(cut), rounds,
+                    static_cast<long long>(repair_iterations), static_cast<long long>(repair_donors),
+                    static_cast<unsigned long long>(g.maximum_degree), on_demand ? "on_demand" : "dense");
     res.cut = cut;
     res.refined = true;
     return res;
