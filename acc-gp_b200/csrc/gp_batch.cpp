@@ -184,6 +184,10 @@ struct gp_server {
                     r.status = GP_CUDA_ERROR;
             }
             r.run_seconds = seconds_since(start);
+            // Arenas only grow, so an idle worker would keep the memory of the
+            // largest request it ran: with a budget, a worker holding more than
+            // its share of it gives the memory back.
+            if (budget && context_reserved(c) > budget / contexts.size()) context_trim(c);
             {
                 std::lock_guard<std::mutex> lock(mu);
                 in_use -= job.bytes;

@@ -342,7 +342,8 @@ __global__ void k_affinity_low(i64 count, const int* rows, RoundParams p) {
     if (row && sub == 0) decode(p, v, src, s);
 }
 
-// Rows of degree 9..256: one warp per row with a 512-slot shared hash
+// Rows of degree 9..256: one warp per row; up to 32 entries one per lane
+// with match_any, longer rows through a 512-slot shared hash
 // (sclp_affinity_medium_hash_kernel, aggregation.cuh:343-422).
 __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count, const int* rows, RoundParams p) {
     __shared__ int keys[kMediumWarps][kMediumHash];
@@ -354,6 +355,26 @@ __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count
         int src;
         if (!is_mover(p, v, src)) continue;
         const i64 begin = p.off[v], end = p.off[v + 1];
+        if (end - begin <= 32) {
+            // One entry per lane: equal clusters are grouped with match_any,
+            // no table needed (as k_affinity_low does for 8 lanes).
+            const i64 e = begin + lane;
+            const int u = e < end ? p.nbr[e] : v;
+            const bool valid = u != v;
+            const int c = valid ? p.clusters[u] : kInvalid;
+            const u64 w = valid ? edge_w(p.ew, e) : 0;
+            const unsigned active = __ballot_sync(0xffffffffu, valid);
+            Summary s{0, 0, 0, 0};
+            if (valid) {
+                const unsigned peers = __match_any_sync(active, c);
+                u64 conn = 0;
+                for (unsigned rem = peers; rem; rem &= rem - 1) conn += __shfl_sync(peers, w, __ffs(rem) - 1);
+                if (lane == __ffs(peers) - 1) consider(p, s, v, src, c, conn);
+            }
+            reduce_summary<32>(s);
+            if (lane == 0) decode(p, v, src, s);
+            continue;
+        }
         int size = 32;
         while (size < 2 * (end - begin)) size <<= 1;
         for (int sl = lane; sl < size; sl += 32) { keys[wib][sl] = -1; vals[wib][sl] = 0; }

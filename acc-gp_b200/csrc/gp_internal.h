@@ -20,6 +20,9 @@ struct WorkerPool;
 WorkerPool*& worker_pool(gp_context* ctx);
 void destroy_worker_pool(WorkerPool* pool);
 int context_device(const gp_context* ctx);
+// Device bytes a context's arenas hold, and their release.
+size_t context_reserved(const gp_context* ctx);
+void context_trim(gp_context* ctx);
 void copy_options(const gp_context* from, gp_context* to);
 
 }  // namespace gp

@@ -28,6 +28,13 @@ namespace gp {
 
 WorkerPool*& worker_pool(gp_context* ctx) { return ctx->pool; }
 int context_device(const gp_context* ctx) { return ctx->ctx.device; }
+size_t context_reserved(const gp_context* ctx) { return ctx->ctx.persist.reserved() + ctx->ctx.scratch.reserved(); }
+void context_trim(gp_context* ctx) {
+    cudaSetDevice(ctx->ctx.device);
+    cudaStreamSynchronize(ctx->ctx.stream);
+    ctx->ctx.persist.reset_device();
+    ctx->ctx.scratch.reset_device();
+}
 void copy_options(const gp_context* from, gp_context* to) {
     to->seed_matching = from->seed_matching;
     to->fast_path = from->fast_path;

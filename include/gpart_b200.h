@@ -180,8 +180,9 @@ gp_status gp_partition_batch(gp_context* ctx, gp_request* requests, int32_t coun
  * estimated device footprint fits in what is left of hbm_budget_bytes
  * (0: no limit) among the requests running; smaller requests may pass a
  * waiting larger one.  Graphs added with gp_server_add_graph stay resident
- * on the device and are partitioned without an upload.  No counterpart in
- * the reference. */
+ * on the device and are partitioned without an upload.  With a budget, a
+ * worker whose device arenas hold more than budget/workers after a request
+ * releases them.  No counterpart in the reference. */
 typedef struct gp_server gp_server;
 gp_status gp_server_create(int device, int32_t workers, uint64_t hbm_budget_bytes, gp_server** out);
 /* Uploads a host CSR once; requests name it by *graph_id. */
