@@ -24,6 +24,7 @@ namespace {
 constexpr int kLowDegree = 8;       // SCLP_LOW_DEGREE
 constexpr int kMediumDegree = 256;  // SCLP_MEDIUM_DEGREE
 constexpr int kLargeDegree = kHeavyRow;   // rows above use a chunked global table
+constexpr int kLargeNarrow = 1024;  // large rows up to this take a half-size shared table
 constexpr int kMediumHash = 512;          // SCLP_MEDIUM_HASH_SIZE
 constexpr int kLargeHash = 2 * kHeavyRow; // shared-memory table of the large class
 constexpr int kSegment = 4096;            // table slots summarised per block
@@ -120,11 +121,13 @@ __global__ void k_weight_sum(i64 m, const u32* ew, u64* out) {
 }
 
 // Degree classes (sclp_compact_degree_classes, aggregation.cuh:5-71): exact
-// max degree, heavy flag and class lists.  Scalars: 0 max degree, 1 heavy,
-// 2..5 list sizes (low, medium, large, heavy), 6 heavy hash slots,
-// 7 isolated vertices.
+// max degree, heavy flag and class lists.  The reference's large class is
+// split at kLargeNarrow so that its shorter rows run with half the shared
+// table.  Scalars: 0 max degree, 1 heavy, 2..5 list sizes (low, medium,
+// large up to kLargeNarrow, heavy), 6 heavy hash slots, 7 isolated vertices,
+// 8 list size of the large rows above kLargeNarrow.
 __global__ void __launch_bounds__(256) k_degree_classes(i64 n, const int* off, int* low, int* medium, int* large,
-                                                        int* heavy, u64* sc) {
+                                                        int* heavy, int* large_wide, u64* sc) {
     u64 d_max = 0, isolated = 0;
     int big = 0;
     // Block-uniform passes: the appends synchronise the block.
@@ -135,11 +138,17 @@ __global__ void __launch_bounds__(256) k_degree_classes(i64 n, const int* off, i
         d_max = static_cast<u64>(deg) > d_max ? static_cast<u64>(deg) : d_max;
         big |= valid && deg >= 4096;
         isolated += valid && deg == 0;
-        const int cls = !valid ? -1 : deg <= kLowDegree ? 0 : deg <= kMediumDegree ? 1 : deg <= kLargeDegree ? 2 : 3;
+        const int cls = !valid                ? -1
+                        : deg <= kLowDegree    ? 0
+                        : deg <= kMediumDegree ? 1
+                        : deg <= kLargeNarrow  ? 2
+                        : deg <= kLargeDegree  ? 4
+                                               : 3;
         block_append(static_cast<int>(v), cls == 0, low, sc + 2);
         block_append(static_cast<int>(v), cls == 1, medium, sc + 3);
         block_append(static_cast<int>(v), cls == 2, large, sc + 4);
         block_append(static_cast<int>(v), cls == 3, heavy, sc + 5);
+        block_append(static_cast<int>(v), cls == 4, large_wide, sc + 8);
     }
     block_atomic_max(sc + 0, d_max);
     if (__syncthreads_or(big) && threadIdx.x == 0) atomicOr(sc + 1, 1ULL);
@@ -291,6 +300,46 @@ __device__ __forceinline__ void consider(const RoundParams& p, Summary& s, int v
     add_candidate(s, conn, tie);
 }
 
+// consider() split in two so that callers can issue the role and weight
+// gathers of several clusters before using any of them.
+__device__ __forceinline__ void gather_cluster(const RoundParams& p, int src, int c, unsigned char& role, u64& base) {
+    const bool other = p.filter_roles && c >= 0 && c != src;
+    role = other ? p.roles[c] : 0;
+    base = other ? p.cw[c] : 0;
+}
+__device__ __forceinline__ void consider_gathered(const RoundParams& p, Summary& s, int v, int src, u64 own, int c,
+                                                  u64 conn, unsigned char role, u64 base) {
+    if (c < 0) return;
+    if (c == src) { s.current = conn; return; }
+    if (p.filter_roles && (role || !(base != 0 && base <= p.capacity && own <= p.capacity - base))) return;
+    const u64 tie = (static_cast<u64>(mix32(static_cast<u32>(v) ^ mix32(static_cast<u32>(c)) ^ p.tie_salt)) << 32) |
+                    (0xffffffffULL - static_cast<u32>(c));
+    add_candidate(s, conn, tie);
+}
+
+// consider() for the table slots first, first + stride, ... (key -1 =
+// empty), four slots per step with their gathers in flight together.
+template <class Slot>
+__device__ __forceinline__ void consider_slots(const RoundParams& p, Summary& s, int v, int src, const int* keys,
+                                               const u64* vals, Slot first, Slot size, int stride) {
+    const u64 own = p.filter_roles ? p.cw[src] : 0;
+    for (Slot s0 = first; s0 < size; s0 += 4 * stride) {
+        int c[4];
+        u64 conn[4], base[4];
+        unsigned char role[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const Slot sl = s0 + j * stride;
+            c[j] = sl < size ? keys[sl] : -1;
+            conn[j] = c[j] >= 0 ? vals[sl] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) gather_cluster(p, src, c[j], role[j], base[j]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) consider_gathered(p, s, v, src, own, c[j], conn[j], role[j], base[j]);
+    }
+}
+
 // sclp_decode_gain_kernel (aggregation.cuh:513-557) for a mover row.
 __device__ __forceinline__ void decode(const RoundParams& p, int v, int src, const Summary& s) {
     const u64 gain = s.best > s.current ? s.best - s.current : 0;
@@ -306,6 +355,42 @@ __device__ __forceinline__ void decode(const RoundParams& p, int v, int src, con
 __device__ __forceinline__ bool is_mover(const RoundParams& p, int v, int& src) {
     src = p.clusters[v];
     return p.roles[src] != 0;
+}
+
+// Adds the entries first, first + stride, ... < end of row v into an
+// open-addressing table of clusters (key -1 = empty, linear probing, `mask`
+// = slots - 1).  Four entries per thread go through together, so that their
+// neighbour and cluster gathers and their CASes are in flight at once.
+template <class Index>
+__device__ __forceinline__ void hash_row(const RoundParams& p, int v, Index first, Index end, int stride, int* keys,
+                                         u64* vals, u64 mask) {
+    constexpr int kUnroll = 4;
+    for (Index e0 = first; e0 < end; e0 += kUnroll * stride) {
+        int u[kUnroll], c[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            const Index e = e0 + j * stride;
+            u[j] = e < end ? p.nbr[e] : v;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) c[j] = u[j] != v ? p.clusters[u[j]] : -1;
+        u64 sl[kUnroll];
+        int found[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            sl[j] = mix32(static_cast<u32>(c[j])) & mask;
+            found[j] = c[j] >= 0 ? atomicCAS(keys + sl[j], -1, c[j]) : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            if (c[j] < 0) continue;
+            while (found[j] != -1 && found[j] != c[j]) {
+                sl[j] = (sl[j] + 1) & mask;
+                found[j] = atomicCAS(keys + sl[j], -1, c[j]);
+            }
+            atomicAdd(vals + sl[j], static_cast<u64>(edge_w(p.ew, e0 + j * stride)));
+        }
+    }
 }
 
 // Rows of degree <= 8: one 8-lane group per row; equal clusters are grouped
@@ -379,72 +464,36 @@ __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count
         while (size < 2 * (end - begin)) size <<= 1;
         for (int sl = lane; sl < size; sl += 32) { keys[wib][sl] = -1; vals[wib][sl] = 0; }
         __syncwarp();
-        for (i64 e = begin + lane; e < end; e += 32) {
-            const int u = p.nbr[e];
-            if (u == v) continue;
-            const int c = p.clusters[u];
-            int sl = static_cast<int>(mix32(static_cast<u32>(c))) & (size - 1);
-            while (true) {
-                const int found = atomicCAS(&keys[wib][sl], -1, c);
-                if (found == -1 || found == c) { atomicAdd(&vals[wib][sl], static_cast<u64>(edge_w(p.ew, e))); break; }
-                sl = (sl + 1) & (size - 1);
-            }
-        }
+        hash_row(p, v, begin + lane, end, 32, keys[wib], vals[wib], static_cast<u64>(size - 1));
         __syncwarp();
         Summary s{0, 0, 0, 0};
-        for (int sl = lane; sl < size; sl += 32) {
-            const int c = keys[wib][sl];
-            if (c >= 0) consider(p, s, v, src, c, vals[wib][sl]);
-        }
+        consider_slots(p, s, v, src, keys[wib], vals[wib], lane, size, 32);
         reduce_summary<32>(s);
         if (lane == 0) decode(p, v, src, s);
         __syncwarp();
     }
 }
 
-// Rows of degree > 256: a 256-thread block per row with an open-addressing
-// table in shared memory (<= 4096 entries) or in a per-row global region.
-template <bool Global>
-__global__ void __launch_bounds__(256) k_affinity_large(i64 count, const int* rows, const u64* region_offsets,
-                                                        int* global_keys, u64* global_vals, RoundParams p) {
-    extern __shared__ unsigned char smem_raw[];
+// Rows of degree 257..kLargeDegree: a 256-thread block per row with an
+// open-addressing table in shared memory of at least twice the row's
+// entries (values first, then keys).
+__global__ void __launch_bounds__(256, 5) k_affinity_large(i64 count, const int* rows, RoundParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Summary warp_sum_s[8];
     const int v = rows[blockIdx.x];
     int src;
     if (!is_mover(p, v, src)) return;
     const i64 begin = p.off[v], end = p.off[v + 1];
-    int* keys;
-    u64* vals;
-    u64 size;
-    if (Global) {
-        keys = global_keys + region_offsets[blockIdx.x];
-        vals = global_vals + region_offsets[blockIdx.x];
-        size = heavy_slots(end - begin);
-    } else {
-        vals = reinterpret_cast<u64*>(smem_raw);
-        keys = reinterpret_cast<int*>(vals + kLargeHash);
-        size = 32;
-        while (size < 2 * static_cast<u64>(end - begin)) size <<= 1;
-    }
+    u64 size = 32;
+    while (size < 2 * static_cast<u64>(end - begin)) size <<= 1;
+    u64* vals = reinterpret_cast<u64*>(smem_raw);
+    int* keys = reinterpret_cast<int*>(vals + size);
     for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) { keys[sl] = -1; vals[sl] = 0; }
     __syncthreads();
-    for (i64 e = begin + threadIdx.x; e < end; e += blockDim.x) {
-        const int u = p.nbr[e];
-        if (u == v) continue;
-        const int c = p.clusters[u];
-        u64 sl = mix32(static_cast<u32>(c)) & (size - 1);
-        while (true) {
-            const int found = atomicCAS(&keys[sl], -1, c);
-            if (found == -1 || found == c) { atomicAdd(&vals[sl], static_cast<u64>(edge_w(p.ew, e))); break; }
-            sl = (sl + 1) & (size - 1);
-        }
-    }
+    hash_row(p, v, begin + static_cast<i64>(threadIdx.x), end, static_cast<int>(blockDim.x), keys, vals, size - 1);
     __syncthreads();
     Summary s{0, 0, 0, 0};
-    for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) {
-        const int c = keys[sl];
-        if (c >= 0) consider(p, s, v, src, c, vals[sl]);
-    }
+    consider_slots(p, s, v, src, keys, vals, static_cast<u64>(threadIdx.x), size, static_cast<int>(blockDim.x));
     reduce_summary<32>(s);
     if ((threadIdx.x & 31) == 0) warp_sum_s[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -458,44 +507,58 @@ __global__ void __launch_bounds__(256) k_affinity_large(i64 count, const int* ro
 // Rows above kHeavyRow: every chunk inserts its entries into the row's
 // global open-addressing table; segments of the table are then summarised
 // block-wise and the partial summaries merged per row.
-__global__ void k_affinity_heavy_insert(DGraph g, const u64* table_off, int* keys, u64* vals, RoundParams p) {
+__global__ void __launch_bounds__(256) k_affinity_heavy_insert(DGraph g, const u64* table_off, int* keys, u64* vals,
+                                                                RoundParams p) {
     const int c = blockIdx.x, v = g.chunk_row[c];
     int src;
     if (!is_mover(p, v, src)) return;
     const int h = g.chunk_hidx[c];
     const u64 size = heavy_slots(g.off[v + 1] - g.off[v]);
-    int* K = keys + table_off[h];
-    u64* V = vals + table_off[h];
-    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
-        const int u = p.nbr[e];
-        if (u == v) continue;
-        const int cl = p.clusters[u];
-        u64 sl = mix32(static_cast<u32>(cl)) & (size - 1);
-        while (true) {
-            const int found = atomicCAS(K + sl, -1, cl);
-            if (found == -1 || found == cl) { atomicAdd(V + sl, static_cast<u64>(edge_w(p.ew, e))); break; }
-            sl = (sl + 1) & (size - 1);
-        }
-    }
+    hash_row(p, v, g.chunk_begin[c] + static_cast<int>(threadIdx.x), chunk_end(g, c, v), static_cast<int>(blockDim.x),
+             keys + table_off[h], vals + table_off[h], size - 1);
 }
 // Also empties the slots it read, so the tables start the next round clean
-// without clearing them all.
-__global__ void k_affinity_heavy_summary(const int* heavy, const int* seg_hidx, const int* seg_index,
-                                         const u64* table_off, int* keys, u64* vals, RoundParams p,
-                                         Summary* partial) {
+// without clearing them all.  Each thread holds 16 slots: four 4-slot vector
+// loads of keys issued together, then the values of the occupied ones.
+__global__ void __launch_bounds__(256) k_affinity_heavy_summary(const int* heavy, const int* seg_hidx,
+                                                                 const int* seg_index, const u64* table_off, int* keys,
+                                                                 u64* vals, RoundParams p, Summary* partial) {
+    static_assert(kSegment == 16 * 256, "one segment is 16 slots for each of 256 threads");
     __shared__ Summary warp_part[8];
     const int sg = blockIdx.x, h = seg_hidx[sg], v = heavy[h];
     int src;
     if (!is_mover(p, v, src)) return;
-    const u64 base = table_off[h] + static_cast<u64>(seg_index[sg]) * kSegment;
+    const u64 base = table_off[h] + static_cast<u64>(seg_index[sg]) * kSegment;  // a multiple of 4 slots
+    int4* K4 = reinterpret_cast<int4*>(keys + base);
+    int4 kv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) kv[j] = K4[j * 256 + threadIdx.x];
+    u64 w[16];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int c4[4] = {kv[j].x, kv[j].y, kv[j].z, kv[j].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[4 * j + q] = c4[q] >= 0 ? vals[base + 4 * (static_cast<u64>(j) * 256 + threadIdx.x) + q] : 0;
+    }
     Summary sm{0, 0, 0, 0};
-    for (int i = threadIdx.x; i < kSegment; i += blockDim.x) {
-        const int c = keys[base + i];
-        if (c >= 0) {
-            consider(p, sm, v, src, c, vals[base + i]);
-            keys[base + i] = -1;
-            vals[base + i] = 0;
+    const u64 own = p.filter_roles ? p.cw[src] : 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int c4[4] = {kv[j].x, kv[j].y, kv[j].z, kv[j].w};
+        unsigned char role[4];
+        u64 cwt[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gather_cluster(p, src, c4[q], role[q], cwt[q]);
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (c4[q] < 0) continue;
+            any = true;
+            consider_gathered(p, sm, v, src, own, c4[q], w[4 * j + q], role[q], cwt[q]);
+            vals[base + 4 * (static_cast<u64>(j) * 256 + threadIdx.x) + q] = 0;
         }
+        if (any) K4[j * 256 + threadIdx.x] = make_int4(-1, -1, -1, -1);
     }
     reduce_summary<32>(sm);
     if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sm;
@@ -1272,8 +1335,8 @@ private:
     u64* gains = nullptr;
     u64* regret = nullptr;
     u32* ties = nullptr;
-    int* lists[4] = {};
-    i64 list_size[4] = {};
+    int* lists[5] = {};
+    i64 list_size[5] = {};
     // Global tables of the heavy rows (see k_affinity_heavy_*).
     u64* table_off = nullptr;
     int* table_keys = nullptr;
@@ -1308,16 +1371,17 @@ void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 
         const int blocks = static_cast<int>(std::min<i64>(blocks_for(list_size[1], kMediumWarps), 148 * 64));
         launch(k_affinity_medium, blocks, kMediumWarps * 32, 0, ctx.stream, list_size[1], lists[1], p);
     }
-    if (list_size[2]) {
-        const size_t smem = kLargeHash * (sizeof(u64) + sizeof(int));
+    // Shared tables: 2048 slots (24 KB) for rows up to kLargeNarrow, 4096 (48 KB) above.
+    for (int c : {2, 4}) {
+        if (!list_size[c]) continue;
+        const size_t smem = static_cast<size_t>(c == 2 ? 2 * kLargeNarrow : 2 * kLargeDegree) * (sizeof(u64) + sizeof(int));
         static bool configured = false;
         if (!configured) {
-            GP_CUDA(cudaFuncSetAttribute(k_affinity_large<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
+            GP_CUDA(cudaFuncSetAttribute(k_affinity_large, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(2 * kLargeDegree * (sizeof(u64) + sizeof(int)))));
             configured = true;
         }
-        launch(k_affinity_large<false>, static_cast<int>(list_size[2]), 256, smem, ctx.stream, 
-            list_size[2], lists[2], static_cast<const u64*>(nullptr), static_cast<int*>(nullptr), static_cast<u64*>(nullptr), p);
+        launch(k_affinity_large, static_cast<int>(list_size[c]), 256, smem, ctx.stream, list_size[c], lists[c], p);
     }
     if (g.heavy_count) {
         launch(k_affinity_heavy_insert, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, table_off, table_keys,
@@ -1365,25 +1429,26 @@ AggregateOut Aggregator::run() {
     // Degree classes, once per level.
     i64 isolated = 0;
     {
-        for (int c = 0; c < 4; ++c) lists[c] = nullptr;
+        for (int c = 0; c < 5; ++c) lists[c] = nullptr;
         if (g.maximum_degree <= kLowDegree) {
             out.stats_max_degree = g.maximum_degree;
             out.stats_heavy = false;
             list_size[0] = n;
-            list_size[1] = list_size[2] = list_size[3] = 0;
+            list_size[1] = list_size[2] = list_size[3] = list_size[4] = 0;
             ctx.clear_scalars(1);
             launch(k_count_isolated, vb, kThreads, 0, s, n, g.off, ctx.dev_scalars);
             isolated = static_cast<i64>(ctx.read_scalars(1)[0]);
         } else {
-            int* storage = A.alloc<int>(static_cast<size_t>(n) * 4);
-            for (int c = 0; c < 4; ++c) lists[c] = storage + static_cast<size_t>(n) * c;
-            ctx.clear_scalars(8);
+            int* storage = A.alloc<int>(static_cast<size_t>(n) * 5);
+            for (int c = 0; c < 5; ++c) lists[c] = storage + static_cast<size_t>(n) * c;
+            ctx.clear_scalars(9);
             launch(k_degree_classes, static_cast<int>(std::min<i64>(vb, 148 * 8)), kThreads, 0, s, n, g.off, lists[0],
-                   lists[1], lists[2], lists[3], ctx.dev_scalars);
-            const u64* sc = ctx.read_scalars(8);
+                   lists[1], lists[2], lists[3], lists[4], ctx.dev_scalars);
+            const u64* sc = ctx.read_scalars(9);
             out.stats_max_degree = sc[0];
             out.stats_heavy = sc[1] != 0;
             for (int c = 0; c < 4; ++c) list_size[c] = static_cast<i64>(sc[2 + c]);
+            list_size[4] = static_cast<i64>(sc[8]);
             isolated = static_cast<i64>(sc[7]);
             if (g.heavy_count) {
                 const i64 hc = g.heavy_count;
