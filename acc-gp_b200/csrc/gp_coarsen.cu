@@ -317,29 +317,6 @@ __device__ __forceinline__ void consider_gathered(const RoundParams& p, Summary&
     add_candidate(s, conn, tie);
 }
 
-// consider() for the table slots first, first + stride, ... (key -1 =
-// empty), four slots per step with their gathers in flight together.
-template <class Slot>
-__device__ __forceinline__ void consider_slots(const RoundParams& p, Summary& s, int v, int src, const int* keys,
-                                               const u64* vals, Slot first, Slot size, int stride) {
-    const u64 own = p.filter_roles ? p.cw[src] : 0;
-    for (Slot s0 = first; s0 < size; s0 += 4 * stride) {
-        int c[4];
-        u64 conn[4], base[4];
-        unsigned char role[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const Slot sl = s0 + j * stride;
-            c[j] = sl < size ? keys[sl] : -1;
-            conn[j] = c[j] >= 0 ? vals[sl] : 0;
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) gather_cluster(p, src, c[j], role[j], base[j]);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) consider_gathered(p, s, v, src, own, c[j], conn[j], role[j], base[j]);
-    }
-}
-
 // sclp_decode_gain_kernel (aggregation.cuh:513-557) for a mover row.
 __device__ __forceinline__ void decode(const RoundParams& p, int v, int src, const Summary& s) {
     const u64 gain = s.best > s.current ? s.best - s.current : 0;
@@ -357,39 +334,106 @@ __device__ __forceinline__ bool is_mover(const RoundParams& p, int v, int& src) 
     return p.roles[src] != 0;
 }
 
-// Adds the entries first, first + stride, ... < end of row v into an
-// open-addressing table of clusters (key -1 = empty, linear probing, `mask`
-// = slots - 1).  Four entries per thread go through together, so that their
-// neighbour and cluster gathers and their CASes are in flight at once.
-template <class Index>
-__device__ __forceinline__ void hash_row(const RoundParams& p, int v, Index first, Index end, int stride, int* keys,
-                                         u64* vals, u64 mask) {
+// Open-addressing tables of (cluster, connection) for the medium, large and
+// heavy affinity classes, linear probing.  SplitTable: int keys (-1 = empty)
+// and u64 connections, two atomics per entry.  PackedTable: one u64 per slot,
+// the cluster in the high 32 bits (all ones = empty) and the connection in the
+// low 32; used when every row's weight sum is below 2^32, so a slot's sum
+// never carries into its key: the CAS that claims a slot deposits the first
+// weight, one atomic per entry, 8 bytes per slot instead of 12.
+struct SplitTable {
+    int* keys;
+    u64* vals;
+    static constexpr bool kClaimCarriesWeight = false;
+    static constexpr size_t kSlotBytes = sizeof(int) + sizeof(u64);
+    __device__ __forceinline__ void clear(u64 sl) const { keys[sl] = -1; vals[sl] = 0; }
+    // Previous key of the slot (-1: it was empty and now holds c).
+    __device__ __forceinline__ int claim(u64 sl, int c, u32) const { return atomicCAS(keys + sl, -1, c); }
+    __device__ __forceinline__ void add(u64 sl, u32 w) const { atomicAdd(vals + sl, static_cast<u64>(w)); }
+    __device__ __forceinline__ void read(u64 sl, int& c, u64& conn) const {
+        c = keys[sl];
+        conn = c >= 0 ? vals[sl] : 0;
+    }
+};
+constexpr u64 kEmptySlot = 0xffffffff00000000ULL;
+struct PackedTable {
+    int* keys;  // unused
+    u64* vals;  // the packed slots
+    static constexpr bool kClaimCarriesWeight = true;
+    static constexpr size_t kSlotBytes = sizeof(u64);
+    __device__ __forceinline__ void clear(u64 sl) const { vals[sl] = kEmptySlot; }
+    __device__ __forceinline__ int claim(u64 sl, int c, u32 w) const {
+        const u64 prev = atomicCAS(vals + sl, kEmptySlot, (static_cast<u64>(static_cast<u32>(c)) << 32) | w);
+        return static_cast<int>(prev >> 32);
+    }
+    __device__ __forceinline__ void add(u64 sl, u32 w) const { atomicAdd(vals + sl, static_cast<u64>(w)); }
+    __device__ __forceinline__ void read(u64 sl, int& c, u64& conn) const {
+        const u64 x = vals[sl];
+        c = static_cast<int>(x >> 32);
+        conn = x & 0xffffffffULL;
+    }
+};
+
+// Adds the entries first, first + stride, ... < end of row v into table T
+// of mask + 1 slots.  Four entries per thread go through together, so that
+// their neighbour and cluster gathers and their claims are in flight at once.
+template <class Table, class Index>
+__device__ __forceinline__ void hash_row(const RoundParams& p, int v, Index first, Index end, int stride, const Table& T,
+                                         u64 mask) {
     constexpr int kUnroll = 4;
     for (Index e0 = first; e0 < end; e0 += kUnroll * stride) {
         int u[kUnroll], c[kUnroll];
+        u32 w[kUnroll];
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
             const Index e = e0 + j * stride;
             u[j] = e < end ? p.nbr[e] : v;
         }
 #pragma unroll
-        for (int j = 0; j < kUnroll; ++j) c[j] = u[j] != v ? p.clusters[u[j]] : -1;
+        for (int j = 0; j < kUnroll; ++j) {
+            c[j] = u[j] != v ? p.clusters[u[j]] : -1;
+            w[j] = u[j] != v ? edge_w(p.ew, e0 + j * stride) : 0;
+        }
         u64 sl[kUnroll];
-        int found[kUnroll];
+        int prev[kUnroll];
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
             sl[j] = mix32(static_cast<u32>(c[j])) & mask;
-            found[j] = c[j] >= 0 ? atomicCAS(keys + sl[j], -1, c[j]) : -1;
+            prev[j] = c[j] >= 0 ? T.claim(sl[j], c[j], w[j]) : -1;
         }
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
             if (c[j] < 0) continue;
-            while (found[j] != -1 && found[j] != c[j]) {
+            while (prev[j] != -1 && prev[j] != c[j]) {
                 sl[j] = (sl[j] + 1) & mask;
-                found[j] = atomicCAS(keys + sl[j], -1, c[j]);
+                prev[j] = T.claim(sl[j], c[j], w[j]);
             }
-            atomicAdd(vals + sl[j], static_cast<u64>(edge_w(p.ew, e0 + j * stride)));
+            if (prev[j] == c[j] || !Table::kClaimCarriesWeight) T.add(sl[j], w[j]);
         }
+    }
+}
+
+// consider() for the table slots first, first + stride, ... < size, four
+// slots per step with their gathers in flight together.
+template <class Table, class Slot>
+__device__ __forceinline__ void consider_slots(const RoundParams& p, Summary& s, int v, int src, const Table& T,
+                                               Slot first, Slot size, int stride) {
+    const u64 own = p.filter_roles ? p.cw[src] : 0;
+    for (Slot s0 = first; s0 < size; s0 += 4 * stride) {
+        int c[4];
+        u64 conn[4], base[4];
+        unsigned char role[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const Slot sl = s0 + j * stride;
+            c[j] = -1;
+            conn[j] = 0;
+            if (sl < size) T.read(sl, c[j], conn[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) gather_cluster(p, src, c[j], role[j], base[j]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) consider_gathered(p, s, v, src, own, c[j], conn[j], role[j], base[j]);
     }
 }
 
@@ -430,10 +474,12 @@ __global__ void k_affinity_low(i64 count, const int* rows, RoundParams p) {
 // Rows of degree 9..256: one warp per row; up to 32 entries one per lane
 // with match_any, longer rows through a 512-slot shared hash
 // (sclp_affinity_medium_hash_kernel, aggregation.cuh:343-422).
+template <class Table>
 __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count, const int* rows, RoundParams p) {
-    __shared__ int keys[kMediumWarps][kMediumHash];
-    __shared__ u64 vals[kMediumWarps][kMediumHash];
+    __shared__ __align__(16) unsigned char raw[kMediumWarps * kMediumHash * Table::kSlotBytes];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    u64* vals = reinterpret_cast<u64*>(raw);
+    const Table T{reinterpret_cast<int*>(vals + kMediumWarps * kMediumHash) + wib * kMediumHash, vals + wib * kMediumHash};
     for (i64 index = static_cast<i64>(blockIdx.x) * kMediumWarps + wib; index < count;
          index += static_cast<i64>(gridDim.x) * kMediumWarps) {
         const int v = rows[index];
@@ -462,12 +508,12 @@ __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count
         }
         int size = 32;
         while (size < 2 * (end - begin)) size <<= 1;
-        for (int sl = lane; sl < size; sl += 32) { keys[wib][sl] = -1; vals[wib][sl] = 0; }
+        for (int sl = lane; sl < size; sl += 32) T.clear(sl);
         __syncwarp();
-        hash_row(p, v, begin + lane, end, 32, keys[wib], vals[wib], static_cast<u64>(size - 1));
+        hash_row(p, v, begin + lane, end, 32, T, static_cast<u64>(size - 1));
         __syncwarp();
         Summary s{0, 0, 0, 0};
-        consider_slots(p, s, v, src, keys[wib], vals[wib], lane, size, 32);
+        consider_slots(p, s, v, src, T, lane, size, 32);
         reduce_summary<32>(s);
         if (lane == 0) decode(p, v, src, s);
         __syncwarp();
@@ -477,6 +523,7 @@ __global__ void __launch_bounds__(kMediumWarps * 32) k_affinity_medium(i64 count
 // Rows of degree 257..kLargeDegree: a 256-thread block per row with an
 // open-addressing table in shared memory of at least twice the row's
 // entries (values first, then keys).
+template <class Table>
 __global__ void __launch_bounds__(256, 5) k_affinity_large(i64 count, const int* rows, RoundParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Summary warp_sum_s[8];
@@ -487,13 +534,13 @@ __global__ void __launch_bounds__(256, 5) k_affinity_large(i64 count, const int*
     u64 size = 32;
     while (size < 2 * static_cast<u64>(end - begin)) size <<= 1;
     u64* vals = reinterpret_cast<u64*>(smem_raw);
-    int* keys = reinterpret_cast<int*>(vals + size);
-    for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) { keys[sl] = -1; vals[sl] = 0; }
+    const Table T{reinterpret_cast<int*>(vals + size), vals};
+    for (u64 sl = threadIdx.x; sl < size; sl += blockDim.x) T.clear(sl);
     __syncthreads();
-    hash_row(p, v, begin + static_cast<i64>(threadIdx.x), end, static_cast<int>(blockDim.x), keys, vals, size - 1);
+    hash_row(p, v, begin + static_cast<i64>(threadIdx.x), end, static_cast<int>(blockDim.x), T, size - 1);
     __syncthreads();
     Summary s{0, 0, 0, 0};
-    consider_slots(p, s, v, src, keys, vals, static_cast<u64>(threadIdx.x), size, static_cast<int>(blockDim.x));
+    consider_slots(p, s, v, src, T, static_cast<u64>(threadIdx.x), size, static_cast<int>(blockDim.x));
     reduce_summary<32>(s);
     if ((threadIdx.x & 31) == 0) warp_sum_s[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -507,6 +554,7 @@ __global__ void __launch_bounds__(256, 5) k_affinity_large(i64 count, const int*
 // Rows above kHeavyRow: every chunk inserts its entries into the row's
 // global open-addressing table; segments of the table are then summarised
 // block-wise and the partial summaries merged per row.
+template <class Table>
 __global__ void __launch_bounds__(256) k_affinity_heavy_insert(DGraph g, const u64* table_off, int* keys, u64* vals,
                                                                 RoundParams p) {
     const int c = blockIdx.x, v = g.chunk_row[c];
@@ -515,51 +563,40 @@ __global__ void __launch_bounds__(256) k_affinity_heavy_insert(DGraph g, const u
     const int h = g.chunk_hidx[c];
     const u64 size = heavy_slots(g.off[v + 1] - g.off[v]);
     hash_row(p, v, g.chunk_begin[c] + static_cast<int>(threadIdx.x), chunk_end(g, c, v), static_cast<int>(blockDim.x),
-             keys + table_off[h], vals + table_off[h], size - 1);
+             Table{keys + table_off[h], vals + table_off[h]}, size - 1);
 }
 // Also empties the slots it read, so the tables start the next round clean
-// without clearing them all.  Each thread holds 16 slots: four 4-slot vector
-// loads of keys issued together, then the values of the occupied ones.
+// without clearing them all.  Each thread holds 16 slots of the segment,
+// 256 apart, all loaded before any is used.
+template <class Table>
 __global__ void __launch_bounds__(256) k_affinity_heavy_summary(const int* heavy, const int* seg_hidx,
                                                                  const int* seg_index, const u64* table_off, int* keys,
                                                                  u64* vals, RoundParams p, Summary* partial) {
-    static_assert(kSegment == 16 * 256, "one segment is 16 slots for each of 256 threads");
+    constexpr int kPerThread = kSegment / 256;
     __shared__ Summary warp_part[8];
     const int sg = blockIdx.x, h = seg_hidx[sg], v = heavy[h];
     int src;
     if (!is_mover(p, v, src)) return;
-    const u64 base = table_off[h] + static_cast<u64>(seg_index[sg]) * kSegment;  // a multiple of 4 slots
-    int4* K4 = reinterpret_cast<int4*>(keys + base);
-    int4 kv[4];
+    const u64 base = table_off[h] + static_cast<u64>(seg_index[sg]) * kSegment + threadIdx.x;
+    const Table T{keys + base, vals + base};
+    int c[kPerThread];
+    u64 conn[kPerThread];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) kv[j] = K4[j * 256 + threadIdx.x];
-    u64 w[16];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int c4[4] = {kv[j].x, kv[j].y, kv[j].z, kv[j].w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            w[4 * j + q] = c4[q] >= 0 ? vals[base + 4 * (static_cast<u64>(j) * 256 + threadIdx.x) + q] : 0;
-    }
+    for (int j = 0; j < kPerThread; ++j) T.read(static_cast<u64>(j) * 256, c[j], conn[j]);
     Summary sm{0, 0, 0, 0};
     const u64 own = p.filter_roles ? p.cw[src] : 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int c4[4] = {kv[j].x, kv[j].y, kv[j].z, kv[j].w};
+    for (int j0 = 0; j0 < kPerThread; j0 += 4) {
         unsigned char role[4];
         u64 cwt[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) gather_cluster(p, src, c4[q], role[q], cwt[q]);
-        bool any = false;
+        for (int q = 0; q < 4; ++q) gather_cluster(p, src, c[j0 + q], role[q], cwt[q]);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (c4[q] < 0) continue;
-            any = true;
-            consider_gathered(p, sm, v, src, own, c4[q], w[4 * j + q], role[q], cwt[q]);
-            vals[base + 4 * (static_cast<u64>(j) * 256 + threadIdx.x) + q] = 0;
-        }
-        if (any) K4[j * 256 + threadIdx.x] = make_int4(-1, -1, -1, -1);
+        for (int q = 0; q < 4; ++q) consider_gathered(p, sm, v, src, own, c[j0 + q], conn[j0 + q], role[q], cwt[q]);
     }
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j)
+        if (c[j] >= 0) T.clear(static_cast<u64>(j) * 256);
     reduce_summary<32>(sm);
     if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = sm;
     __syncthreads();
@@ -1339,8 +1376,9 @@ private:
     i64 list_size[5] = {};
     // Global tables of the heavy rows (see k_affinity_heavy_*).
     u64* table_off = nullptr;
-    int* table_keys = nullptr;
-    u64* table_vals = nullptr;
+    int* table_keys = nullptr;  // SplitTable keys (unused when packed)
+    u64* table_vals = nullptr;  // SplitTable connections, or PackedTable slots
+    bool packed = false;        // every row's weight sum below 2^32: PackedTable
     u64 table_slots = 0;
     int* seg_off = nullptr;
     int* seg_hidx = nullptr;
@@ -1355,6 +1393,28 @@ private:
         return ctx.read_scalars(1)[0];
     }
     void form_proposals(u64 capacity, int round, bool filter_roles, u32 threshold, bool need_regret);
+    // Table-based classes: medium, large (two table sizes) and heavy rows.
+    template <class Table>
+    void launch_tables(const RoundParams& p) {
+        if (list_size[1]) {
+            const int blocks = static_cast<int>(std::min<i64>(blocks_for(list_size[1], kMediumWarps), 148 * 64));
+            launch(k_affinity_medium<Table>, blocks, kMediumWarps * 32, 0, ctx.stream, list_size[1], lists[1], p);
+        }
+        // Shared tables of 2048 slots for rows up to kLargeNarrow, 4096 above.
+        for (int c : {2, 4}) {
+            if (!list_size[c]) continue;
+            const size_t smem = static_cast<size_t>(c == 2 ? 2 * kLargeNarrow : 2 * kLargeDegree) * Table::kSlotBytes;
+            GP_CUDA(cudaFuncSetAttribute(k_affinity_large<Table>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+            launch(k_affinity_large<Table>, static_cast<int>(list_size[c]), 256, smem, ctx.stream, list_size[c], lists[c], p);
+        }
+        if (g.heavy_count) {
+            launch(k_affinity_heavy_insert<Table>, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, table_off,
+                   table_keys, table_vals, p);
+            launch(k_affinity_heavy_summary<Table>, static_cast<int>(segments), 256, 0, ctx.stream, g.heavy, seg_hidx,
+                   seg_index, table_off, table_keys, table_vals, p, partial);
+        }
+    }
 };
 
 void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 threshold, bool need_regret) {
@@ -1367,27 +1427,9 @@ void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 
                   filter_roles && need_regret, proposals, gains, regret, ties};
     if (list_size[0])
         launch(k_affinity_low, blocks_for(list_size[0] * 8, kThreads), kThreads, 0, ctx.stream, list_size[0], lists[0], p);
-    if (list_size[1]) {
-        const int blocks = static_cast<int>(std::min<i64>(blocks_for(list_size[1], kMediumWarps), 148 * 64));
-        launch(k_affinity_medium, blocks, kMediumWarps * 32, 0, ctx.stream, list_size[1], lists[1], p);
-    }
-    // Shared tables: 2048 slots (24 KB) for rows up to kLargeNarrow, 4096 (48 KB) above.
-    for (int c : {2, 4}) {
-        if (!list_size[c]) continue;
-        const size_t smem = static_cast<size_t>(c == 2 ? 2 * kLargeNarrow : 2 * kLargeDegree) * (sizeof(u64) + sizeof(int));
-        static bool configured = false;
-        if (!configured) {
-            GP_CUDA(cudaFuncSetAttribute(k_affinity_large, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(2 * kLargeDegree * (sizeof(u64) + sizeof(int)))));
-            configured = true;
-        }
-        launch(k_affinity_large, static_cast<int>(list_size[c]), 256, smem, ctx.stream, list_size[c], lists[c], p);
-    }
+    if (packed) launch_tables<PackedTable>(p);
+    else launch_tables<SplitTable>(p);
     if (g.heavy_count) {
-        launch(k_affinity_heavy_insert, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, table_off, table_keys,
-               table_vals, p);
-        launch(k_affinity_heavy_summary, static_cast<int>(segments), 256, 0, ctx.stream, g.heavy, seg_hidx, seg_index,
-               table_off, table_keys, table_vals, p, partial);
         launch(k_affinity_heavy_finish, blocks_for(g.heavy_count * 32, kThreads), kThreads, 0, ctx.stream,
                g.heavy_count, g.heavy, seg_off, partial, p);
     }
@@ -1426,6 +1468,8 @@ AggregateOut Aggregator::run() {
     } else {
         launch(k_iota_clusters, vb, kThreads, 0, s, n, g.vw, clusters, cw);
     }
+    // A slot's connection is at most its row's weight sum.
+    packed = ws.maximum_row_weight < 0xffffffffULL;
     // Degree classes, once per level.
     i64 isolated = 0;
     {
@@ -1460,11 +1504,15 @@ AggregateOut Aggregator::run() {
                 const u64* hs = ctx.read_scalars(2);
                 table_slots = hs[0];
                 segments = static_cast<i64>(hs[1] & 0xffffffffULL);
-                table_keys = A.alloc<int>(table_slots);
                 table_vals = A.alloc<u64>(table_slots);
+                table_keys = packed ? nullptr : A.alloc<int>(table_slots);
                 // Cleared once; every round's summary empties what it used.
-                GP_CUDA(cudaMemsetAsync(table_keys, 0xff, sizeof(int) * table_slots, s));
-                GP_CUDA(cudaMemsetAsync(table_vals, 0, sizeof(u64) * table_slots, s));
+                if (packed) {
+                    fill<u64>(s, table_vals, static_cast<i64>(table_slots), kEmptySlot);
+                } else {
+                    GP_CUDA(cudaMemsetAsync(table_keys, 0xff, sizeof(int) * table_slots, s));
+                    GP_CUDA(cudaMemsetAsync(table_vals, 0, sizeof(u64) * table_slots, s));
+                }
                 seg_hidx = A.alloc<int>(segments);
                 seg_index = A.alloc<int>(segments);
                 partial = A.alloc<Summary>(segments);

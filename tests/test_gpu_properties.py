@@ -57,6 +57,22 @@ def test_weighted_rmat(gp, ctx, oracle):
     np.testing.assert_array_equal(labels, oracle.partition(g, 50, 1.05, 4)[0])
 
 
+def test_row_weight_sums_beyond_32_bits(gp, ctx, oracle):
+    """Edge weights of 2^20..2^21 on hubs of thousands of entries: row weight
+    sums exceed 32 bits, so the coarsening affinity tables keep clusters and
+    connections apart instead of packing both into one 64-bit slot.  (Coarse
+    edge weights are 32-bit sums of parallel edges, as in the reference, so the
+    weights stay small enough for those sums.)"""
+    g = gp.with_weights(gp.rmat(16, 16, 0.57, 0.19, 0.19, 6), 13, (1, 8), (1 << 20, 1 << 21))
+    degree = np.diff(g.offsets)
+    assert int(degree.max()) > 2048  # heavy rows: global tables too
+    row_sums = np.add.reduceat(g.edge_weights.astype(np.uint64), g.offsets[:-1][degree > 0])
+    assert int(row_sums.max()) >= 1 << 32
+    labels, st = ctx.partition(g, 64, 1.03, 2)
+    check(gp, g, labels, st, 64, 1.03)
+    np.testing.assert_array_equal(labels, oracle.partition(g, 64, 1.03, 2)[0])
+
+
 def test_fewer_vertices_than_parts_is_rejected(gp, ctx):
     g = gp.grid2d(3, 3)
     with pytest.raises(gp.GpartError) as e:
