@@ -13,6 +13,7 @@
 #include "gp_primitives.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 
 namespace gp {
@@ -1842,8 +1843,10 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
                               (avg < 8 || current.maximum_degree <= 256) && avg < o.heavy_limit && ws.sorted_unique &&
                               ws.positive;
         const Arena::Mark mark = ctx.scratch.mark();
+        const auto t_begin = std::chrono::steady_clock::now();
         Aggregator aggregator(ctx, current, ws, o, level, factor, level_seed, matching);
         AggregateOut agg = aggregator.run();
+        const auto t_aggregated = std::chrono::steady_clock::now();
         current.has_heavy_rows = agg.stats_heavy;
         current.maximum_degree = agg.stats_max_degree;
         const double ratio = static_cast<double>(agg.nc) / static_cast<double>(current.n);
@@ -1858,6 +1861,13 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
         }
         DGraph coarse = contract(ctx, current, agg, ws);
         ctx.scratch.release(mark);
+        if (o.log) {  // host time per stage; the stream is drained first
+            GP_CUDA(cudaStreamSynchronize(s));
+            const auto t_contracted = std::chrono::steady_clock::now();
+            std::printf("ml_level_time level=%d aggregate_ms=%.3f contract_ms=%.3f\n", level,
+                        std::chrono::duration<double, std::milli>(t_aggregated - t_begin).count(),
+                        std::chrono::duration<double, std::milli>(t_contracted - t_aggregated).count());
+        }
         if (o.verify) {
             verify_level(ctx, current, coarse, agg.map, agg.capacity);
             if (o.log) std::printf("ml_layer_verify level=%d map=ok weights=ok csr=ok projection_cut=ok\n", level);

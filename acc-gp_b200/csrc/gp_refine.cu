@@ -9,6 +9,7 @@
 #include "gp_primitives.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <climits>
 #include <type_traits>
@@ -1314,13 +1315,23 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                     const u64 w = vw[v];
                     const int src = labels[v];
                     const u64 t0 = tried[2 * i], t1 = tried[2 * i + 1];
+                    const C* row = A + static_cast<i64>(v) * k;
                     u64 best = 0, room = 0;
-                    for (int p = 0; p < k; ++p) {
-                        if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
-                        const u64 avail = s_requests[p] < s_slack[p] ? s_slack[p] - s_requests[p] : 0;
-                        if (avail < w) continue;
-                        const u64 c = A[static_cast<i64>(v) * k + p];
-                        if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                    // Eight affinities loaded together, then scanned in part order.
+                    for (int p0 = 0; p0 < k; p0 += 8) {
+                        C c8[8];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) c8[q] = p0 + q < k ? row[p0 + q] : C(0);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int p = p0 + q;
+                            if (p >= k) break;
+                            if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+                            const u64 avail = s_avail[p];
+                            if (avail < w) continue;
+                            const u64 c = c8[q];
+                            if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                        }
                     }
                 }
                 if (target < 0) state[i] = 2;
@@ -1502,36 +1513,64 @@ __global__ void k_quotient(i64 n, const int* labels, const C* A, int k, u64* quo
         }
     }
 }
-// joint_match (exchange.cuh:55-82): rounds of mutual best choices.
-__global__ void k_match_parts(int k, const u64* quotient, int* partner, int* visits) {
-    __shared__ int choice[128], progress;
-    const int p = threadIdx.x;
-    if (p < k) partner[p] = -1;
-    __syncthreads();
-    for (int round = 0; round < k / 2; ++round) {
-        if (!p) progress = 0;
-        int best = -1;
+// joint_match (exchange.cuh:55-82): rounds of mutual best choices.  The
+// pair scores quotient / (1 + visits)^2 are computed once into shared memory
+// (a pair's visits change only when it is matched, after which neither part
+// takes part in later rounds); each round a warp per part picks its best
+// unmatched partner, the highest score and on ties the lowest part.
+constexpr int kMatchThreads = 1024;
+__global__ void __launch_bounds__(kMatchThreads) k_match_parts(int k, const u64* quotient, int* partner, int* visits) {
+    extern __shared__ double s_score[];  // k * k, pair (a, b) with a < b at a * k + b; -1 = no edge
+    __shared__ int s_partner[kMaxParts], s_choice[kMaxParts], s_progress;
+    for (int x = threadIdx.x; x < k * k; x += blockDim.x) {
+        const int a = x / k, b = x % k;
         double score = -1;
-        if (p < k && partner[p] < 0)
-            for (int q = 0; q < k; ++q)
-                if (q != p && partner[q] < 0) {
-                    const int pair = min(p, q) * k + max(p, q);
-                    if (!quotient[pair]) continue;
-                    const double penalty = 1.0 + visits[pair];
-                    const double value = __ddiv_rn(static_cast<double>(quotient[pair]), __dmul_rn(penalty, penalty));
-                    if (value > score || (value == score && q < best)) { score = value; best = q; }
+        if (a < b && quotient[x]) {
+            const double penalty = 1.0 + visits[x];
+            score = __ddiv_rn(static_cast<double>(quotient[x]), __dmul_rn(penalty, penalty));
+        }
+        s_score[x] = score;
+    }
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_partner[p] = -1;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int round = 0; round < k / 2; ++round) {
+        if (threadIdx.x == 0) s_progress = 0;
+        for (int p = warp; p < k; p += warps) {
+            double score = -1;
+            int best = -1;
+            if (s_partner[p] < 0) {
+                for (int q = lane; q < k; q += 32) {
+                    if (q == p || s_partner[q] >= 0) continue;
+                    const double value = s_score[min(p, q) * k + max(p, q)];
+                    if (value > score) { score = value; best = q; }
                 }
-        if (p < k) choice[p] = best;
-        __syncthreads();
-        if (p < k && best >= 0 && choice[best] == p) {
-            partner[p] = best;
-            if (p < best) { ++visits[p * k + best]; atomicAdd(&progress, 1); }
+            }
+#pragma unroll
+            for (int d = 16; d; d >>= 1) {
+                const double other = __shfl_xor_sync(0xffffffffu, score, d);
+                const int other_best = __shfl_xor_sync(0xffffffffu, best, d);
+                if (other > score || (other == score && other_best >= 0 && (best < 0 || other_best < best))) {
+                    score = other;
+                    best = other_best;
+                }
+            }
+            if (lane == 0) s_choice[p] = best;
         }
         __syncthreads();
-        const int gained = progress;
+        if (threadIdx.x < k) {
+            const int p = threadIdx.x, best = s_choice[p];
+            if (best >= 0 && s_choice[best] == p) {
+                s_partner[p] = best;
+                if (p < best) { ++visits[p * k + best]; atomicAdd(&s_progress, 1); }
+            }
+        }
+        __syncthreads();
+        const int gained = s_progress;
         __syncthreads();
         if (!gained) break;
     }
+    for (int p = threadIdx.x; p < k; p += blockDim.x) partner[p] = s_partner[p];
 }
 // joint_seeds (exchange.cuh:83-93).
 template <class C>
@@ -1742,54 +1781,116 @@ __global__ void k_mark(int count, const JointMove* moves, const int* labels, int
             targets[v] = labels[v] == moves[i].a ? moves[i].b : moves[i].a;
         }
 }
-// joint_events (exchange.cuh:227-262).
-__global__ void k_events(int count, const JointMove* moves, const int* owners, const int* targets, const int* labels,
-                         const int* off, const int* nbr, const u32* ew, u64* events) {
-    const int lane = threadIdx.x & 31, i = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (i >= count || !moves[i].size) return;
-    u64 own = 0;
-    for (int j = 0; j < moves[i].size; ++j) {
-        const int v = moves[i].vertices[j];
-        for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+// joint_events (exchange.cuh:227-262).  The rows of the moves' vertices
+// are cut into chunks of kEventChunk entries, a warp per chunk, so that a
+// hub among a move's vertices does not leave one warp with the whole row.
+// chunk_off[x] (x = move * 8 + vertex slot) is the exclusive prefix of the
+// chunk counts (EventChunks) and *total_chunks their sum.
+constexpr int kEventChunk = 256;
+struct EventChunks {
+    const JointMove* moves;
+    const int* off;
+    __device__ u32 operator()(i64 x) const {
+        const JointMove& m = moves[x >> 3];
+        const int j = static_cast<int>(x & 7);
+        if (j >= m.size) return 0;
+        const int v = m.vertices[j];
+        return static_cast<u32>((off[v + 1] - off[v] + kEventChunk - 1) / kEventChunk);
+    }
+};
+__global__ void k_events(int count, const JointMove* moves, const u32* chunk_off, const u32* total_chunks,
+                         const int* owners, const int* targets, const int* labels, const int* off, const int* nbr,
+                         const u32* ew, u64* events) {
+    const int lane = threadIdx.x & 31;
+    const u32 total = *total_chunks;
+    const int items = count * 8;
+    for (u32 w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += (gridDim.x * blockDim.x) >> 5) {
+        int lo = 0, hi = items - 1;  // the last item whose chunks start at or before w
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (chunk_off[mid] <= w) lo = mid; else hi = mid - 1;
+        }
+        const int i = lo >> 3;
+        const int ma = moves[i].a, mb = moves[i].b, v = moves[i].vertices[lo & 7];
+        const int begin = off[v] + static_cast<int>(w - chunk_off[lo]) * kEventChunk;
+        const int end = min(off[v + 1], begin + kEventChunk);
+        u64 own = 0;
+        for (int e = begin + lane; e < end; e += 32) {
             const int u = nbr[e], other = owners[u];
             if (u == v || (other != INT_MAX && v > u)) continue;
-            if (other != INT_MAX && labels[u] != moves[i].a && labels[u] != moves[i].b) continue;
-            const long long w = edge_w(ew, e);
+            if (other != INT_MAX && labels[u] != ma && labels[u] != mb) continue;
+            const long long wt = edge_w(ew, e);
             const int before = labels[v] != labels[u];
             if (other == i || other == INT_MAX) {
                 const int after = targets[v] != (other == i ? targets[u] : labels[u]);
-                own += static_cast<u64>((before - after) * w);
+                own += static_cast<u64>((before - after) * wt);
             } else {
                 const int middle = i < other ? targets[v] != labels[u] : labels[v] != targets[u];
                 const int after = targets[v] != targets[u];
-                const u64 first = static_cast<u64>((before - middle) * w), last = static_cast<u64>((middle - after) * w);
+                const u64 first = static_cast<u64>((before - middle) * wt), last = static_cast<u64>((middle - after) * wt);
                 own += i < other ? first : last;
                 atomicAdd(events + other, i < other ? last : first);
             }
         }
+        own = warp_sum(own);
+        if (!lane && own) atomicAdd(events + i, own);
     }
-    own = warp_sum(own);
-    if (!lane && own) atomicAdd(events + i, own);
 }
-// joint_prefix (exchange.cuh:263-284).
-__global__ void k_prefix(int count, int k, const JointMove* moves, const u64* events, const u64* loads, u64 capacity,
-                         int* stops) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= k) return;
-    long long gain = 0, net = 0, best = 0;
+// joint_prefix (exchange.cuh:263-284), a block per part a: the running gain
+// and net of a's moves (in order, empty moves adding nothing) are block
+// scans, and the stop is the first feasible move whose running gain is the
+// largest one above zero, the move at which the serial scan last improved.
+constexpr int kPrefixThreads = kScanThreads;
+__global__ void __launch_bounds__(kPrefixThreads) k_prefix(int count, int k, const JointMove* moves, const u64* events,
+                                                           const u64* loads, u64 capacity, int* stops) {
+    __shared__ long long s_scan[9];
+    __shared__ int s_range[2];
+    __shared__ long long s_best_gain[kPrefixThreads / 32];
+    __shared__ int s_best_index[kPrefixThreads / 32];
+    const int a = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < 2) {
+        const int key = a + static_cast<int>(threadIdx.x);  // first move of part a, first after it
+        int low = 0, high = count;
+        while (low < high) { const int mid = (low + high) / 2; if (moves[mid].a < key) low = mid + 1; else high = mid; }
+        s_range[threadIdx.x] = low;
+    }
+    __syncthreads();
+    const int first = s_range[0], last = s_range[1];
+    const long long lo = static_cast<long long>(loads[a]) - static_cast<long long>(capacity);
+    long long gain_carry = 0, net_carry = 0, best = 0;
     int stop = -1;
-    int low = 0, high = count;
-    while (low < high) { const int mid = (low + high) / 2; if (moves[mid].a < a) low = mid + 1; else high = mid; }
-    for (int i = low; i < count && moves[i].a == a; ++i)
-        if (moves[i].size) {
-            gain += static_cast<long long>(events[i]);
-            net += moves[i].net;
-            const int b = moves[i].b;
-            const long long lo = static_cast<long long>(loads[a]) - static_cast<long long>(capacity);
-            const long long hi = static_cast<long long>(capacity) - static_cast<long long>(loads[b]);
+    for (int base = first; base < last; base += kPrefixThreads) {
+        const int i = base + static_cast<int>(threadIdx.x);
+        const bool valid = i < last && moves[i].size;
+        const long long g = valid ? static_cast<long long>(events[i]) : 0;
+        const long long d = valid ? moves[i].net : 0;
+        long long g_total, d_total;
+        const long long gain = gain_carry + block_exclusive_scan(g, g_total, s_scan) + g;
+        const long long net = net_carry + block_exclusive_scan(d, d_total, s_scan) + d;
+        gain_carry += g_total;
+        net_carry += d_total;
+        if (valid) {
+            const long long hi = static_cast<long long>(capacity) - static_cast<long long>(loads[moves[i].b]);
             if (!joint_gap(net, lo, hi) && gain > best) { best = gain; stop = i; }
         }
-    stops[a] = stop;
+    }
+    // Largest gain, earliest move on ties.
+#pragma unroll
+    for (int d = 16; d; d >>= 1) {
+        const long long og = __shfl_xor_sync(0xffffffffu, best, d);
+        const int oi = __shfl_xor_sync(0xffffffffu, stop, d);
+        if (og > best || (og == best && oi >= 0 && (stop < 0 || oi < stop))) { best = og; stop = oi; }
+    }
+    if (!lane) { s_best_gain[warp] = best; s_best_index[warp] = stop; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kPrefixThreads / 32; ++w)
+            if (s_best_gain[w] > best || (s_best_gain[w] == best && s_best_index[w] >= 0 && (stop < 0 || s_best_index[w] < stop))) {
+                best = s_best_gain[w];
+                stop = s_best_index[w];
+            }
+        stops[a] = stop;
+    }
 }
 __global__ void k_accept(int count, const JointMove* moves, const int* stops, int* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2233,7 +2334,9 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
     };
     int empty = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        launch(k_match_parts, 1, 128, 0, s(), k, quotient, partner, visits);
+        const size_t match_smem = sizeof(double) * k * k;
+        GP_CUDA(cudaFuncSetAttribute(k_match_parts, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(match_smem)));
+        launch(k_match_parts, 1, kMatchThreads, match_smem, s(), k, quotient, partner, visits);
         GP_CUDA(cudaMemsetAsync(seeds, 0xff, sizeof(u64) * k * sw, s()));
         launch(k_seeds<T>, grid_for(n, kThreads), kThreads, 0, s(), n, labels, static_cast<const T*>(A), k, partner,
                seeds, sw, pass);
@@ -2262,10 +2365,18 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         launch(k_mark, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
                static_cast<const int*>(labels), owners, targets);
         GP_CUDA(cudaMemsetAsync(events, 0, sizeof(u64) * active, s()));
-        launch(k_events, blocks_for(active, 8), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
-               static_cast<const int*>(owners), static_cast<const int*>(targets), static_cast<const int*>(labels), g.off,
-               g.nbr, g.ew, events);
-        launch(k_prefix, blocks_for(k, 128), 128, 0, s(), active, k, static_cast<const JointMove*>(act_sorted),
+        {
+            ArenaScope es(A_);
+            u32* chunk_off = A_.alloc<u32>(static_cast<size_t>(active) * 8);
+            u32* total_chunks = A_.alloc<u32>(1);
+            exclusive_scan<u32>(A_, s(), static_cast<i64>(active) * 8,
+                                EventChunks{static_cast<const JointMove*>(act_sorted), g.off}, chunk_off, total_chunks);
+            launch(k_events, 148 * 8, kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
+                   static_cast<const u32*>(chunk_off), static_cast<const u32*>(total_chunks),
+                   static_cast<const int*>(owners), static_cast<const int*>(targets), static_cast<const int*>(labels),
+                   g.off, g.nbr, g.ew, events);
+        }
+        launch(k_prefix, k, kPrefixThreads, 0, s(), active, k, static_cast<const JointMove*>(act_sorted),
                static_cast<const u64*>(events), static_cast<const u64*>(loads), C, stops);
         launch(k_accept, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
                static_cast<const int*>(stops), flags);
@@ -2444,9 +2555,17 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
     u64 total = 0, maxload = 0;
     for (int p = 0; p < k; ++p) { total += ctx.host_scalars[p]; maxload = std::max<u64>(maxload, ctx.host_scalars[p]); }
     auto refine = [&](const DGraph& g, int* lab, bool has_known, u64 known) {
-        if (g.incident_bound <= 0xffffffffULL)
-            return LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
-        return LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
+        const auto t_begin = std::chrono::steady_clock::now();
+        const LevelResult r =
+            g.incident_bound <= 0xffffffffULL
+                ? LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known)
+                : LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
+        if (log) {  // host time of the level; the stream is drained first
+            GP_CUDA(cudaStreamSynchronize(s));
+            std::printf("refine_level_time vertices=%lld ms=%.3f\n", static_cast<long long>(g.n),
+                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count());
+        }
+        return r;
     };
     LevelResult res = refine(coarsest, level_labels[L - 1], false, 0);
     u64 last_cut = res.cut;
