@@ -138,7 +138,8 @@ constexpr int kBuildShort = 64;
 template <class C, int W, bool Vectorized>
 __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const int* nbr, const u32* ew,
                                                     const int* labels, int k, C* A, C* totals, u64* directed_cut,
-                                                    const u64* gate, u64 threshold, u64* work, u64 work_bytes) {
+                                                    const u64* gate, u64 threshold, u64* work, u64 work_bytes,
+                                                    bool long_rows_apart) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ WarpSum cut_sum;
     if (gate && *gate <= threshold) return;  // incremental update chosen
@@ -167,7 +168,9 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         if (deg <= kBuildShort) {
             accumulate_row(nbr, ew, labels, static_cast<int>(v), begin + sub, end, W, hist);
         }
-        for (unsigned rest = __ballot_sync(0xffffffffu, deg > kBuildShort && deg <= kHeavyRow) & leaders; rest;
+        // Rows of kBuildShort..kHeavyRow entries go to k_build_long when it runs.
+        const bool mine = valid && !(long_rows_apart && deg > kBuildShort && deg <= kHeavyRow);
+        for (unsigned rest = __ballot_sync(0xffffffffu, mine && deg > kBuildShort && deg <= kHeavyRow) & leaders; rest;
              rest &= rest - 1) {
             const int leader = __ffs(rest) - 1;
             const int vv = static_cast<int>(base) + leader / W;
@@ -177,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         }
         __syncwarp();
         C total = 0;
-        if (valid) {
+        if (mine) {
             C* row = A + v * k;
             for (int p0 = sub * N; p0 < k; p0 += W * N) {
                 if constexpr (Vectorized) {
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
         }
 #pragma unroll
         for (int d = W / 2; d; d >>= 1) total += __shfl_xor_sync(0xffffffffu, total, d, W);
-        if (valid && sub == 0) {
+        if (mine && sub == 0) {
             totals[v] = total;
             if (directed_cut) cut += static_cast<u64>(total - hist[labels[v]]);
         }
@@ -201,6 +204,60 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
     }
     if (directed_cut) cut_sum.finish(warp_sum(cut), directed_cut);
 }
+
+// The rows of kBuildShort..kHeavyRow entries (listed in `rows`), a warp per
+// row: taken off a list, they spread evenly over all warps instead of
+// stalling the warps of k_build that drew them.
+template <class C>
+__global__ void __launch_bounds__(kThreads) k_build_long(i64 count, const int* rows, const int* off, const int* nbr,
+                                                         const u32* ew, const int* labels, int k, C* A, C* totals,
+                                                         u64* directed_cut, const u64* gate, u64 threshold, u64* work,
+                                                         u64 work_bytes) {
+    extern __shared__ __align__(16) unsigned char smem_long[];
+    __shared__ WarpSum cut_sum;
+    if (gate && *gate <= threshold) return;
+    if (work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(work, work_bytes);
+    cut_sum.init();
+    const int lane = threadIdx.x & 31;
+    C* hist = reinterpret_cast<C*>(smem_long) + static_cast<size_t>(threadIdx.x >> 5) * k;
+    u64 cut = 0;
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        const int v = rows[i];
+        for (int p = lane; p < k; p += 32) hist[p] = 0;
+        __syncwarp();
+        accumulate_row(nbr, ew, labels, v, off[v] + lane, off[v + 1], 32, hist);
+        __syncwarp();
+        C total = 0;
+        C* row = A + static_cast<i64>(v) * k;
+        for (int p = lane; p < k; p += 32) {
+            row[p] = hist[p];
+            total += hist[p];
+        }
+        total = warp_sum(total);
+        if (lane == 0) {
+            totals[v] = total;
+            if (directed_cut) cut += static_cast<u64>(total - hist[labels[v]]);
+        }
+        __syncwarp();
+    }
+    if (directed_cut) cut_sum.finish(cut, directed_cut);
+}
+// Sum of the row lengths of rows[0 .. *count).
+__global__ void k_row_entries(const u32* count, const int* rows, const int* off, u64* out) {
+    const i64 c = static_cast<i64>(*count);
+    u64 sum = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < c; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        sum += static_cast<u64>(off[rows[i] + 1] - off[rows[i]]);
+    block_atomic_add(out, sum);
+}
+struct IsLongRow {
+    const int* off;
+    __device__ bool operator()(i64 v) const {
+        const int d = off[v + 1] - off[v];
+        return d > kBuildShort && d <= kHeavyRow;
+    }
+};
 
 // GP_FLAG_VERIFY: the incremental cache against an independent rebuild.
 template <class C>
@@ -227,17 +284,17 @@ __global__ void k_heavy_cut(i64 count, const int* heavy, const int* labels, int 
 }
 
 template <class C>
-__global__ void k_build_chunks(DGraph g, const int* labels, int k, C* A, C* totals, const u64* gate, u64 threshold) {
+__global__ void k_build_chunks(DGraph g, const int* labels, int k, C* A, C* totals, const u64* gate, u64 threshold,
+                               u64* work, u64 work_bytes) {
     extern __shared__ unsigned char smem_build[];
     if (gate && *gate <= threshold) return;
+    if (work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(work, work_bytes);
     C* hist = reinterpret_cast<C*>(smem_build);
     const int c = blockIdx.x, v = g.chunk_row[c];
     for (int p = threadIdx.x; p < k; p += blockDim.x) hist[p] = 0;
     __syncthreads();
-    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
-        const int u = g.nbr[e];
-        if (u != v) atomicAdd(hist + labels[u], static_cast<C>(edge_w(g.ew, e)));
-    }
+    accumulate_row(g.nbr, g.ew, labels, v, g.chunk_begin[c] + static_cast<int>(threadIdx.x), chunk_end(g, c, v),
+                   static_cast<int>(blockDim.x), hist);
     __syncthreads();
     C total = 0;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
@@ -1950,6 +2007,8 @@ private:
     u64 rebuild_entries = ~0ULL;  // mover entries above which apply() rebuilds the cache
     i64 repair_iterations = 0, repair_donors = 0;  // for the per-level log line
     bool on_demand = false;  // no dense cache: affinities recomputed from the rows
+    int* long_rows = nullptr;  // rows built by k_build_long (large levels)
+    i64 long_count = 0, long_entries = 0;
     u64 max_load_host = 0;
 
     cudaStream_t s() const { return ctx.stream; }
@@ -1966,21 +2025,31 @@ private:
         const bool vec = (static_cast<size_t>(k) * sizeof(T)) % 16 == 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * (32 / W) * k * sizeof(T);
         const int grid = grid_for(n * W, kThreads);
-        // Algorithmic bytes: offsets, the light rows' neighbours (weights)
-        // and label gathers, every row of the cache and its total written,
-        // each row's own label.
-        const u64 light = static_cast<u64>(g.m - g.heavy_entries);
-        const u64 bytes = 4ULL * (n + 1) + light * (8ULL + (g.ew ? 4ULL : 0ULL)) +
-                          static_cast<u64>(n) * (static_cast<u64>(k) + 1) * sizeof(T) + 4ULL * n;
+        // Algorithmic bytes of each kernel: the CSR entries it reads (each
+        // neighbour, its weight and its label gather), the offsets, the
+        // cache rows and totals it writes and each written row's own label.
+        // k_build writes the rows of every vertex but the long ones (heavy
+        // rows as zeros, their sums added by k_build_chunks).
+        const u64 entry = 8ULL + (g.ew ? 4ULL : 0ULL), row = (static_cast<u64>(k) + 1) * sizeof(T) + 4ULL;
+        const u64 short_entries = static_cast<u64>(g.m - g.heavy_entries - long_entries);
+        const u64 bytes = 4ULL * (n + 1) + short_entries * entry + static_cast<u64>(n - long_count) * row;
+        const u64 long_bytes = static_cast<u64>(long_count) * (12ULL + row) + static_cast<u64>(long_entries) * entry;
+        const u64 chunk_bytes = 12ULL * static_cast<u64>(g.chunks) + static_cast<u64>(g.heavy_entries) * entry;
+        const bool apart = long_count > 0;
         if (vec)
             launch(k_build<T, W, true>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes, apart);
         else
             launch(k_build<T, W, false>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes, apart);
+        if (apart)
+            launch(k_build_long<T>, grid_for(long_count * 32, kThreads), kThreads, (kThreads / 32) * k * sizeof(T), s(),
+                   long_count, static_cast<const int*>(long_rows), g.off, g.nbr, g.ew, static_cast<const int*>(labels), k,
+                   A, totals, directed_cut, gate, threshold, work_counter(k_build_long<T>), long_bytes);
         if (g.chunks) {
             launch(k_build_chunks<T>, static_cast<int>(g.chunks), 256, sizeof(T) * k, s(), g,
-                   static_cast<const int*>(labels), k, A, totals, gate, threshold);
+                   static_cast<const int*>(labels), k, A, totals, gate, threshold, work_counter(k_build_chunks<T>),
+                   chunk_bytes);
             if (directed_cut)
                 launch(k_heavy_cut<T>, blocks_for(g.heavy_count, kThreads), kThreads, 0, s(), g.heavy_count,
                        static_cast<const int*>(g.heavy), static_cast<const int*>(labels), k, static_cast<const T*>(A),
@@ -2415,6 +2484,17 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     if (!on_demand) {
         A = A_.alloc<T>(static_cast<size_t>(n) * k);
         totals = A_.alloc<T>(n);
+        if (n > 65536) {  // long rows of the level and their entries, for k_build_long
+            long_rows = A_.alloc<int>(n);
+            ctx.clear_scalars(2);
+            u32* count_dev = reinterpret_cast<u32*>(ctx.dev_scalars);
+            select_if(A_, s(), n, IsLongRow{g.off}, WriteIndex{long_rows}, count_dev);
+            launch(k_row_entries, grid_for(n, kThreads), kThreads, 0, s(), static_cast<const u32*>(count_dev),
+                   static_cast<const int*>(long_rows), g.off, ctx.dev_scalars + 1);
+            const u64* sc = ctx.read_scalars(2);
+            long_count = static_cast<i64>(static_cast<u32>(sc[0] & 0xffffffffULL));
+            long_entries = static_cast<i64>(sc[1]);
+        }
     }
     targets = A_.alloc<int>(n);
     gains = A_.alloc<long long>(n);
