@@ -62,6 +62,10 @@ class _Stats(_C.Structure):
                 ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64)]
 
 
+class _Level(_C.Structure):
+    _fields_ = [("graph", _Csr), ("map", _C.c_void_p)]
+
+
 class _Request(_C.Structure):
     _fields_ = [("graph", _Csr), ("k", _C.c_int32), ("epsilon", _C.c_double), ("seed", _C.c_uint32),
                 ("flags", _C.c_uint32), ("labels_out", _C.c_void_p), ("stats", _Stats), ("status", _C.c_int),
@@ -180,6 +184,42 @@ def with_weights(graph: Graph, seed: int, vw=(1, 1), ew=(1, 1)) -> Graph:
     _check(library().gp_generate_weights(_C.byref(g), _C.c_uint64(seed), vw[0], vw[1], ew[0], ew[1],
                                          _ptr(vws), _ptr(ews)))
     return Graph(graph.offsets, graph.neighbors, vws, ews)
+
+
+def write_hierarchy(levels: list, path: str) -> None:
+    """write_hierarchy (include/hierarchy.hpp:38-123): ``levels`` is a list of
+    (Graph, map) pairs, map (int32, length n of its level) for every level but
+    the last, None for the last."""
+    arr = (_Level * max(1, len(levels)))()
+    keep = []
+    for i, (graph, mp) in enumerate(levels):
+        mp = None if mp is None else _np.ascontiguousarray(mp, dtype=_np.int32)
+        keep.append(mp)
+        arr[i] = _Level(graph.as_c(), _ptr(mp))
+    _check(library().gp_write_hierarchy(arr, _C.c_int32(len(levels)), str(path).encode()))
+
+
+def read_hierarchy(path: str) -> list[dict]:
+    """Parse a file of write_hierarchy: per level offsets, neighbors, edge and
+    vertex weights (int32) and the map of the previous level to this one."""
+    data = _np.fromfile(path, dtype=_np.int32)
+    pos = 1
+    out = []
+    for i in range(int(data[0])):
+        n, m = int(data[pos]), int(data[pos + 1])
+        pos += 2
+        level = {}
+        for name, size in (("offsets", n + 1), ("neighbors", m), ("edge_weights", m), ("vertex_weights", n)):
+            level[name] = data[pos:pos + size].copy()
+            pos += size
+        if i:
+            fine = out[-1]["offsets"].shape[0] - 1
+            level["map_from_previous"] = data[pos:pos + fine].copy()
+            pos += fine
+        out.append(level)
+    if pos != data.shape[0]:
+        raise ValueError(f"{path}: {data.shape[0] - pos} trailing int32 values")
+    return out
 
 
 def read_csr_int64(indptr_path: str, indices_path: str) -> Graph:
@@ -364,6 +404,10 @@ class Context:
                             maximum_degree=int(meta[0]), has_heavy_rows=int(meta[1]),
                             incident_weight_bound=int(meta[2])))
         return out
+
+    def write_kept_hierarchy(self, path: str) -> None:
+        """gp_write_kept_hierarchy: the hierarchy kept by FLAG_KEEP_HIERARCHY, as write_hierarchy writes it."""
+        _check(self._lib.gp_write_kept_hierarchy(self._handle, str(path).encode()))
 
     def initial_labels(self, n: int) -> _np.ndarray:
         out = _np.empty(n, _np.int32)

@@ -165,6 +165,79 @@ gp_status gp_write_csr_int64(const char* indptr_path, const char* indices_path, 
     return GP_OK;
 }
 
+// write_hierarchy (include/hierarchy.hpp:38-123): checks first, then the
+// int32 stream into a temporary that is renamed into place.
+gp_status gp_write_hierarchy(const gp_level* levels, int32_t count, const char* path) {
+    if (!path) { set_error("path is NULL"); return GP_INVALID_ARGUMENT; }
+    if (!levels || count < 1) { set_error("cannot write an incomplete hierarchy"); return GP_INVALID_ARGUMENT; }
+    constexpr int64_t kMax = std::numeric_limits<int32_t>::max();
+    for (int32_t i = 0; i < count; ++i) {
+        const gp_csr& g = levels[i].graph;
+        if (i + 1 < count && !levels[i].map) { set_error("cannot write an incomplete hierarchy"); return GP_INVALID_ARGUMENT; }
+        if (g.n < 0 || g.m < 0 || g.n > kMax || g.m > kMax) {
+            set_error("hierarchy export requires 32-bit dimensions");
+            return GP_INVALID_ARGUMENT;
+        }
+        if (!g.offsets || (g.m && !g.neighbors)) { set_error("cannot write an incomplete hierarchy"); return GP_INVALID_ARGUMENT; }
+        for (int64_t v = 0; v <= g.n; ++v)
+            if (g.offsets[v] < 0) { set_error("hierarchy row offset exceeds int32"); return GP_INVALID_ARGUMENT; }
+        if (g.edge_weights)
+            for (int64_t e = 0; e < g.m; ++e)
+                if (g.edge_weights[e] > static_cast<uint32_t>(kMax)) {
+                    set_error("hierarchy edge weight exceeds int32");
+                    return GP_INVALID_ARGUMENT;
+                }
+        if (g.vertex_weights)
+            for (int64_t v = 0; v < g.n; ++v)
+                if (g.vertex_weights[v] > static_cast<uint32_t>(kMax)) {
+                    set_error("hierarchy vertex weight exceeds int32");
+                    return GP_INVALID_ARGUMENT;
+                }
+        if (i > 0)
+            for (int64_t v = 0; v < levels[i - 1].graph.n; ++v)
+                if (levels[i - 1].map[v] < 0 || levels[i - 1].map[v] >= g.n) {
+                    set_error("hierarchy map contains an invalid coarse id");
+                    return GP_INVALID_ARGUMENT;
+                }
+    }
+    const std::string temporary = std::string(path) + ".tmp";
+    std::ofstream out(temporary, std::ios::binary | std::ios::trunc);
+    if (!out) { set_error("cannot open hierarchy temporary file"); return GP_IO_ERROR; }
+    auto put = [&](const void* data, int64_t ints) {
+        out.write(static_cast<const char*>(data), static_cast<std::streamsize>(ints * 4));
+    };
+    std::vector<int32_t> ones;
+    auto unit = [&](int64_t len) -> const int32_t* {
+        if (static_cast<int64_t>(ones.size()) < len) ones.assign(static_cast<size_t>(len), 1);
+        return ones.data();
+    };
+    put(&count, 1);
+    for (int32_t i = 0; i < count; ++i) {
+        const gp_csr& g = levels[i].graph;
+        const int32_t dims[2] = {static_cast<int32_t>(g.n), static_cast<int32_t>(g.m)};
+        put(dims, 2);
+        put(g.offsets, g.n + 1);
+        if (g.m) put(g.neighbors, g.m);
+        put(g.edge_weights ? static_cast<const void*>(g.edge_weights) : unit(g.m), g.m);
+        put(g.vertex_weights ? static_cast<const void*>(g.vertex_weights) : unit(g.n), g.n);
+        if (i > 0) put(levels[i - 1].map, levels[i - 1].graph.n);
+    }
+    out.flush();
+    const bool written = static_cast<bool>(out);
+    out.close();
+    if (!written) {
+        std::remove(temporary.c_str());
+        set_error("failed while writing hierarchy");
+        return GP_IO_ERROR;
+    }
+    if (std::rename(temporary.c_str(), path) != 0) {
+        std::remove(temporary.c_str());
+        set_error("cannot commit hierarchy output");
+        return GP_IO_ERROR;
+    }
+    return GP_OK;
+}
+
 // host_cut (src/graph.cpp:184-203).
 gp_status gp_edge_cut(const gp_csr* g, const int32_t* labels, uint64_t* cut) {
     if (auto s = validate_host_csr(g, false); s != GP_OK) return s;

@@ -468,6 +468,18 @@ gp_status gp_level_copy(gp_context* ctx, int32_t level, int32_t* offsets, int32_
     return GP_OK;
 }
 
+gp_status gp_write_kept_hierarchy(gp_context* ctx, const char* path) {
+    if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
+    const auto& kept = ctx->ctx.kept;
+    std::vector<gp_level> levels(kept.size());
+    for (size_t i = 0; i < kept.size(); ++i) {
+        const auto& L = kept[i];
+        levels[i].graph = gp_csr{L.n, L.m, L.off.data(), L.nbr.data(), L.vw.data(), L.ew.data()};
+        levels[i].map = L.map.empty() ? nullptr : L.map.data();
+    }
+    return gp_write_hierarchy(levels.data(), static_cast<int32_t>(levels.size()), path);
+}
+
 gp_status gp_initial_labels(gp_context* ctx, int32_t* labels, int64_t capacity) {
     if (!ctx || !labels) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
     const auto& v = ctx->ctx.initial_labels;

@@ -236,6 +236,27 @@ gp_status gp_read_csr_int64(const char* indptr_path, const char* indices_path,
 gp_status gp_write_csr_int64(const char* indptr_path, const char* indices_path,
                              const gp_csr* graph);
 
+/* One level of a hierarchy for gp_write_hierarchy: its CSR (NULL weights
+ * are unit weights) and, for every level but the last, `map`: the level's
+ * vertices (length graph.n) to the next level's. */
+typedef struct gp_level {
+    gp_csr graph;
+    const int32_t* map;
+} gp_level;
+
+/* write_hierarchy (include/hierarchy.hpp:38-123): the Jet-compatible int32
+ * file of a hierarchy.  Layout, all int32: the level count, then per level
+ * i: n, m, offsets[n+1], neighbors[m], edge weights[m], vertex weights[n]
+ * and, for i > 0, the map of level i-1 (n_{i-1} entries, each < n_i).  The
+ * file is written to path + ".tmp" and renamed into place; on any error the
+ * temporary is removed and the reference's message is set
+ * (GP_INVALID_ARGUMENT for a value outside int32 or an invalid map entry,
+ * GP_IO_ERROR for the file). */
+gp_status gp_write_hierarchy(const gp_level* levels, int32_t count, const char* path);
+/* The hierarchy kept by the last GP_FLAG_KEEP_HIERARCHY call of `ctx`,
+ * written as gp_write_hierarchy does. */
+gp_status gp_write_kept_hierarchy(gp_context* ctx, const char* path);
+
 /* Exact undirected cut of `labels` (directed sum / 2; odd sum is an error). */
 gp_status gp_edge_cut(const gp_csr* graph, const int32_t* labels, uint64_t* cut);
 

@@ -183,3 +183,21 @@ def test_verify_flag_rejects_unequal_reverse_weights(gp, ctx):
     with pytest.raises(gp.GpartError) as e:
         ctx.partition(bad, 4, 1.03, 0, gp.FLAG_QUIET | gp.FLAG_VERIFY)
     assert e.value.status == 1 and "reverse edge weights differ" in str(e.value)
+
+
+def test_kept_hierarchy_written_like_write_hierarchy(gp, ctx, tmp_path):
+    """gp_write_kept_hierarchy writes the levels and maps of the last call
+    kept with FLAG_KEEP_HIERARCHY in write_hierarchy's int32 layout."""
+    g = gp.with_weights(gp.rmat(14, 8, 0.57, 0.19, 0.19, 2), 3, (1, 4), (1, 9))
+    ctx.partition(g, 16, 1.03, 0, gp.FLAG_QUIET | gp.FLAG_KEEP_HIERARCHY)
+    kept = ctx.levels()
+    assert len(kept) > 2
+    path = tmp_path / "hierarchy.bin"
+    ctx.write_kept_hierarchy(path)
+    written = gp.read_hierarchy(path)
+    assert len(written) == len(kept)
+    for i, (w, k) in enumerate(zip(written, kept)):
+        for name in ("offsets", "neighbors", "edge_weights", "vertex_weights"):
+            np.testing.assert_array_equal(w[name], k[name].astype(np.int32), err_msg=f"level {i} {name}")
+        if i:
+            np.testing.assert_array_equal(w["map_from_previous"], kept[i - 1]["map"])

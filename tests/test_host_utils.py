@@ -120,3 +120,49 @@ def test_partition_cli_usage_errors():
     env = dict(os.environ, GPART_REFINE_MODE="x")
     r = subprocess.run([exe, "a", "b", "4", "c"], capture_output=True, text=True, env=env)
     assert r.returncode == 1 and r.stderr.startswith("gpart_partition:")
+
+
+def test_write_hierarchy_layout(gp, tmp_path):
+    """write_hierarchy's int32 layout (include/hierarchy.hpp:38-123): level
+    count, then n, m, offsets, neighbors, edge weights, vertex weights and the
+    previous level's map; unit weights are written as ones."""
+    fine = gp.grid2d(4, 4)
+    mp = (np.arange(16) // 2).astype(np.int32)  # pairs along rows
+    coarse = gp.Graph(np.arange(9, dtype=np.int32), np.array([1, 0, 3, 2, 5, 4, 7, 6], np.int32),
+                      vertex_weights=np.full(8, 2, np.uint32), edge_weights=np.arange(1, 9, dtype=np.uint32))
+    path = tmp_path / "h.bin"
+    gp.write_hierarchy([(fine, mp), (coarse, None)], path)
+    assert not (tmp_path / "h.bin.tmp").exists()
+    raw = np.fromfile(path, np.int32)
+    expected = np.concatenate([[2, fine.n, fine.m], fine.offsets, fine.neighbors, np.ones(fine.m), np.ones(fine.n),
+                               [coarse.n, coarse.m], coarse.offsets, coarse.neighbors, coarse.edge_weights,
+                               coarse.vertex_weights, mp]).astype(np.int32)
+    np.testing.assert_array_equal(raw, expected)
+    levels = gp.read_hierarchy(path)
+    assert len(levels) == 2
+    np.testing.assert_array_equal(levels[1]["map_from_previous"], mp)
+    np.testing.assert_array_equal(levels[1]["edge_weights"], coarse.edge_weights)
+
+
+@pytest.mark.parametrize("defect, message", [
+    ("map", "hierarchy map contains an invalid coarse id"),
+    ("edge_weight", "hierarchy edge weight exceeds int32"),
+    ("vertex_weight", "hierarchy vertex weight exceeds int32"),
+    ("missing_map", "cannot write an incomplete hierarchy"),
+])
+def test_write_hierarchy_rejects_like_the_reference(gp, tmp_path, defect, message):
+    fine = gp.grid2d(3, 3)
+    mp = np.zeros(9, np.int32)
+    coarse = gp.Graph(np.zeros(2, np.int32), np.zeros(0, np.int32))
+    if defect == "map":
+        mp[4] = 1  # the coarse level has one vertex
+    if defect == "edge_weight":
+        fine = gp.Graph(fine.offsets, fine.neighbors, edge_weights=np.full(fine.m, 1 << 31, np.uint32))
+    if defect == "vertex_weight":
+        fine = gp.Graph(fine.offsets, fine.neighbors, vertex_weights=np.full(fine.n, 1 << 31, np.uint32))
+    levels = [(fine, None if defect == "missing_map" else mp), (coarse, None)]
+    path = tmp_path / "h.bin"
+    with pytest.raises(gp.GpartError) as e:
+        gp.write_hierarchy(levels, path)
+    assert message in str(e.value)
+    assert not path.exists() and not (tmp_path / "h.bin.tmp").exists()
