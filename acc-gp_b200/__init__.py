@@ -321,6 +321,22 @@ class Context:
                                       _C.c_uint32(seed), _C.c_uint32(flags), _ptr(labels), _C.byref(stats)))
         return labels, Stats._from(stats)
 
+    def load_csr_int64(self, indptr_path: str, indices_path: str) -> tuple[int, int]:
+        """gp_load_csr_int64: the reference's int64 files streamed into device memory; returns (n, m)."""
+        n, m = _C.c_int64(), _C.c_int64()
+        _check(self._lib.gp_load_csr_int64(self._handle, str(indptr_path).encode(), str(indices_path).encode(),
+                                           _C.byref(n), _C.byref(m)))
+        self._loaded_n = n.value
+        return n.value, m.value
+
+    def partition_loaded(self, k: int, epsilon: float = 1.03, seed: int = 0, flags: int = FLAG_QUIET):
+        """gp_partition_loaded: partition the graph of the last load_csr_int64; returns (labels, Stats)."""
+        labels = _np.empty(getattr(self, "_loaded_n", 0), _np.int32)
+        stats = _Stats()
+        _check(self._lib.gp_partition_loaded(self._handle, _C.c_int32(k), _C.c_double(epsilon), _C.c_uint32(seed),
+                                             _C.c_uint32(flags), _ptr(labels), _C.byref(stats)))
+        return labels, Stats._from(stats)
+
     def partition_device(self, offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
                          edge_weights_ptr, k: int, epsilon: float, seed: int, labels_ptr: int,
                          stream_ptr=None, flags: int = FLAG_QUIET) -> Stats:

@@ -22,6 +22,14 @@ struct gp_context {
     bool seed_matching = true, fast_path = true;
     int cluster_size_factor = 0, fine_factor = 64, growth = 8, heavy_limit = 64;
     gp::WorkerPool* pool = nullptr;  // batch workers, created on first use
+    // gp_load_csr_int64: the loaded graph's device arrays (their own arena,
+    // kept across partitions), the pinned staging buffers and their events.
+    gp::Arena input;
+    gp::DGraph loaded;
+    int* loaded_labels = nullptr;
+    bool has_loaded = false;
+    long long* pinned[2] = {nullptr, nullptr};
+    cudaEvent_t staged[2] = {nullptr, nullptr};
 };
 
 namespace gp {
@@ -79,6 +87,29 @@ void KernelProfiler::after(cudaStream_t s) {
 }
 
 namespace {
+
+// load_weighted_graph's narrowing (src/graph.cpp:70-107) of one chunk of
+// the int64 files, values copied to int32 at out[0..count).  The first
+// failing position (first_index + i) of each check is kept with atomicMin:
+// bad[0] an offset negative or below its predecessor (`previous` is the value
+// before the chunk), bad[1] an offset above int32, bad[2] a neighbor outside
+// [0, n).
+__global__ void k_narrow(i64 count, const long long* in, int* out, bool neighbors, long long n, long long previous,
+                         u64 first_index, u64* bad) {
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const long long x = in[i];
+        const u64 at = first_index + static_cast<u64>(i);
+        if (neighbors) {
+            if (x < 0 || x >= n) atomicMin(bad + 2, at);
+        } else {
+            const long long before = i ? in[i - 1] : previous;
+            if (x < 0 || x < before) atomicMin(bad, at);
+            else if (x > 0x7fffffffLL) atomicMin(bad + 1, at);
+        }
+        out[i] = static_cast<int>(x);
+    }
+}
 
 __global__ void k_fill_ones(i64 n, u32* p) {
     for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<i64>(gridDim.x) * blockDim.x)
@@ -362,6 +393,11 @@ void gp_context_destroy(gp_context* h) {
     destroy_worker_pool(h->pool);
     h->pool = nullptr;
     Context& c = h->ctx;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    h->input.reset_device();
+    for (auto& p : h->pinned) if (p) cudaFreeHost(p);
+    for (auto& e : h->staged) if (e) cudaEventDestroy(e);
     if (h->profiler.device_bytes) {
         cudaSetDevice(c.device);
         cudaFree(h->profiler.device_bytes);
@@ -387,6 +423,105 @@ gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k, d
                               uint32_t flags, int32_t* labels_out_device, void* stream, gp_stats* stats) {
     if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
     return guarded([&] { return run(ctx, graph, true, k, epsilon, seed, flags, labels_out_device, stream, stats); });
+}
+
+// load_weighted_graph + make_device_weighted (src/graph.cpp:47-116,205-218)
+// in one pass: each file is read in chunks of kLoadChunk int64 values into
+// one of two pinned buffers while the other chunk is copied to the device and
+// narrowed there, so the disk read, the copy and the narrowing overlap.
+constexpr int64_t kLoadChunk = int64_t{1} << 23;  // 64 MB of int64 per buffer
+gp_status gp_load_csr_int64(gp_context* ctx, const char* indptr_path, const char* indices_path, int64_t* n_out,
+                            int64_t* m_out) {
+    if (!ctx || !indptr_path || !indices_path) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    int64_t n = 0, m = 0;
+    if (gp_status st = gp_read_csr_int64(indptr_path, indices_path, &n, &m, nullptr, nullptr); st != GP_OK) return st;
+    return guarded([&]() -> gp_status {
+        ctx->has_loaded = false;
+        FILE* a = std::fopen(indptr_path, "rb");
+        if (!a) fail(GP_IO_ERROR, std::string("cannot open ") + indptr_path);
+        long long ends[2] = {0, 0};
+        const bool ends_ok = std::fread(&ends[0], 8, 1, a) == 1 && std::fseek(a, -8, SEEK_END) == 0 &&
+                             std::fread(&ends[1], 8, 1, a) == 1 && std::fseek(a, 0, SEEK_SET) == 0;
+        if (!ends_ok) { std::fclose(a); fail(GP_IO_ERROR, std::string("cannot read ") + indptr_path); }
+        if (ends[0] != 0 || ends[1] != m) { std::fclose(a); fail(GP_INVALID_ARGUMENT, "CSR offsets do not match indices"); }
+        FILE* b = std::fopen(indices_path, "rb");
+        if (!b) { std::fclose(a); fail(GP_IO_ERROR, std::string("cannot open ") + indices_path); }
+        struct Files { FILE* a; FILE* b; ~Files() { std::fclose(a); std::fclose(b); } } files{a, b};
+        Context& c = ctx->ctx;
+        GP_CUDA(cudaSetDevice(c.device));
+        cudaStream_t s = c.stream;
+        for (int i = 0; i < 2; ++i) {
+            if (!ctx->pinned[i]) GP_CUDA(cudaMallocHost(&ctx->pinned[i], sizeof(long long) * kLoadChunk));
+            if (!ctx->staged[i]) GP_CUDA(cudaEventCreateWithFlags(&ctx->staged[i], cudaEventDisableTiming));
+        }
+        GP_CUDA(cudaStreamSynchronize(s));
+        ctx->input.release({0, 0});
+        DGraph g;
+        g.n = n;
+        g.m = m;
+        g.off = ctx->input.alloc<int>(n + 1);
+        g.nbr = ctx->input.alloc<int>(m);
+        int* labels = ctx->input.alloc<int>(n);
+        long long* staging[2] = {ctx->input.alloc<long long>(kLoadChunk), ctx->input.alloc<long long>(kLoadChunk)};
+        GP_CUDA(cudaMemsetAsync(c.dev_scalars, 0xff, 3 * sizeof(u64), s));
+        int chunk = 0;
+        auto stream_file = [&](FILE* f, const char* path, int64_t count, int* out, bool neighbors) {
+            long long previous = 0;
+            for (int64_t done = 0; done < count; ++chunk) {
+                const int buf = chunk & 1;
+                const int64_t take = std::min(kLoadChunk, count - done);
+                // The buffer's previous copy must have left it before it is refilled.
+                if (chunk >= 2) GP_CUDA(cudaEventSynchronize(ctx->staged[buf]));
+                if (std::fread(ctx->pinned[buf], 8, static_cast<size_t>(take), f) != static_cast<size_t>(take))
+                    fail(GP_IO_ERROR, std::string("cannot read ") + path);
+                GP_CUDA(cudaMemcpyAsync(staging[buf], ctx->pinned[buf], sizeof(long long) * take, cudaMemcpyHostToDevice, s));
+                GP_CUDA(cudaEventRecord(ctx->staged[buf], s));
+                launch(k_narrow, std::min(blocks_for(take, 256), 148 * 8), 256, 0, s, take,
+                       static_cast<const long long*>(staging[buf]), out + done, neighbors, static_cast<long long>(n),
+                       previous, static_cast<u64>(done), c.dev_scalars);
+                previous = ctx->pinned[buf][take - 1];
+                done += take;
+            }
+        };
+        stream_file(a, indptr_path, n + 1, g.off, false);
+        stream_file(b, indices_path, m, g.nbr, true);
+        // The reference stops at the first failing offset, then at the first
+        // failing neighbor.
+        const u64* bad = c.read_scalars(3);
+        if (bad[0] != ~0ULL && bad[0] <= bad[1]) fail(GP_INVALID_ARGUMENT, "CSR offsets are not monotone");
+        if (bad[1] != ~0ULL) fail(GP_INVALID_ARGUMENT, "graph exceeds supported 32-bit CSR limits; dataset excluded");
+        if (bad[2] != ~0ULL) fail(GP_INVALID_ARGUMENT, "CSR contains an invalid neighbor");
+        ctx->loaded = g;
+        ctx->loaded_labels = labels;
+        ctx->has_loaded = true;
+        if (n_out) *n_out = n;
+        if (m_out) *m_out = m;
+        return GP_OK;
+    });
+}
+
+gp_status gp_partition_loaded(gp_context* ctx, int32_t k, double epsilon, uint32_t seed, uint32_t flags,
+                              int32_t* labels_out, gp_stats* stats) {
+    if (!ctx || !labels_out) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    if (!ctx->has_loaded) { set_error("no graph loaded; call gp_load_csr_int64 first"); return GP_INVALID_ARGUMENT; }
+    return guarded([&]() -> gp_status {
+        Context& c = ctx->ctx;
+        const DGraph& g = ctx->loaded;
+        GP_CUDA(cudaSetDevice(c.device));
+        int* labels_dev = ctx->loaded_labels;
+        const gp_csr dg{g.n, g.m, g.off, g.nbr, nullptr, nullptr};
+        gp_stats local{};
+        gp_stats* st = stats ? stats : &local;
+        const gp_status status = run(ctx, &dg, true, k, epsilon, seed, flags, labels_dev, nullptr, st);
+        if (status == GP_OK && !(flags & GP_FLAG_COARSEN_ONLY)) {
+            GP_CUDA(cudaEventRecord(c.ev[5], c.stream));
+            GP_CUDA(cudaMemcpyAsync(labels_out, labels_dev, sizeof(int) * g.n, cudaMemcpyDeviceToHost, c.stream));
+            GP_CUDA(cudaEventRecord(c.ev[6], c.stream));
+            GP_CUDA(cudaStreamSynchronize(c.stream));
+            st->d2h_seconds = elapsed(c.ev[5], c.ev[6]) * 1e-3;
+        }
+        return status;
+    });
 }
 
 gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {

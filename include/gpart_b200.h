@@ -207,6 +207,22 @@ gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring);
 gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms,
                          double* algorithmic_bytes);
 
+/* load_weighted_graph + make_device_weighted (src/graph.cpp:47-116,
+ * 205-218): the reference's int64 indptr/indices files read straight into
+ * device memory owned by the context.  Each file is read in chunks of 8 Mi
+ * values into two pinned buffers, so that the read of one chunk overlaps the
+ * copy and the device-side narrowing to int32 of the previous one.  The
+ * checks and messages are load_weighted_graph's.  The graph (unit weights)
+ * stays on the device until the next load or gp_context_destroy; n and m
+ * are returned. */
+gp_status gp_load_csr_int64(gp_context* ctx, const char* indptr_path,
+                            const char* indices_path, int64_t* n, int64_t* m);
+/* gp_partition of the graph of the last gp_load_csr_int64 (the upload is
+ * already done); labels_out is host memory of n entries. */
+gp_status gp_partition_loaded(gp_context* ctx, int32_t k, double epsilon,
+                              uint32_t seed, uint32_t flags, int32_t* labels_out,
+                              gp_stats* stats);
+
 /* Hierarchy of the last call made with GP_FLAG_KEEP_HIERARCHY.  Level 0 is
  * the input.  gp_level_copy fills any non-NULL array; `map` (length n of the
  * level) maps this level's vertices to the next level and is absent for the
