@@ -66,6 +66,12 @@ class _Level(_C.Structure):
     _fields_ = [("graph", _Csr), ("map", _C.c_void_p)]
 
 
+class _Tuning(_C.Structure):
+    _fields_ = [("medium_degree", _C.c_int32), ("large_narrow", _C.c_int32), ("build_short", _C.c_int32),
+                ("rebuild_divisor", _C.c_int32), ("on_demand_degree", _C.c_int32), ("default_ms", _C.c_double),
+                ("tuned_ms", _C.c_double), ("trials", _C.c_int32)]
+
+
 class _Request(_C.Structure):
     _fields_ = [("graph", _Csr), ("k", _C.c_int32), ("epsilon", _C.c_double), ("seed", _C.c_uint32),
                 ("flags", _C.c_uint32), ("labels_out", _C.c_void_p), ("stats", _Stats), ("status", _C.c_int),
@@ -395,6 +401,15 @@ class Context:
         launches, ms, nbytes = _C.c_uint64(), _C.c_double(), _C.c_double()
         _check(self._lib.gp_profile_end(self._handle, _C.byref(launches), _C.byref(ms), _C.byref(nbytes)))
         return launches.value, ms.value, nbytes.value
+
+    def autotune(self, graph: Graph, k: int, epsilon: float = 1.03, seed: int = 0, repeats: int = 2) -> dict:
+        """gp_autotune: choose the thread-mapping thresholds for this workload
+        (kept on the context); returns them with the default and tuned times."""
+        t = _Tuning()
+        g = graph.as_c()
+        _check(self._lib.gp_autotune(self._handle, _C.byref(g), _C.c_int32(k), _C.c_double(epsilon),
+                                     _C.c_uint32(seed), _C.c_int32(repeats), _C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _Tuning._fields_}
 
     def set_option(self, name: str, value: int) -> None:
         _check(self._lib.gp_set_option(self._handle, name.encode(), _C.c_int64(value)))

@@ -25,7 +25,6 @@ namespace {
 constexpr int kLowDegree = 8;       // SCLP_LOW_DEGREE
 constexpr int kMediumDegree = 256;  // SCLP_MEDIUM_DEGREE
 constexpr int kLargeDegree = kHeavyRow;   // rows above use a chunked global table
-constexpr int kLargeNarrow = 1024;  // large rows up to this take a half-size shared table
 constexpr int kMediumHash = 512;          // SCLP_MEDIUM_HASH_SIZE
 constexpr int kLargeHash = 2 * kHeavyRow; // shared-memory table of the large class
 constexpr int kSegment = 4096;            // table slots summarised per block
@@ -122,13 +121,15 @@ __global__ void k_weight_sum(i64 m, const u32* ew, u64* out) {
 }
 
 // Degree classes (sclp_compact_degree_classes, aggregation.cuh:5-71): exact
-// max degree, heavy flag and class lists.  The reference's large class is
-// split at kLargeNarrow so that its shorter rows run with half the shared
+// max degree, heavy flag and class lists, the medium class ending at
+// medium_degree (at most kMediumDegree).  The reference's large class is
+// split at large_narrow so that its shorter rows run with a smaller shared
 // table.  Scalars: 0 max degree, 1 heavy, 2..5 list sizes (low, medium,
-// large up to kLargeNarrow, heavy), 6 heavy hash slots, 7 isolated vertices,
-// 8 list size of the large rows above kLargeNarrow.
+// large up to large_narrow, heavy), 6 heavy hash slots, 7 isolated vertices,
+// 8 list size of the large rows above large_narrow.
 __global__ void __launch_bounds__(256) k_degree_classes(i64 n, const int* off, int* low, int* medium, int* large,
-                                                        int* heavy, int* large_wide, u64* sc) {
+                                                        int* heavy, int* large_wide, int medium_degree,
+                                                        int large_narrow, u64* sc) {
     u64 d_max = 0, isolated = 0;
     int big = 0;
     // Block-uniform passes: the appends synchronise the block.
@@ -141,8 +142,8 @@ __global__ void __launch_bounds__(256) k_degree_classes(i64 n, const int* off, i
         isolated += valid && deg == 0;
         const int cls = !valid                ? -1
                         : deg <= kLowDegree    ? 0
-                        : deg <= kMediumDegree ? 1
-                        : deg <= kLargeNarrow  ? 2
+                        : deg <= medium_degree ? 1
+                        : deg <= large_narrow  ? 2
                         : deg <= kLargeDegree  ? 4
                                                : 3;
         block_append(static_cast<int>(v), cls == 0, low, sc + 2);
@@ -1401,10 +1402,13 @@ private:
             const int blocks = static_cast<int>(std::min<i64>(blocks_for(list_size[1], kMediumWarps), 148 * 64));
             launch(k_affinity_medium<Table>, blocks, kMediumWarps * 32, 0, ctx.stream, list_size[1], lists[1], p);
         }
-        // Shared tables of 2048 slots for rows up to kLargeNarrow, 4096 above.
+        // Shared tables of at least twice the longest row of the class.
         for (int c : {2, 4}) {
             if (!list_size[c]) continue;
-            const size_t smem = static_cast<size_t>(c == 2 ? 2 * kLargeNarrow : 2 * kLargeDegree) * Table::kSlotBytes;
+            size_t slots = 32;
+            while (slots < 2 * static_cast<size_t>(c == 2 ? std::min(o.mapping.large_narrow, kLargeDegree) : kLargeDegree))
+                slots <<= 1;
+            const size_t smem = slots * Table::kSlotBytes;
             GP_CUDA(cudaFuncSetAttribute(k_affinity_large<Table>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem)));
             launch(k_affinity_large<Table>, static_cast<int>(list_size[c]), 256, smem, ctx.stream, list_size[c], lists[c], p);
@@ -1488,7 +1492,8 @@ AggregateOut Aggregator::run() {
             for (int c = 0; c < 5; ++c) lists[c] = storage + static_cast<size_t>(n) * c;
             ctx.clear_scalars(9);
             launch(k_degree_classes, static_cast<int>(std::min<i64>(vb, 148 * 8)), kThreads, 0, s, n, g.off, lists[0],
-                   lists[1], lists[2], lists[3], lists[4], ctx.dev_scalars);
+                   lists[1], lists[2], lists[3], lists[4], std::min(o.mapping.medium_degree, kMediumDegree),
+                   std::min(o.mapping.large_narrow, kLargeDegree), ctx.dev_scalars);
             const u64* sc = ctx.read_scalars(9);
             out.stats_max_degree = sc[0];
             out.stats_heavy = sc[1] != 0;

@@ -50,6 +50,18 @@ struct Hierarchy {
     std::vector<int*> maps;      // maps[i]: level i -> level i+1
 };
 
+// Thread-mapping thresholds.  They decide which kernel and how many threads
+// handle a row, never a value: every choice computes the same exact integer
+// sums, so results do not depend on them and gp_autotune may set them per
+// workload.  The defaults are the fixed values this library was tuned with.
+struct Mapping {
+    int medium_degree = 256;    // coarsening: rows of 9..this, a warp and a 512-slot shared hash (<= 256)
+    int large_narrow = 1024;    // coarsening: large rows up to this use a half-size shared table
+    int build_short = 64;       // refinement: cache-build rows up to this, 8 lanes per row
+    int rebuild_divisor = 100;  // refinement: rebuild the cache when moved entries exceed (n k size + 8 m) / this
+    int on_demand_degree = 32;  // refinement: no cache when the maximum degree is at most this (0: never)
+};
+
 // Coarsening options, app/partition_main.cu:52-87 with no environment overrides.
 struct CoarsenOptions {
     int parts = 4;
@@ -64,6 +76,7 @@ struct CoarsenOptions {
     int heavy_limit = 64;
     bool log = true;
     bool verify = false;  // GP_FLAG_VERIFY: strict per-level checks
+    Mapping mapping;
 };
 
 // Device-resident scalars read back in batches through pinned memory.
@@ -111,7 +124,7 @@ struct RefineOutcome {
 // Refines from the coarsest level down to level 0 (refine_hierarchy_impl,
 // src/refine.cu:483-730); `labels` (device, level-0 sized) receives the result.
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
-                        int* labels, bool log, bool verify);
+                        int* labels, bool log, bool verify, const Mapping& mapping);
 
 // Device edge cut of labels (directed sum / 2); throws on an odd sum.
 u64 device_cut(Context& ctx, const DGraph& g, const int* labels);

@@ -21,6 +21,7 @@ struct gp_context {
     gp::CoarsenOptions defaults;  // overridable per context, see gp_set_option
     bool seed_matching = true, fast_path = true;
     int cluster_size_factor = 0, fine_factor = 64, growth = 8, heavy_limit = 64;
+    gp::Mapping mapping;  // thread-mapping thresholds (gp_set_option, gp_autotune)
     gp::WorkerPool* pool = nullptr;  // batch workers, created on first use
     // gp_load_csr_int64: the loaded graph's device arrays (their own arena,
     // kept across partitions), the pinned staging buffers and their events.
@@ -49,6 +50,7 @@ void copy_options(const gp_context* from, gp_context* to) {
     to->cluster_size_factor = from->cluster_size_factor;
     to->fine_factor = from->fine_factor;
     to->growth = from->growth;
+    to->mapping = from->mapping;
     to->heavy_limit = from->heavy_limit;
 }
 
@@ -279,6 +281,7 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     o.fast_path = handle->fast_path;
     o.log = !(flags & GP_FLAG_QUIET);
     o.verify = (flags & GP_FLAG_VERIFY) != 0;
+    o.mapping = handle->mapping;
     // --verify: the input must be bidirectional with equal reverse weights
     // (validate_weighted_csr, src/graph.cpp:157-182).
     if (o.verify) verify_csr(ctx, g, true, GP_INVALID_ARGUMENT);
@@ -305,7 +308,7 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     ctx.initial_labels = coarse_labels;
     GP_CUDA(cudaEventRecord(ctx.ev[3], s));
     int* labels_dev = device_input ? labels_out : ctx.persist.alloc<int>(n);
-    RefineOutcome r = uncoarsen(ctx, h, coarse_labels, k, eps, labels_dev, o.log, o.verify);
+    RefineOutcome r = uncoarsen(ctx, h, coarse_labels, k, eps, labels_dev, o.log, o.verify, o.mapping);
     GP_CUDA(cudaEventRecord(ctx.ev[4], s));
     if (directed & 1ULL) fail(GP_INTERNAL, "symmetric graph has odd directed edge weight");
     if (!device_input)
@@ -524,6 +527,91 @@ gp_status gp_partition_loaded(gp_context* ctx, int32_t k, double epsilon, uint32
     });
 }
 
+// Coordinate search over the mapping thresholds, each candidate timed by the
+// best of `repeats` partitions of the same device-resident graph.
+gp_status gp_autotune(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon, uint32_t seed, int32_t repeats,
+                      gp_tuning* out) {
+    if (!ctx || !graph || !out || repeats < 1) { set_error("NULL argument or repeats < 1"); return GP_INVALID_ARGUMENT; }
+    if (graph->n <= 0 || graph->n > std::numeric_limits<int>::max() || graph->m < 0 ||
+        graph->m > std::numeric_limits<int>::max() || !graph->offsets || (graph->m && !graph->neighbors)) {
+        set_error("invalid graph");
+        return GP_INVALID_ARGUMENT;
+    }
+    struct Buffers {
+        void* p[5] = {};
+        ~Buffers() { for (void* q : p) if (q) cudaFree(q); }
+    } buf;
+    return guarded([&]() -> gp_status {
+        Context& c = ctx->ctx;
+        GP_CUDA(cudaSetDevice(c.device));
+        const i64 n = graph->n, m = graph->m;
+        GP_CUDA(cudaMalloc(&buf.p[0], sizeof(int) * (n + 1)));
+        GP_CUDA(cudaMalloc(&buf.p[1], sizeof(int) * std::max<i64>(m, 1)));
+        GP_CUDA(cudaMalloc(&buf.p[4], sizeof(int) * n));
+        GP_CUDA(cudaMemcpy(buf.p[0], graph->offsets, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        if (m) GP_CUDA(cudaMemcpy(buf.p[1], graph->neighbors, sizeof(int) * m, cudaMemcpyHostToDevice));
+        if (graph->vertex_weights) {
+            GP_CUDA(cudaMalloc(&buf.p[2], sizeof(u32) * n));
+            GP_CUDA(cudaMemcpy(buf.p[2], graph->vertex_weights, sizeof(u32) * n, cudaMemcpyHostToDevice));
+        }
+        if (graph->edge_weights && m) {
+            GP_CUDA(cudaMalloc(&buf.p[3], sizeof(u32) * m));
+            GP_CUDA(cudaMemcpy(buf.p[3], graph->edge_weights, sizeof(u32) * m, cudaMemcpyHostToDevice));
+        }
+        const gp_csr dg{n, m, static_cast<int*>(buf.p[0]), static_cast<int*>(buf.p[1]), static_cast<u32*>(buf.p[2]),
+                        static_cast<u32*>(buf.p[3])};
+        int* labels_dev = static_cast<int*>(buf.p[4]);
+        std::vector<int> reference(static_cast<size_t>(n)), labels(static_cast<size_t>(n));
+        int trials = 0;
+        // Best algorithm time of `repeats` partitions; the labels must not change.
+        auto time_setting = [&](bool first) {
+            double best = std::numeric_limits<double>::infinity();
+            for (int r = 0; r < repeats + (first ? 1 : 0); ++r) {  // the very first partition only warms up
+                gp_stats st{};
+                if (gp_status s = run(ctx, &dg, true, k, epsilon, seed, GP_FLAG_QUIET, labels_dev, nullptr, &st); s != GP_OK)
+                    fail(s, last_error());
+                GP_CUDA(cudaMemcpy(labels.data(), labels_dev, sizeof(int) * n, cudaMemcpyDeviceToHost));
+                if (first && r == 0) { reference = labels; continue; }
+                if (labels != reference) fail(GP_INTERNAL, "mapping thresholds changed the partition");
+                best = std::min(best, st.algorithm_seconds * 1e3);
+                ++trials;
+            }
+            return best;
+        };
+        struct Restore {  // a failed search leaves the thresholds it started from
+            gp_context* ctx;
+            Mapping start;
+            bool done = false;
+            ~Restore() { if (!done) ctx->mapping = start; }
+        } restore{ctx, ctx->mapping};
+        const double default_ms = time_setting(true);
+        double best_ms = default_ms;
+        struct Knob { int Mapping::*field; std::vector<int> values; };
+        const Knob knobs[] = {
+            {&Mapping::medium_degree, {64, 128, 256}},
+            {&Mapping::large_narrow, {512, 1024, 2048}},
+            {&Mapping::build_short, {32, 64, 128}},
+            {&Mapping::rebuild_divisor, {25, 50, 100, 200, 400}},
+            {&Mapping::on_demand_degree, {0, 32}},
+        };
+        for (const Knob& knob : knobs) {
+            const int kept = ctx->mapping.*knob.field;
+            int chosen = kept;
+            for (int value : knob.values) {
+                if (value == kept) continue;
+                ctx->mapping.*knob.field = value;
+                const double ms = time_setting(false);
+                if (ms < 0.99 * best_ms) { best_ms = ms; chosen = value; }
+            }
+            ctx->mapping.*knob.field = chosen;
+        }
+        restore.done = true;
+        *out = gp_tuning{ctx->mapping.medium_degree, ctx->mapping.large_narrow, ctx->mapping.build_short,
+                         ctx->mapping.rebuild_divisor, ctx->mapping.on_demand_degree, default_ms, best_ms, trials};
+        return GP_OK;
+    });
+}
+
 gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
     if (!ctx || !name) { set_error("context/name is NULL"); return GP_INVALID_ARGUMENT; }
     const std::string key(name);
@@ -533,6 +621,11 @@ gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
     else if (key == "progressive_fine_factor" && value >= 2 && value <= (1 << 20)) ctx->fine_factor = static_cast<int>(value);
     else if (key == "progressive_capacity_growth" && value >= 2 && value <= 16) ctx->growth = static_cast<int>(value);
     else if (key == "heavy_edge_degree_limit" && value >= 2 && value <= 256) ctx->heavy_limit = static_cast<int>(value);
+    else if (key == "medium_degree" && value >= 8 && value <= 256) ctx->mapping.medium_degree = static_cast<int>(value);
+    else if (key == "large_narrow" && value >= 256 && value <= 2048) ctx->mapping.large_narrow = static_cast<int>(value);
+    else if (key == "build_short" && value >= 8 && value <= 2048) ctx->mapping.build_short = static_cast<int>(value);
+    else if (key == "rebuild_divisor" && value >= 1 && value <= 100000) ctx->mapping.rebuild_divisor = static_cast<int>(value);
+    else if (key == "on_demand_degree" && value >= 0 && value <= 32) ctx->mapping.on_demand_degree = static_cast<int>(value);
     else { set_error("unknown option or value out of range: " + key); return GP_INVALID_ARGUMENT; }
     return GP_OK;
 }

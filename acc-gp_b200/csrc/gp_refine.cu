@@ -130,16 +130,15 @@ __device__ __forceinline__ void accumulate_row(const int* nbr, const u32* ew, co
 
 // incremental_build_affinity (incremental.cuh:61-140), dense layout.  A warp
 // builds 32/W rows at a time, W lanes per row, each row's k-wide histogram in
-// shared memory; rows longer than kBuildShort entries are accumulated by the
+// shared memory; rows longer than short_max entries are accumulated by the
 // whole warp afterwards.  Heavy rows are written as zeros (k_build_chunks
 // adds their sums).  Optionally sums the directed cut of the light rows,
 // total - own-part affinity per row.
-constexpr int kBuildShort = 64;
 template <class C, int W, bool Vectorized>
 __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const int* nbr, const u32* ew,
                                                     const int* labels, int k, C* A, C* totals, u64* directed_cut,
                                                     const u64* gate, u64 threshold, u64* work, u64 work_bytes,
-                                                    bool long_rows_apart) {
+                                                    int short_max, bool long_rows_apart) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ WarpSum cut_sum;
     if (gate && *gate <= threshold) return;  // incremental update chosen
@@ -165,12 +164,12 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
             for (int p = sub; p < k; p += W) hist[p] = 0;
         }
         __syncwarp();
-        if (deg <= kBuildShort) {
+        if (deg <= short_max) {
             accumulate_row(nbr, ew, labels, static_cast<int>(v), begin + sub, end, W, hist);
         }
-        // Rows of kBuildShort..kHeavyRow entries go to k_build_long when it runs.
-        const bool mine = valid && !(long_rows_apart && deg > kBuildShort && deg <= kHeavyRow);
-        for (unsigned rest = __ballot_sync(0xffffffffu, mine && deg > kBuildShort && deg <= kHeavyRow) & leaders; rest;
+        // Rows of short_max..kHeavyRow entries go to k_build_long when it runs.
+        const bool mine = valid && !(long_rows_apart && deg > short_max && deg <= kHeavyRow);
+        for (unsigned rest = __ballot_sync(0xffffffffu, mine && deg > short_max && deg <= kHeavyRow) & leaders; rest;
              rest &= rest - 1) {
             const int leader = __ffs(rest) - 1;
             const int vv = static_cast<int>(base) + leader / W;
@@ -205,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
     if (directed_cut) cut_sum.finish(warp_sum(cut), directed_cut);
 }
 
-// The rows of kBuildShort..kHeavyRow entries (listed in `rows`), a warp per
+// The rows of short_max..kHeavyRow entries (listed in `rows`), a warp per
 // row: taken off a list, they spread evenly over all warps instead of
 // stalling the warps of k_build that drew them.
 template <class C>
@@ -253,9 +252,10 @@ __global__ void k_row_entries(const u32* count, const int* rows, const int* off,
 }
 struct IsLongRow {
     const int* off;
+    int short_max;
     __device__ bool operator()(i64 v) const {
         const int d = off[v + 1] - off[v];
-        return d > kBuildShort && d <= kHeavyRow;
+        return d > short_max && d <= kHeavyRow;
     }
 };
 
@@ -1970,8 +1970,9 @@ template <class T>
 class LevelRefiner {
 public:
     LevelRefiner(Context& c, const DGraph& g, int k, double eps, int* labels, u64* loads, u64 total, bool log,
-                 bool verify)
-        : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log), verify(verify) {}
+                 bool verify, const Mapping& mapping)
+        : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log), verify(verify),
+          mapping(mapping) {}
 
     LevelResult run(bool has_known, u64 known);
 
@@ -1985,6 +1986,7 @@ private:
     u64 total;
     bool log;
     bool verify;
+    const Mapping& mapping;
     T* check_A = nullptr;       // verify: independent rebuild of the cache
     T* check_totals = nullptr;
 
@@ -2038,10 +2040,12 @@ private:
         const bool apart = long_count > 0;
         if (vec)
             launch(k_build<T, W, true>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes, apart);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes,
+                   mapping.build_short, apart);
         else
             launch(k_build<T, W, false>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
-                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes, apart);
+                   k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes,
+                   mapping.build_short, apart);
         if (apart)
             launch(k_build_long<T>, grid_for(long_count * 32, kThreads), kThreads, (kThreads / 32) * k * sizeof(T), s(),
                    long_count, static_cast<const int*>(long_rows), g.off, g.nbr, g.ew, static_cast<const int*>(labels), k,
@@ -2479,7 +2483,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     const bool priced = total > static_cast<u64>(n);
     // Short rows next to k (levels large enough to skip the exchange step,
     // which reads the cache): recompute affinities on demand.
-    on_demand = n > 65536 && g.maximum_degree <= static_cast<u64>(kOnDemandDegree) &&
+    on_demand = n > 65536 && g.maximum_degree <= static_cast<u64>(std::min(mapping.on_demand_degree, kOnDemandDegree)) &&
                 3 * g.maximum_degree < static_cast<u64>(k);
     if (!on_demand) {
         A = A_.alloc<T>(static_cast<size_t>(n) * k);
@@ -2488,7 +2492,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
             long_rows = A_.alloc<int>(n);
             ctx.clear_scalars(2);
             u32* count_dev = reinterpret_cast<u32*>(ctx.dev_scalars);
-            select_if(A_, s(), n, IsLongRow{g.off}, WriteIndex{long_rows}, count_dev);
+            select_if(A_, s(), n, IsLongRow{g.off, mapping.build_short}, WriteIndex{long_rows}, count_dev);
             launch(k_row_entries, grid_for(n, kThreads), kThreads, 0, s(), static_cast<const u32*>(count_dev),
                    static_cast<const int*>(long_rows), g.off, ctx.dev_scalars + 1);
             const u64* sc = ctx.read_scalars(2);
@@ -2526,7 +2530,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     // An entry-by-entry update touches two random cache counters per entry
     // (about 128 bytes of DRAM traffic); a rebuild writes the whole cache and
     // reads the CSR once.
-    rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) / 100;
+    rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) /
+                      static_cast<u64>(std::max(1, mapping.rebuild_divisor));
     GP_CUDA(cudaMemsetAsync(counters + 7, 0, sizeof(u64), s()));
     build(has_known ? nullptr : counters + 7);
     launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
@@ -2618,7 +2623,7 @@ u64 device_cut(Context& ctx, const DGraph& g, const int* labels) {
 
 // refine_hierarchy_impl (src/refine.cu:483-730).
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
-                        int* labels, bool log, bool verify) {
+                        int* labels, bool log, bool verify, const Mapping& mapping) {
     cudaStream_t s = ctx.stream;
     const size_t L = h.levels.size();
     std::vector<int*> level_labels(L);
@@ -2638,8 +2643,8 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
         const auto t_begin = std::chrono::steady_clock::now();
         const LevelResult r =
             g.incident_bound <= 0xffffffffULL
-                ? LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known)
-                : LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log, verify).run(has_known, known);
+                ? LevelRefiner<u32>(ctx, g, k, eps, lab, loads, total, log, verify, mapping).run(has_known, known)
+                : LevelRefiner<u64>(ctx, g, k, eps, lab, loads, total, log, verify, mapping).run(has_known, known);
         if (log) {  // host time of the level; the stream is drained first
             GP_CUDA(cudaStreamSynchronize(s));
             std::printf("refine_level_time vertices=%lld ms=%.3f\n", static_cast<long long>(g.n),

@@ -413,6 +413,23 @@ def run_batch(args):
     ctx.close()
 
 
+def run_tune(args):
+    """gp_autotune on the R-MAT-22 k=64 workload and the 256^3 weighted mesh
+    (k=128): the partition time with the default thread-mapping thresholds
+    and with the ones the tuner chose (labels identical by construction)."""
+    gp = load_package()
+    cases = [("rmat22_k64", gp.rmat(22, 16, 0.57, 0.19, 0.19, 0), 64),
+             ("m3_k128", gp.mesh3d(256, 256, 256, weighted=True, seed=0), 128)]
+    out = []
+    for name, g, k in cases:
+        with gp.Context(0) as ctx:
+            t = ctx.autotune(g, k, WORKLOAD["epsilon"], WORKLOAD["seed"], repeats=args.tune_repeats)
+        out.append({"workload": name, "default_ms": t.pop("default_ms"), "tuned_ms": t.pop("tuned_ms"),
+                    "trials": t.pop("trials"), "thresholds": t})
+    print(json.dumps({"metric": "partition ms, default vs autotuned thread-mapping thresholds",
+                      "unit": "ms", "higher_is_better": False, "data": "synthetic", "cases": out}), flush=True)
+
+
 def run_serving(args):
     """Serving form: a Poisson stream of requests (mean args.rate per second)
     against a gp_server whose graphs are resident on the device.  The graph
@@ -488,7 +505,7 @@ def main():
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
     ap.add_argument("--side", type=int, default=256, help="mesh side of --launch-list --workload m3")
-    ap.add_argument("--workload", choices=["rmat22", "batch", "serving", "m3"], default="rmat22",
+    ap.add_argument("--workload", choices=["rmat22", "batch", "serving", "m3", "tune"], default="rmat22",
                     help="batch: the uneven 512-graph set, serial vs gp_partition_batch; "
                          "serving: Poisson requests against a gp_server")
     ap.add_argument("--requests", type=int, default=1000)
@@ -497,6 +514,7 @@ def main():
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0)
     ap.add_argument("--batch-graphs", type=int, default=512)
     ap.add_argument("--concurrency", type=int, default=16)
+    ap.add_argument("--tune-repeats", type=int, default=2, help="--workload tune: partitions per setting")
     ap.add_argument("--profile-pattern", default="",
                     help="--launch-list: report launches, time and algorithmic bytes of the kernels matching this")
     ap.add_argument("--scale", type=int, default=22,
@@ -506,6 +524,8 @@ def main():
         launch_list(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "tune":
+        run_tune(args)
     elif args.workload == "serving":
         run_serving(args)
     elif args.impl == "reference":

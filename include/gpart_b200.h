@@ -207,6 +207,31 @@ gp_status gp_profile_begin(gp_context* ctx, const char* kernel_substring);
 gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms,
                          double* algorithmic_bytes);
 
+/* Thread-mapping thresholds (gp_set_option names in brackets).  They decide
+ * which kernel and how many threads handle a row, never a value, so a
+ * partition does not depend on them.  They replace fixed thresholds of the
+ * reference (src/coarsen.cu:288-291, incremental.cuh:8, src/coarsen.cu:1513):
+ *   medium_degree     [8, 256]    coarsening rows up to this: a warp and a shared hash
+ *   large_narrow      [256, 2048] coarsening rows up to this: the smaller shared table
+ *   build_short       [8, 2048]   cache-build rows up to this: 8 lanes per row
+ *   rebuild_divisor   [1, 1e5]    cache rebuilt when moved entries exceed (n k w + 8 m) / this
+ *   on_demand_degree  [0, 32]     no cache on levels whose maximum degree is at most this */
+typedef struct gp_tuning {
+    int32_t medium_degree, large_narrow, build_short, rebuild_divisor, on_demand_degree;
+    double default_ms;  /* best partition time with the thresholds the call started from */
+    double tuned_ms;    /* best partition time with the thresholds chosen */
+    int32_t trials;     /* partitions timed */
+} gp_tuning;
+
+/* Autotuner: partitions `graph` (host memory; uploaded once) `repeats` times
+ * per candidate setting, one threshold at a time over a fixed candidate
+ * list, keeping a value when it is at least 1% faster (best of the repeats,
+ * CUDA-event algorithm time).  Every trial's labels must equal those of the
+ * starting thresholds (GP_INTERNAL otherwise).  The chosen thresholds stay
+ * set on `ctx` and are reported in `out`. */
+gp_status gp_autotune(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon,
+                      uint32_t seed, int32_t repeats, gp_tuning* out);
+
 /* load_weighted_graph + make_device_weighted (src/graph.cpp:47-116,
  * 205-218): the reference's int64 indptr/indices files read straight into
  * device memory owned by the context.  Each file is read in chunks of 8 Mi
