@@ -1272,12 +1272,12 @@ __global__ void k_copy_chunks(DGraph g, const int* raw_off, const int* raw_t, co
 
 // ---------------------------------------------------------------- chunk lists
 
-__global__ void k_heavy_counts(i64 n, const int* off, u64* sc) {
+__global__ void k_heavy_counts(i64 n, const int* off, int heavy_min, u64* sc) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     u64 rows = 0, chunks = 0, entries = 0;
     if (v < n) {
         const int d = off[v + 1] - off[v];
-        if (d > kHeavyRow) { rows = 1; chunks = (d + kChunk - 1) / kChunk; entries = d; }
+        if (d > heavy_min) { rows = 1; chunks = (d + kChunk - 1) / kChunk; entries = d; }
     }
     block_atomic_add(sc, rows);
     block_atomic_add(sc + 1, chunks);
@@ -1285,7 +1285,8 @@ __global__ void k_heavy_counts(i64 n, const int* off, u64* sc) {
 }
 struct IsHeavyRow {
     const int* off;
-    __device__ bool operator()(i64 v) const { return off[v + 1] - off[v] > kHeavyRow; }
+    int heavy_min;
+    __device__ bool operator()(i64 v) const { return off[v + 1] - off[v] > heavy_min; }
 };
 struct ChunkCount {
     const int* heavy;
@@ -1762,27 +1763,29 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
 }  // namespace
 
 // Heavy-row list and chunk list of a level, in the hierarchy's storage.
-void build_chunks(Context& ctx, DGraph& g) {
+void build_chunks(Context& ctx, DGraph& g, int heavy_min, Arena* storage) {
     cudaStream_t s = ctx.stream;
+    Arena& out = storage ? *storage : ctx.persist;
+    g.heavy_min = heavy_min;
     g.heavy = nullptr;
     g.heavy_count = 0;
     g.chunks = 0;
     g.heavy_entries = 0;
     if (g.n <= 0) return;
     ctx.clear_scalars(3);
-    launch(k_heavy_counts, blocks_for(g.n, kThreads), kThreads, 0, s, g.n, g.off, ctx.dev_scalars);
+    launch(k_heavy_counts, blocks_for(g.n, kThreads), kThreads, 0, s, g.n, g.off, heavy_min, ctx.dev_scalars);
     const u64* sc = ctx.read_scalars(3);
     g.heavy_count = static_cast<i64>(sc[0]);
     g.chunks = static_cast<i64>(sc[1]);
     g.heavy_entries = static_cast<i64>(sc[2]);
     if (!g.heavy_count) return;
-    g.heavy = ctx.persist.alloc<int>(g.heavy_count);
-    g.chunk_row = ctx.persist.alloc<int>(g.chunks);
-    g.chunk_hidx = ctx.persist.alloc<int>(g.chunks);
-    g.chunk_begin = ctx.persist.alloc<int>(g.chunks);
+    g.heavy = out.alloc<int>(g.heavy_count);
+    g.chunk_row = out.alloc<int>(g.chunks);
+    g.chunk_hidx = out.alloc<int>(g.chunks);
+    g.chunk_begin = out.alloc<int>(g.chunks);
     ArenaScope scope(ctx.scratch);
     int* chunk_off = ctx.scratch.alloc<int>(g.heavy_count);
-    select_if(ctx.scratch, s, g.n, IsHeavyRow{g.off}, WriteIndex{g.heavy}, static_cast<u32*>(nullptr));
+    select_if(ctx.scratch, s, g.n, IsHeavyRow{g.off, heavy_min}, WriteIndex{g.heavy}, static_cast<u32*>(nullptr));
     exclusive_scan<int>(ctx.scratch, s, g.heavy_count, ChunkCount{g.heavy, g.off}, chunk_off, static_cast<int*>(nullptr));
     launch(k_emit_chunks, blocks_for(g.heavy_count, kThreads), kThreads, 0, s, g.heavy_count, g.heavy, g.off,
            static_cast<const int*>(chunk_off), g.chunk_row, g.chunk_hidx, g.chunk_begin);

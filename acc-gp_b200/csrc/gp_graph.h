@@ -36,6 +36,7 @@ struct DGraph {
     int* chunk_begin = nullptr;
     i64 chunks = 0;
     i64 heavy_entries = 0;  // CSR entries in heavy rows
+    int heavy_min = kHeavyRow;  // rows longer than this are the heavy (chunked) rows
 };
 
 // Chunk-parallel loop body helpers: the chunk's edge range.
@@ -112,7 +113,9 @@ struct Context {
 };
 
 // Entry points of the pipeline stages.
-void build_chunks(Context& ctx, DGraph& g);
+// Rows longer than heavy_min entries become g's heavy rows, listed with their
+// kChunk-entry chunks in `storage` (the context's persist arena by default).
+void build_chunks(Context& ctx, DGraph& g, int heavy_min = kHeavyRow, Arena* storage = nullptr);
 Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o);
 void keep_levels(Context& ctx, const Hierarchy& h);
 

@@ -36,7 +36,7 @@ __global__ void k_cut_chunks(DGraph g, const int* labels, u64* out) {
         if (labels[g.nbr[e]] != p) local += edge_w(g.ew, e);
     block_atomic_add(out, local);
 }
-__global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, u64* out) {
+__global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, const int* labels, int heavy_min, u64* out) {
     __shared__ WarpSum cut_sum;
     cut_sum.init();
     const int lane = threadIdx.x & 31;
@@ -44,7 +44,7 @@ __global__ void k_cut(i64 n, const int* off, const int* nbr, const u32* ew, cons
     for (i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
          v += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int p = labels[v];
-        if (off[v + 1] - off[v] > kHeavyRow) continue;  // k_cut_chunks
+        if (off[v + 1] - off[v] > heavy_min) continue;  // k_cut_chunks
         for (int e = off[v] + lane; e < off[v + 1]; e += 32)
             if (labels[nbr[e]] != p) local += edge_w(ew, e);
     }
@@ -138,7 +138,7 @@ template <class C, int W, bool Vectorized>
 __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const int* nbr, const u32* ew,
                                                     const int* labels, int k, C* A, C* totals, u64* directed_cut,
                                                     const u64* gate, u64 threshold, u64* work, u64 work_bytes,
-                                                    int short_max, bool long_rows_apart) {
+                                                    int short_max, bool long_rows_apart, int heavy_min) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ WarpSum cut_sum;
     if (gate && *gate <= threshold) return;  // incremental update chosen
@@ -164,12 +164,12 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
             for (int p = sub; p < k; p += W) hist[p] = 0;
         }
         __syncwarp();
-        if (deg <= short_max) {
+        if (deg <= short_max && deg <= heavy_min) {  // heavier rows belong to the chunk kernels
             accumulate_row(nbr, ew, labels, static_cast<int>(v), begin + sub, end, W, hist);
         }
-        // Rows of short_max..kHeavyRow entries go to k_build_long when it runs.
-        const bool mine = valid && !(long_rows_apart && deg > short_max && deg <= kHeavyRow);
-        for (unsigned rest = __ballot_sync(0xffffffffu, mine && deg > short_max && deg <= kHeavyRow) & leaders; rest;
+        // Rows of short_max..heavy_min entries go to k_build_long when it runs.
+        const bool mine = valid && !(long_rows_apart && deg > short_max && deg <= heavy_min);
+        for (unsigned rest = __ballot_sync(0xffffffffu, mine && deg > short_max && deg <= heavy_min) & leaders; rest;
              rest &= rest - 1) {
             const int leader = __ffs(rest) - 1;
             const int vv = static_cast<int>(base) + leader / W;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_build(i64 n, const int* off, const
     if (directed_cut) cut_sum.finish(warp_sum(cut), directed_cut);
 }
 
-// The rows of short_max..kHeavyRow entries (listed in `rows`), a warp per
+// The rows of short_max..heavy_min entries (listed in `rows`), a warp per
 // row: taken off a list, they spread evenly over all warps instead of
 // stalling the warps of k_build that drew them.
 template <class C>
@@ -252,10 +252,10 @@ __global__ void k_row_entries(const u32* count, const int* rows, const int* off,
 }
 struct IsLongRow {
     const int* off;
-    int short_max;
+    int short_max, heavy_min;
     __device__ bool operator()(i64 v) const {
         const int d = off[v + 1] - off[v];
-        return d > short_max && d <= kHeavyRow;
+        return d > short_max && d <= heavy_min;
     }
 };
 
@@ -327,6 +327,7 @@ struct LpParams {
     int* cand;
     int* movers;
     u64* counters;  // 0 candidates, 1 movers, 2 delta (signed), 3 max load
+    int heavy_min;  // rows longer than this go through the chunk kernels
 };
 
 // incremental_lp_proposal (incremental.cuh:166-198).  A warp takes 32
@@ -549,7 +550,7 @@ __global__ void k_filter(LpParams q) {
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
          i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int v = q.cand[i];
-        if (q.off[v + 1] - q.off[v] > kHeavyRow) continue;  // k_filter_chunks / k_filter_finish
+        if (q.off[v + 1] - q.off[v] > q.heavy_min) continue;  // k_filter_chunks / k_filter_finish
         const int s = q.labels[v], t = q.targets[v];
         const long long gain = q.gains[v];
         const int end = q.off[v + 1];
@@ -711,7 +712,7 @@ __global__ void k_compact_movers(LpParams q) {
 template <class C>
 __global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
                          const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
-                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold) {
+                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold, int heavy_min) {
     __shared__ WarpSum delta_sum;
     const int lane = threadIdx.x & 31;
     if (gate && *gate > threshold) return;  // rebuild chosen
@@ -721,7 +722,7 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
          i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int v = movers[i];
-        if (off[v + 1] - off[v] > kHeavyRow) continue;  // k_update_chunks
+        if (off[v + 1] - off[v] > heavy_min) continue;  // k_update_chunks
         const int s = labels[v], t = targets[v];
         const int end = off[v + 1];
         long long gain = 0;
@@ -1961,6 +1962,8 @@ struct Flagged {
 
 // ---------------------------------------------------------------- host side
 
+constexpr int kSmallLevelHeavyRow = 256;  // heavy-row threshold of levels of at most 65,536 vertices
+
 struct LevelResult {
     u64 cut = 0;
     bool refined = false, repair_failed = false;
@@ -1978,7 +1981,7 @@ public:
 
 private:
     Context& ctx;
-    const DGraph& g;
+    DGraph g;  // the level; small levels get their own chunk list (run())
     int k;
     double eps;
     int* labels;
@@ -2041,11 +2044,11 @@ private:
         if (vec)
             launch(k_build<T, W, true>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
                    k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, true>), bytes,
-                   mapping.build_short, apart);
+                   mapping.build_short, apart, g.heavy_min);
         else
             launch(k_build<T, W, false>, grid, kThreads, smem, s(), n, g.off, g.nbr, g.ew, static_cast<const int*>(labels),
                    k, A, totals, directed_cut, gate, threshold, work_counter(k_build<T, W, false>), bytes,
-                   mapping.build_short, apart);
+                   mapping.build_short, apart, g.heavy_min);
         if (apart)
             launch(k_build_long<T>, grid_for(long_count * 32, kThreads), kThreads, (kThreads / 32) * k * sizeof(T), s(),
                    long_count, static_cast<const int*>(long_rows), g.off, g.nbr, g.ew, static_cast<const int*>(labels), k,
@@ -2085,7 +2088,7 @@ private:
         else
             launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
                    g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
-                   sample ? samples : static_cast<Sample*>(nullptr), gate, threshold);
+                   sample ? samples : static_cast<Sample*>(nullptr), gate, threshold, g.heavy_min);
         if (g.chunks)
             launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
                    static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
@@ -2170,7 +2173,8 @@ private:
 template <class T>
 i64 LevelRefiner<T>::lp_round(double filter) {
     GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
-    LpParams q{n, k, C, filter, g.off, g.nbr, g.ew, g.vw, labels, loads, prices, targets, gains, locks, flags, cand, movers, counters};
+    LpParams q{n,     k,      C,     filter, g.off, g.nbr, g.ew,   g.vw,     labels, loads,
+               prices, targets, gains, locks, flags, cand,  movers, counters, g.heavy_min};
     proposals(q);
     if (on_demand)
         with_row_size([&](auto d) { launch(k_filter_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), q); });
@@ -2477,6 +2481,11 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     Arena& A_ = ctx.scratch;
     ArenaScope scope(A_);
     n = g.n;
+    // Small levels: rows above kSmallLevelHeavyRow entries (coarse hubs) go
+    // through the block-per-chunk kernels instead of one warp each, which
+    // otherwise set the time of every row-parallel pass of the level.
+    if (n <= 65536 && g.maximum_degree > static_cast<u64>(kSmallLevelHeavyRow))
+        build_chunks(ctx, g, kSmallLevelHeavyRow, &A_);
     uint64_t cap = 0;
     if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
     C = cap;
@@ -2492,7 +2501,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
             long_rows = A_.alloc<int>(n);
             ctx.clear_scalars(2);
             u32* count_dev = reinterpret_cast<u32*>(ctx.dev_scalars);
-            select_if(A_, s(), n, IsLongRow{g.off, mapping.build_short}, WriteIndex{long_rows}, count_dev);
+            select_if(A_, s(), n, IsLongRow{g.off, mapping.build_short, g.heavy_min}, WriteIndex{long_rows}, count_dev);
             launch(k_row_entries, grid_for(n, kThreads), kThreads, 0, s(), static_cast<const u32*>(count_dev),
                    static_cast<const int*>(long_rows), g.off, ctx.dev_scalars + 1);
             const u64* sc = ctx.read_scalars(2);
@@ -2614,7 +2623,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
 u64 device_cut(Context& ctx, const DGraph& g, const int* labels) {
     ctx.clear_scalars(1);
     launch(k_cut, std::min(blocks_for(g.n * 32, 256), 148 * 32), 256, 0, ctx.stream, g.n, g.off, g.nbr, g.ew, labels,
-           ctx.dev_scalars);
+           g.heavy_min, ctx.dev_scalars);
     if (g.chunks) launch(k_cut_chunks, static_cast<int>(g.chunks), 256, 0, ctx.stream, g, labels, ctx.dev_scalars);
     const u64 d = ctx.read_scalars(1)[0];
     if (d & 1ULL) fail(GP_INTERNAL, "refinement cut is not symmetric");
