@@ -1963,6 +1963,7 @@ struct Flagged {
 // ---------------------------------------------------------------- host side
 
 constexpr int kSmallLevelHeavyRow = 256;  // heavy-row threshold of levels of at most 65,536 vertices
+constexpr int kMidLevelHeavyRow = 512;    // and of levels of at most 2^20 vertices
 
 struct LevelResult {
     u64 cut = 0;
@@ -2481,11 +2482,11 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     Arena& A_ = ctx.scratch;
     ArenaScope scope(A_);
     n = g.n;
-    // Small levels: rows above kSmallLevelHeavyRow entries (coarse hubs) go
-    // through the block-per-chunk kernels instead of one warp each, which
-    // otherwise set the time of every row-parallel pass of the level.
-    if (n <= 65536 && g.maximum_degree > static_cast<u64>(kSmallLevelHeavyRow))
-        build_chunks(ctx, g, kSmallLevelHeavyRow, &A_);
+    // Smaller levels: rows above a lower threshold (coarse hubs) go through
+    // the block-per-chunk kernels instead of one warp each, which otherwise
+    // set the time of every row-parallel pass of the level.
+    const int heavy_min = n <= 65536 ? kSmallLevelHeavyRow : n <= (1 << 20) ? kMidLevelHeavyRow : kHeavyRow;
+    if (heavy_min < kHeavyRow && g.maximum_degree > static_cast<u64>(heavy_min)) build_chunks(ctx, g, heavy_min, &A_);
     uint64_t cap = 0;
     if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
     C = cap;
