@@ -541,36 +541,62 @@ __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q) {
     }
 }
 
-// incremental_priority_filter (incremental.cuh:361-393): one warp per
-// candidate; a vertex keeps its move when its gain corrected by the intended
-// moves of higher-priority neighbours stays non-negative.
+// Correction of candidate v (part s to t, gain `gain`) from the entries
+// first, first + stride, ... < end: the moves of its higher-priority
+// neighbours.  Two entries per lane at a time; the neighbour's target, gain
+// and label are gathered together.
+__device__ __forceinline__ long long filter_entries(const LpParams& q, int v, int s, int t, long long gain, int first,
+                                                    int end, int stride) {
+    long long corr = 0;
+    for (int e0 = first; e0 < end; e0 += 2 * stride) {
+        const int e1 = e0 + stride;
+        const int u0 = q.nbr[e0], u1 = e1 < end ? q.nbr[e1] : v;
+        const int t0 = q.targets[u0], l0 = q.labels[u0];
+        const long long g0 = q.gains[u0];
+        const int t1 = u1 != v ? q.targets[u1] : -1, l1 = u1 != v ? q.labels[u1] : 0;
+        const long long g1 = u1 != v ? q.gains[u1] : 0;
+        if (u0 != v && t0 >= 0 && (g0 > gain || (g0 == gain && u0 < v)))
+            corr += static_cast<long long>(edge_w(q.ew, e0)) * ((t0 == t) - (t0 == s) - (l0 == t) + (l0 == s));
+        if (u1 != v && t1 >= 0 && (g1 > gain || (g1 == gain && u1 < v)))
+            corr += static_cast<long long>(edge_w(q.ew, e1)) * ((t1 == t) - (t1 == s) - (l1 == t) + (l1 == s));
+    }
+    return corr;
+}
+// incremental_priority_filter (incremental.cuh:361-393): a vertex keeps its
+// move when its gain corrected by the intended moves of higher-priority
+// neighbours stays non-negative.  A warp takes four candidates at a time: rows of up to kFilterShort
+// entries are read by eight lanes each, longer ones (up to heavy_min) by the
+// whole warp after them.
+constexpr int kFilterShort = 16;
 __global__ void k_filter(LpParams q) {
-    const int lane = threadIdx.x & 31;
+    constexpr int W = 8, G = 32 / W;
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
     const i64 count = static_cast<i64>(q.counters[0]);
-    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
-         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
-        const int v = q.cand[i];
-        if (q.off[v + 1] - q.off[v] > q.heavy_min) continue;  // k_filter_chunks / k_filter_finish
-        const int s = q.labels[v], t = q.targets[v];
-        const long long gain = q.gains[v];
-        const int end = q.off[v + 1];
-        long long corr = 0;
-        // Two entries per lane at a time; the neighbour's target, gain and
-        // label are gathered together.
-        for (int e0 = q.off[v] + lane; e0 < end; e0 += 64) {
-            const int e1 = e0 + 32;
-            const int u0 = q.nbr[e0], u1 = e1 < end ? q.nbr[e1] : v;
-            const int t0 = q.targets[u0], l0 = q.labels[u0];
-            const long long g0 = q.gains[u0];
-            const int t1 = u1 != v ? q.targets[u1] : -1, l1 = u1 != v ? q.labels[u1] : 0;
-            const long long g1 = u1 != v ? q.gains[u1] : 0;
-            if (u0 != v && t0 >= 0 && (g0 > gain || (g0 == gain && u0 < v)))
-                corr += static_cast<long long>(edge_w(q.ew, e0)) * ((t0 == t) - (t0 == s) - (l0 == t) + (l0 == s));
-            if (u1 != v && t1 >= 0 && (g1 > gain || (g1 == gain && u1 < v)))
-                corr += static_cast<long long>(edge_w(q.ew, e1)) * ((t1 == t) - (t1 == s) - (l1 == t) + (l1 == s));
+    unsigned leaders = 0;
+    for (int g = 0; g < G; ++g) leaders |= 1u << (g * W);
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
+    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; base < count;
+         base += warps * G) {
+        const i64 i = base + gid;
+        const int v = i < count ? q.cand[i] : -1;
+        const int begin = v >= 0 ? q.off[v] : 0, end = v >= 0 ? q.off[v + 1] : 0;
+        const bool light = v >= 0 && end - begin <= q.heavy_min;  // heavier rows: k_filter_chunks / k_filter_finish
+        const int s = light ? q.labels[v] : 0, t = light ? q.targets[v] : 0;
+        const long long gain = light ? q.gains[v] : 0;
+        long long corr = light && end - begin <= kFilterShort ? filter_entries(q, v, s, t, gain, begin + sub, end, W) : 0;
+        for (unsigned rest = __ballot_sync(0xffffffffu, light && end - begin > kFilterShort) & leaders; rest;
+             rest &= rest - 1) {
+            const int leader = __ffs(rest) - 1;
+            const int vv = __shfl_sync(0xffffffffu, v, leader), ss = __shfl_sync(0xffffffffu, s, leader),
+                      tt = __shfl_sync(0xffffffffu, t, leader), b = __shfl_sync(0xffffffffu, begin, leader),
+                      e = __shfl_sync(0xffffffffu, end, leader);
+            const long long gg = __shfl_sync(0xffffffffu, gain, leader);
+            const long long c = warp_sum(filter_entries(q, vv, ss, tt, gg, b + lane, e, 32));
+            if (lane == leader) corr += c;
         }
-        corr = warp_sum(corr);
-        if (lane == 0) {
+#pragma unroll
+        for (int d = W / 2; d; d >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, d, W);
+        if (sub == 0 && light) {
             bool keep;
             if (q.prices) {
                 const u64 w = q.vw[v];
@@ -706,61 +732,94 @@ __global__ void k_compact_movers(LpParams q) {
     }
 }
 
+// Cut change and cache updates of the entries first, first + stride, ... <
+// end of mover v (part s to part t); two entries per lane at a time, so that
+// their gathers are in flight together.  An edge whose both ends move is
+// counted by its larger endpoint's partner rule.
+template <class C>
+__device__ __forceinline__ long long update_entries(int v, int s, int t, int first, int end, int stride, const int* nbr,
+                                                    const u32* ew, const int* labels, const int* targets,
+                                                    const int* flags, int k, C* A) {
+    long long gain = 0;
+    for (int e0 = first; e0 < end; e0 += 2 * stride) {
+        const int e1 = e0 + stride;
+        const int u0 = nbr[e0], u1 = e1 < end ? nbr[e1] : v;
+        const int old0 = labels[u0], f0 = flags[u0], t0 = targets[u0];
+        const int old1 = u1 != v ? labels[u1] : 0, f1 = u1 != v ? flags[u1] : 0, t1 = u1 != v ? targets[u1] : 0;
+        if (u0 != v) {
+            const u32 w = edge_w(ew, e0);
+            const bool moves = f0 != 0;
+            const int nw = moves ? t0 : old0;
+            if (A) {  // no cache with on-demand affinities
+                atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
+            }
+            if (!moves || u0 > v) gain += static_cast<long long>(w) * ((s != old0) - (t != nw));
+        }
+        if (u1 != v) {
+            const u32 w = edge_w(ew, e1);
+            const bool moves = f1 != 0;
+            const int nw = moves ? t1 : old1;
+            if (A) {
+                atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
+                atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
+            }
+            if (!moves || u1 > v) gain += static_cast<long long>(w) * ((s != old1) - (t != nw));
+        }
+    }
+    return gain;
+}
+
 // incremental_update_cache_and_cut (incremental.cuh:440-506): exact cut delta
-// (an edge whose both ends move is counted by its larger endpoint's partner
-// rule) and dense cache updates; optional repair samples per source part.
+// and dense cache updates; optional repair samples per source part.  A warp
+// takes four movers at a time: rows of up to kUpdateShort entries are done by
+// eight lanes each, longer ones (up to heavy_min) by the whole warp after
+// them, so a warp's memory chains cover four short rows at once.
+constexpr int kUpdateShort = 16;
 template <class C>
 __global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
                          const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
                          C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold, int heavy_min) {
+    constexpr int W = 8, G = 32 / W;
     __shared__ WarpSum delta_sum;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
     if (gate && *gate > threshold) return;  // rebuild chosen
     delta_sum.init();
     if (live_count) count = static_cast<i64>(*live_count);
+    unsigned leaders = 0;
+    for (int g = 0; g < G; ++g) leaders |= 1u << (g * W);
+    const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
     long long total = 0;
-    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
-         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
-        const int v = movers[i];
-        if (off[v + 1] - off[v] > heavy_min) continue;  // k_update_chunks
-        const int s = labels[v], t = targets[v];
-        const int end = off[v + 1];
-        long long gain = 0;
-        // Two entries per lane at a time: their gathers are in flight together.
-        for (int e0 = off[v] + lane; e0 < end; e0 += 64) {
-            const int e1 = e0 + 32;
-            const int u0 = nbr[e0], u1 = e1 < end ? nbr[e1] : v;
-            const int old0 = labels[u0], f0 = flags[u0], t0 = targets[u0];
-            const int old1 = u1 != v ? labels[u1] : 0, f1 = u1 != v ? flags[u1] : 0, t1 = u1 != v ? targets[u1] : 0;
-            if (u0 != v) {
-                const u32 w = edge_w(ew, e0);
-                const bool moves = f0 != 0;
-                const int nw = moves ? t0 : old0;
-                if (A) {  // no cache with on-demand affinities
-                    atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                    atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
-                }
-                if (!moves || u0 > v) gain += static_cast<long long>(w) * ((s != old0) - (t != nw));
-            }
-            if (u1 != v) {
-                const u32 w = edge_w(ew, e1);
-                const bool moves = f1 != 0;
-                const int nw = moves ? t1 : old1;
-                if (A) {
-                    atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                    atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
-                }
-                if (!moves || u1 > v) gain += static_cast<long long>(w) * ((s != old1) - (t != nw));
-            }
+    for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; base < count;
+         base += warps * G) {
+        const i64 i = base + gid;
+        const int v = i < count ? movers[i] : -1;
+        const int begin = v >= 0 ? off[v] : 0, end = v >= 0 ? off[v + 1] : 0;
+        const bool light = v >= 0 && end - begin <= heavy_min;  // heavier rows: k_update_chunks
+        const int s = light ? labels[v] : 0, t = light ? targets[v] : 0;
+        long long gain = light && end - begin <= kUpdateShort
+                             ? update_entries(v, s, t, begin + sub, end, W, nbr, ew, labels, targets, flags, k, A)
+                             : 0;
+        for (unsigned rest = __ballot_sync(0xffffffffu, light && end - begin > kUpdateShort) & leaders; rest;
+             rest &= rest - 1) {
+            const int leader = __ffs(rest) - 1;
+            const int vv = __shfl_sync(0xffffffffu, v, leader), ss = __shfl_sync(0xffffffffu, s, leader),
+                      tt = __shfl_sync(0xffffffffu, t, leader), b = __shfl_sync(0xffffffffu, begin, leader),
+                      e = __shfl_sync(0xffffffffu, end, leader);
+            const long long g = warp_sum(update_entries(vv, ss, tt, b + lane, e, 32, nbr, ew, labels, targets, flags, k, A));
+            if (lane == leader) gain += g;
         }
-        gain = warp_sum(gain);
-        total += gain;
-        if (samples && lane == 0) {
-            atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
-            atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
+#pragma unroll
+        for (int d = W / 2; d; d >>= 1) gain += __shfl_xor_sync(0xffffffffu, gain, d, W);
+        if (sub == 0 && light) {
+            total += gain;
+            if (samples) {
+                atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
+                atomicAdd(&samples[s].weight, static_cast<u64>(vw[v]));
+            }
         }
     }
-    delta_sum.finish(static_cast<u64>(total), reinterpret_cast<u64*>(delta));
+    delta_sum.finish(static_cast<u64>(warp_sum(total)), reinterpret_cast<u64*>(delta));
 }
 
 // Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,
@@ -2087,7 +2146,7 @@ private:
                        sample ? samples : static_cast<Sample*>(nullptr));
             });
         else
-            launch(k_update<T>, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
+            launch(k_update<T>, grid_for(host_count * 8, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
                    g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
                    sample ? samples : static_cast<Sample*>(nullptr), gate, threshold, g.heavy_min);
         if (g.chunks)
@@ -2180,7 +2239,7 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     if (on_demand)
         with_row_size([&](auto d) { launch(k_filter_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), q); });
     else
-        launch(k_filter, grid_for(n * 32, kThreads), kThreads, 0, s(), q);
+        launch(k_filter, grid_for(n * 8, kThreads), kThreads, 0, s(), q);
     if (g.chunks) {
         GP_CUDA(cudaMemsetAsync(corr_acc, 0, sizeof(long long) * g.heavy_count, s()));
         launch(k_filter_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, q, corr_acc);
