@@ -488,16 +488,20 @@ struct RowRegs {
 // k_proposals with on-demand affinities: the same target (largest
 // affinity, or affinity minus repair price; lowest part on ties), filter
 // and outputs.
+// `rows` (*row_count entries), when given, lists the vertices to visit (the
+// level's frontier); every other vertex is interior and would not propose.
 template <int D>
-__global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q) {
+__global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q, const int* rows, const u64* row_count) {
     __shared__ u64 s_slack[kMaxParts];
     __shared__ double s_price[kMaxParts];
     if (q.prices)
         for (int p = threadIdx.x; p < q.k; p += blockDim.x) { s_slack[p] = q.capacity - q.loads[p]; s_price[p] = q.prices[p]; }
     __syncthreads();
-    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < q.n;
+    const i64 visits = rows ? static_cast<i64>(*row_count) : q.n;
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < visits;
          block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
-        const i64 v = block_base + threadIdx.x;
+        const i64 index = block_base + threadIdx.x;
+        const i64 v = index < visits ? (rows ? rows[index] : index) : q.n;
         bool propose = false;
         if (v < q.n) {
             if (q.locks[v]) {
@@ -678,6 +682,60 @@ __global__ void __launch_bounds__(kThreads) k_update_od(i64 count, const int* mo
         }
     }
     delta_sum.finish(static_cast<u64>(warp_sum(total)), reinterpret_cast<u64*>(delta));
+}
+
+// Conservative frontier of a level (initialize_affinity_frontier and
+// AffinityView::touch, incremental.cuh:210-224, affinity.cuh:33-40): every
+// vertex that was a boundary vertex at some point of the level, listed once.
+// The LP proposals visit only these; a vertex outside it has every
+// neighbour in its own part and would not propose.
+struct Frontier {
+    int* members;  // 1 when listed
+    int* rows;
+    u64* count;
+};
+__device__ __forceinline__ void touch(const Frontier& f, int v) {
+    if (!f.members[v] && atomicExch(f.members + v, 1) == 0) f.rows[atomicAdd(f.count, 1ULL)] = v;
+}
+// After a batch of moves: the movers and their neighbours, whose boundary
+// status may have changed, join the frontier; a warp per mover.
+__global__ void k_touch_rows(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
+                             Frontier f) {
+    if (live_count) count = static_cast<i64>(*live_count);
+    const int lane = threadIdx.x & 31;
+    for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
+         i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
+        const int v = movers[i];
+        if (lane == 0) touch(f, v);
+        for (int e = off[v] + lane; e < off[v + 1]; e += 32) touch(f, nbr[e]);
+    }
+}
+// The initial frontier of an on-demand level: rows whose connection to their
+// own part is below their total weight (the proposal's boundary test).
+// Every target is reset to -1, as a proposal pass over all rows leaves the
+// rows that do not propose.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_frontier_init_od(i64 n, const int* off, const int* nbr, const u32* ew,
+                                                               const int* labels, int* targets, Frontier f) {
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < n;
+         block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 v = block_base + threadIdx.x;
+        bool boundary = false;
+        if (v < n) {
+            RowRegs<D> r;
+            r.load(static_cast<int>(v), off, nbr, ew, labels);
+            boundary = r.of(labels[v]) != r.total;
+            f.members[v] = boundary;
+            targets[v] = -1;
+        }
+        block_append(static_cast<int>(v), boundary, f.rows, f.count);
+    }
+}
+// Repair donors that are not in the frontier must read as non-proposers
+// (target -1) in the next LP round, as after a proposal pass over all rows.
+__global__ void k_reset_targets(i64 count, const u32* donors, int* targets) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) targets[donors[i]] = -1;
 }
 
 // Heavy candidates: partial corrections per chunk, then the decision
@@ -2072,6 +2130,8 @@ private:
     u64 rebuild_entries = ~0ULL;  // mover entries above which apply() rebuilds the cache
     i64 repair_iterations = 0, repair_donors = 0;  // for the per-level log line
     bool on_demand = false;  // no dense cache: affinities recomputed from the rows
+    Frontier frontier{};         // on-demand levels: the rows the LP proposals visit
+    bool frontier_on = false;
     int* long_rows = nullptr;  // rows built by k_build_long (large levels)
     i64 long_count = 0, long_entries = 0;
     u64 max_load_host = 0;
@@ -2157,6 +2217,9 @@ private:
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
         launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
+        if (frontier_on)
+            launch(k_touch_rows, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
+                   g.nbr, frontier);
         if (gate) build(counters + 7, gate, threshold);
         launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     }
@@ -2192,7 +2255,11 @@ private:
     void proposals(const LpParams& q) {
         const int grid = grid_for(n, kThreads);
         if (on_demand) {
-            with_row_size([&](auto d) { launch(k_proposals_od<decltype(d)::value>, grid, kThreads, 0, s(), q); });
+            const int* rows = frontier_on ? frontier.rows : nullptr;
+            const u64* count = frontier_on ? frontier.count : nullptr;
+            with_row_size([&](auto d) {
+                launch(k_proposals_od<decltype(d)::value>, grid, kThreads, 0, s(), q, rows, count);
+            });
             return;
         }
         const T* a = A;
@@ -2412,6 +2479,9 @@ bool LevelRefiner<T>::repair() {
                 }
             }
         }
+        if (frontier_on && dcount > 0)
+            launch(k_reset_targets, blocks_for(dcount, kThreads), kThreads, 0, s(), dcount,
+                   static_cast<const u32*>(donors), targets);
         ++iterations;
         const bool feasible = max_load_host <= C;
         if (feasible || placed == 0 || iterations >= 2 * k + 4) return feasible;
@@ -2622,6 +2692,23 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
             res.repair_failed = true;
             return res;
         }
+    }
+    // Levels without a cache: the LP proposals visit a conservative frontier
+    // when it starts with at most a quarter of the rows (the reference's rule,
+    // incremental.cuh:783-797).
+    if (on_demand) {
+        frontier.members = A_.alloc<int>(n);
+        frontier.rows = A_.alloc<int>(n);
+        frontier.count = A_.alloc<u64>(1);
+        GP_CUDA(cudaMemsetAsync(frontier.count, 0, sizeof(u64), s()));
+        with_row_size([&](auto d) {
+            launch(k_frontier_init_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), n,
+                   static_cast<const int*>(g.off), static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
+                   static_cast<const int*>(labels), targets, frontier);
+        });
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, frontier.count, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        frontier_on = ctx.host_scalars[0] <= static_cast<u64>(n) / 4;
     }
     const u64 feasible_start = cut;
     u64 best = cut;

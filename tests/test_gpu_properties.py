@@ -73,6 +73,18 @@ def test_row_weight_sums_beyond_32_bits(gp, ctx, oracle):
     np.testing.assert_array_equal(labels, oracle.partition(g, 64, 1.03, 2)[0])
 
 
+@pytest.mark.parametrize("side, k, seed", [(64, 128, 2), (48, 64, 5)])
+def test_weighted_mesh_levels_without_cache_match_oracle(gp, ctx, oracle, side, k, seed):
+    """Levels above 65,536 vertices whose rows are short next to k keep no
+    affinity cache, and their LP proposals visit only the frontier of rows
+    that have been boundary rows; capacity repair runs with prices (weighted
+    vertices).  The labels must still equal the oracle's full scan."""
+    g = gp.mesh3d(side, side, side, weighted=True, seed=1)
+    labels, st = ctx.partition(g, k, 1.03, seed)
+    check(gp, g, labels, st, k, 1.03)
+    np.testing.assert_array_equal(labels, oracle.partition(g, k, 1.03, seed)[0])
+
+
 def test_fewer_vertices_than_parts_is_rejected(gp, ctx):
     g = gp.grid2d(3, 3)
     with pytest.raises(gp.GpartError) as e:
