@@ -338,7 +338,8 @@ struct LpParams {
 // appends per warp, append_warp, incremental.cuh:201-208; the order of the
 // candidate list does not affect any result).
 template <class C, int W, bool Vectorized>
-__global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, const C* totals) {
+__global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, const C* totals, const int* rows,
+                                                        const u64* row_count) {
     using Vec = AffinityVec<C>;
     constexpr int N = Vectorized ? Vec::N : 1;
     constexpr int G = 32 / W;
@@ -351,11 +352,13 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
     __syncthreads();
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
     // Block-uniform passes (the append synchronises the block); warp w of the
-    // block takes vertices [32w, 32w + 32) of the block's 256.
-    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < q.n;
+    // block takes entries [32w, 32w + 32) of the block's 256: vertices, or
+    // positions of `rows` (*row_count entries, the level's frontier) when given.
+    const i64 visits = rows ? static_cast<i64>(*row_count) : q.n;
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < visits;
          block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
-        const i64 base = block_base + (threadIdx.x & ~31);
-        const i64 v = base + lane;
+        const i64 index = block_base + threadIdx.x;
+        const i64 v = index < visits ? (rows ? rows[index] : index) : q.n;
         int src = 0;
         u64 current = 0;
         bool act = false;
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
             const int owner = mine ? __ffs(mine) - 1 : -1;
             const int osrc = __shfl_sync(0xffffffffu, src, owner < 0 ? 0 : owner);
             const u64 ocur = __shfl_sync(0xffffffffu, current, owner < 0 ? 0 : owner);
-            const i64 vv = base + owner;
+            const i64 vv = __shfl_sync(0xffffffffu, v, owner < 0 ? 0 : owner);
             int target = -1;
             u64 best = 0;
             double best_score = -DBL_MAX;
@@ -698,17 +701,25 @@ __device__ __forceinline__ void touch(const Frontier& f, int v) {
     if (!f.members[v] && atomicExch(f.members + v, 1) == 0) f.rows[atomicAdd(f.count, 1ULL)] = v;
 }
 // After a batch of moves: the movers and their neighbours, whose boundary
-// status may have changed, join the frontier; a warp per mover.
+// status may have changed, join the frontier; a warp per mover, the
+// neighbours of heavy movers by k_touch_chunks.
 __global__ void k_touch_rows(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
-                             Frontier f) {
+                             int heavy_min, Frontier f) {
     if (live_count) count = static_cast<i64>(*live_count);
     const int lane = threadIdx.x & 31;
     for (i64 i = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < count;
          i += (static_cast<i64>(gridDim.x) * blockDim.x) >> 5) {
         const int v = movers[i];
         if (lane == 0) touch(f, v);
+        if (off[v + 1] - off[v] > heavy_min) continue;
         for (int e = off[v] + lane; e < off[v + 1]; e += 32) touch(f, nbr[e]);
     }
+}
+// The chunks of heavy rows whose vertex moves (flag set), a block per chunk.
+__global__ void k_touch_chunks(DGraph g, const int* flags, Frontier f) {
+    const int c = blockIdx.x, v = g.chunk_row[c];
+    if (!flags[v]) return;
+    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) touch(f, g.nbr[e]);
 }
 // The initial frontier of an on-demand level: rows whose connection to their
 // own part is below their total weight (the proposal's boundary test).
@@ -725,6 +736,22 @@ __global__ void __launch_bounds__(kThreads) k_frontier_init_od(i64 n, const int*
             RowRegs<D> r;
             r.load(static_cast<int>(v), off, nbr, ew, labels);
             boundary = r.of(labels[v]) != r.total;
+            f.members[v] = boundary;
+            targets[v] = -1;
+        }
+        block_append(static_cast<int>(v), boundary, f.rows, f.count);
+    }
+}
+// The same for a level with a dense cache: own-part affinity below the total.
+template <class C>
+__global__ void k_frontier_init(i64 n, const C* A, const C* totals, int k, const int* labels, int* targets,
+                                Frontier f) {
+    for (i64 block_base = static_cast<i64>(blockIdx.x) * blockDim.x; block_base < n;
+         block_base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 v = block_base + threadIdx.x;
+        bool boundary = false;
+        if (v < n) {
+            boundary = A[v * k + labels[v]] != totals[v];
             f.members[v] = boundary;
             targets[v] = -1;
         }
@@ -2130,7 +2157,7 @@ private:
     u64 rebuild_entries = ~0ULL;  // mover entries above which apply() rebuilds the cache
     i64 repair_iterations = 0, repair_donors = 0;  // for the per-level log line
     bool on_demand = false;  // no dense cache: affinities recomputed from the rows
-    Frontier frontier{};         // on-demand levels: the rows the LP proposals visit
+    Frontier frontier{};         // levels above 65,536 vertices: the rows the LP proposals visit
     bool frontier_on = false;
     int* long_rows = nullptr;  // rows built by k_build_long (large levels)
     i64 long_count = 0, long_entries = 0;
@@ -2216,10 +2243,13 @@ private:
                    threshold);
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
-        launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
-        if (frontier_on)
+        if (frontier_on) {
             launch(k_touch_rows, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
-                   g.nbr, frontier);
+                   g.nbr, g.heavy_min, frontier);
+            if (g.chunks)
+                launch(k_touch_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(flags), frontier);
+        }
+        launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
         if (gate) build(counters + 7, gate, threshold);
         launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     }
@@ -2264,8 +2294,11 @@ private:
         }
         const T* a = A;
         const T* t = totals;
+        const int* rows = frontier_on ? frontier.rows : nullptr;
+        const u64* count = frontier_on ? frontier.count : nullptr;
         with_groups([&](auto width, auto vec) {
-            launch(k_proposals<T, decltype(width)::value, decltype(vec)::value>, grid, kThreads, 0, s(), q, a, t);
+            launch(k_proposals<T, decltype(width)::value, decltype(vec)::value>, grid, kThreads, 0, s(), q, a, t, rows,
+                   count);
         });
     }
     // GP_FLAG_VERIFY after every batch (incremental.cuh:846-853, 870-877):
@@ -2693,19 +2726,23 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
             return res;
         }
     }
-    // Levels without a cache: the LP proposals visit a conservative frontier
-    // when it starts with at most a quarter of the rows (the reference's rule,
-    // incremental.cuh:783-797).
-    if (on_demand) {
+    // Levels above 65,536 vertices (no exchange step): the LP proposals visit
+    // a conservative frontier when it starts with at most a quarter of the
+    // rows (the reference's rule, incremental.cuh:783-797).
+    if (n > 65536) {
         frontier.members = A_.alloc<int>(n);
         frontier.rows = A_.alloc<int>(n);
         frontier.count = A_.alloc<u64>(1);
         GP_CUDA(cudaMemsetAsync(frontier.count, 0, sizeof(u64), s()));
-        with_row_size([&](auto d) {
-            launch(k_frontier_init_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), n,
-                   static_cast<const int*>(g.off), static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
-                   static_cast<const int*>(labels), targets, frontier);
-        });
+        if (on_demand)
+            with_row_size([&](auto d) {
+                launch(k_frontier_init_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), n,
+                       static_cast<const int*>(g.off), static_cast<const int*>(g.nbr), static_cast<const u32*>(g.ew),
+                       static_cast<const int*>(labels), targets, frontier);
+            });
+        else
+            launch(k_frontier_init<T>, grid_for(n, kThreads), kThreads, 0, s(), n, static_cast<const T*>(A),
+                   static_cast<const T*>(totals), k, static_cast<const int*>(labels), targets, frontier);
         GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, frontier.count, sizeof(u64), cudaMemcpyDeviceToHost, s()));
         GP_CUDA(cudaStreamSynchronize(s()));
         frontier_on = ctx.host_scalars[0] <= static_cast<u64>(n) / 4;
