@@ -949,8 +949,11 @@ __global__ void k_mover_entries(i64 count, const int* movers, const u64* live_co
 
 // incremental_commit (incremental.cuh:532-547) with per-block aggregation of
 // the part-load changes.
+// Also keeps rlabels (the labels in repair order, rposition[v] the place of
+// v) current.
 __global__ void k_commit(i64 count, const int* movers, const u64* live_count, int* labels, const int* targets,
-                         const u32* vw, int k, u64* loads, unsigned char* locks, int* flags) {
+                         const u32* vw, int k, u64* loads, unsigned char* locks, int* flags, const u32* rposition,
+                         int* rlabels) {
     extern __shared__ long long diff[];
     if (live_count) count = static_cast<i64>(*live_count);
     for (int p = threadIdx.x; p < k; p += blockDim.x) diff[p] = 0;
@@ -962,6 +965,7 @@ __global__ void k_commit(i64 count, const int* movers, const u64* live_count, in
         atomicAdd(reinterpret_cast<u64*>(diff + s), static_cast<u64>(-w));
         atomicAdd(reinterpret_cast<u64*>(diff + t), static_cast<u64>(w));
         labels[v] = t;
+        rlabels[rposition[v]] = t;
         if (locks) locks[v] = 1;
     }
     __syncthreads();
@@ -1039,13 +1043,23 @@ __global__ void __launch_bounds__(kMaxParts) k_slack(int k, const u64* loads, u6
     }
 }
 
+// Position i of the repair order is a donor when its vertex's part is
+// overloaded; rlabels holds the labels in repair order, so this reads
+// sequentially.
 struct IsDonor {
-    const u32* order;
-    const int* labels;
+    const int* rlabels;
     const u64* loads;
     u64 capacity;
-    __device__ bool operator()(i64 i) const { return loads[labels[order[i]]] > capacity; }
+    __device__ bool operator()(i64 i) const { return loads[rlabels[i]] > capacity; }
 };
+// Labels in repair order, and each vertex's position in that order.
+__global__ void k_repair_positions(i64 n, const u32* order, const int* labels, u32* position, int* rlabels) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32 v = order[i];
+    position[v] = static_cast<u32>(i);
+    rlabels[i] = labels[v];
+}
 struct WriteOrdered {
     const u32* order;
     u32* out;
@@ -2151,6 +2165,8 @@ private:
     double* prices = nullptr;
     Sample* samples = nullptr;
     u32* rorder = nullptr;
+    u32* rposition = nullptr;  // place of each vertex in the repair order
+    int* rlabels = nullptr;    // labels in repair order
     u64* counters = nullptr;  // device: 0 cand, 1 movers, 2 delta, 3 max load, 4.. scratch
     long long* corr_acc = nullptr;  // per heavy row: priority-filter correction
     u64 cut = 0, revision = 0;
@@ -2242,7 +2258,8 @@ private:
                    reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr), gate,
                    threshold);
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
-               labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags);
+               labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags,
+               static_cast<const u32*>(rposition), rlabels);
         if (frontier_on) {
             launch(k_touch_rows, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    g.nbr, g.heavy_min, frontier);
@@ -2382,7 +2399,7 @@ bool LevelRefiner<T>::repair() {
     while (true) {
         ArenaScope it(A_);
         launch(k_slack, 1, kMaxParts, 0, s(), k, loads, C, slack, requests, cdf);
-        select_if(A_, s(), n, IsDonor{rorder, labels, loads, C}, WriteOrdered{rorder, donors}, donor_count);
+        select_if(A_, s(), n, IsDonor{rlabels, loads, C}, WriteOrdered{rorder, donors}, donor_count);
         GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
         GP_CUDA(cudaStreamSynchronize(s()));
         const i64 dcount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
@@ -2698,6 +2715,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
         u64* keys_alt = A_.alloc<u64>(n);
         launch(k_repair_keys, blocks_for(n, kThreads), kThreads, 0, s(), n, keys, rorder);
         radix_sort_pairs(A_, s(), n, keys, rorder, keys_alt, rorder_alt, 0, 32);
+        rposition = A_.alloc<u32>(n);
+        rlabels = A_.alloc<int>(n);
+        launch(k_repair_positions, blocks_for(n, kThreads), kThreads, 0, s(), n, static_cast<const u32*>(rorder),
+               static_cast<const int*>(labels), rposition, rlabels);
     }
     // An entry-by-entry update touches two random cache counters per entry
     // (about 128 bytes of DRAM traffic); a rebuild writes the whole cache and
@@ -2779,6 +2800,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     const bool restored = revision != best_revision;
     if (restored) {
         GP_CUDA(cudaMemcpyAsync(labels, saved_labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
+        launch(k_repair_positions, blocks_for(n, kThreads), kThreads, 0, s(), n, static_cast<const u32*>(rorder),
+               static_cast<const int*>(labels), rposition, rlabels);
         GP_CUDA(cudaMemcpyAsync(loads, saved_loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
         launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
         GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, sizeof(u64), cudaMemcpyDeviceToHost, s()));
