@@ -1410,8 +1410,11 @@ private:
             while (slots < 2 * static_cast<size_t>(c == 2 ? std::min(o.mapping.large_narrow, kLargeDegree) : kLargeDegree))
                 slots <<= 1;
             const size_t smem = slots * Table::kSlotBytes;
+            // The limit belongs to the kernel for the whole process, and
+            // worker contexts launch it from several threads: every call sets
+            // the same value, the largest table (2 x kLargeDegree slots).
             GP_CUDA(cudaFuncSetAttribute(k_affinity_large<Table>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
+                                         static_cast<int>(2 * kLargeDegree * Table::kSlotBytes)));
             launch(k_affinity_large<Table>, static_cast<int>(list_size[c]), 256, smem, ctx.stream, list_size[c], lists[c], p);
         }
         if (g.heavy_count) {
@@ -1697,12 +1700,10 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
                ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[3]) {
-        static bool configured = false;  // per process: the attribute belongs to the kernel
-        if (!configured) {
-            GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kBigSortSmem)));
-            configured = true;
-        }
+        // Set on every call (one fixed value): the attribute belongs to the
+        // kernel, on whichever device is current.
+        GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kBigSortSmem)));
         launch(k_sort_rows_big, static_cast<int>(count[3]), kBigSortThreads, kBigSortSmem, s, lists + 3 * nc, raw_off,
                raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     }

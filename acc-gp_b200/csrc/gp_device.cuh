@@ -75,6 +75,10 @@ inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem
     if (g_profiler) g_profiler->last_timed = timed;
     if (timed) g_profiler->before(stream);
     kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
+    // A launch that did not start (bad configuration, missing shared-memory
+    // opt-in) must fail the call, not leave its results silently unwritten.
+    if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess)
+        ::gp::fail(GP_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));
     if (timed) g_profiler->after(stream);
 }
 

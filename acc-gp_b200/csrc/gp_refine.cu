@@ -2592,7 +2592,11 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
     int empty = 0;
     for (int pass = 0; pass < 2; ++pass) {
         const size_t match_smem = sizeof(double) * k * k;
-        GP_CUDA(cudaFuncSetAttribute(k_match_parts, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(match_smem)));
+        // One value for every k: the limit belongs to the kernel for the whole
+        // process, and concurrent worker contexts must not lower it under
+        // each other's launches.
+        GP_CUDA(cudaFuncSetAttribute(k_match_parts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(sizeof(double) * kMaxParts * kMaxParts)));
         launch(k_match_parts, 1, kMatchThreads, match_smem, s(), k, quotient, partner, visits);
         GP_CUDA(cudaMemsetAsync(seeds, 0xff, sizeof(u64) * k * sw, s()));
         launch(k_seeds<T>, grid_for(n, kThreads), kThreads, 0, s(), n, labels, static_cast<const T*>(A), k, partner,
