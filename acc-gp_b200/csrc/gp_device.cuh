@@ -74,9 +74,13 @@ inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem
     const bool timed = g_profiler && g_profiler->matches(reinterpret_cast<const void*>(kernel));
     if (g_profiler) g_profiler->last_timed = timed;
     if (timed) g_profiler->before(stream);
-    kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
     // A launch that did not start (bad configuration, missing shared-memory
     // opt-in) must fail the call, not leave its results silently unwritten.
+    // The error left by an earlier call whose failure was already handled (an
+    // allocation the caller reported as out of memory) is cleared first;
+    // device faults stay set and are still reported.
+    cudaGetLastError();
+    kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
     if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess)
         ::gp::fail(GP_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));
     if (timed) g_profiler->after(stream);
