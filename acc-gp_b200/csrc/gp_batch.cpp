@@ -145,6 +145,7 @@ struct gp_server {
         while (true) {
             uint64_t ticket = 0;
             Job job;
+            Graph g;  // copied under the lock: gp_server_add_graph may grow `graphs` meanwhile
             {
                 std::unique_lock<std::mutex> lock(mu);
                 work_cv.wait(lock, [&] { return (stopping && queue.empty()) || admissible() >= 0; });
@@ -153,6 +154,7 @@ struct gp_server {
                 ticket = queue[static_cast<size_t>(at)];
                 queue.erase(queue.begin() + at);
                 job = jobs.at(ticket);
+                if (job.graph >= 0) g = graphs[static_cast<size_t>(job.graph)];
                 in_use += job.bytes;
             }
             gp_request& r = *job.request;
@@ -161,7 +163,6 @@ struct gp_server {
             if (job.graph < 0) {
                 r.status = gp_partition(c, &r.graph, r.k, r.epsilon, r.seed, r.flags, r.labels_out, &r.stats);
             } else {
-                const Graph& g = graphs[static_cast<size_t>(job.graph)];
                 r.status = GP_OK;
                 if (labels_cap < static_cast<size_t>(g.n)) {
                     cudaSetDevice(device);
