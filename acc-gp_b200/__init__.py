@@ -35,6 +35,7 @@ FLAG_KEEP_HIERARCHY = 0x2
 FLAG_NO_SEED_MATCHING = 0x4
 FLAG_QUIET = 0x8
 FLAG_COARSEN_ONLY = 0x10
+FLAG_REQUIRE_BALANCED = 0x20
 
 
 class GpartError(RuntimeError):
@@ -60,6 +61,17 @@ class _Stats(_C.Structure):
                 ("uncoarsen_seconds", _C.c_double), ("algorithm_seconds", _C.c_double),
                 ("h2d_seconds", _C.c_double), ("d2h_seconds", _C.c_double),
                 ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64)]
+
+
+class _RefineStats(_C.Structure):
+    _fields_ = [("rounds", _C.c_int32), ("admission_iterations", _C.c_int32),
+                ("checkpoint_updates", _C.c_int32), ("reserved", _C.c_int32),
+                ("proposals", _C.c_uint64), ("accepted", _C.c_uint64), ("initial_cut", _C.c_uint64),
+                ("final_cut", _C.c_uint64), ("final_max_part_weight", _C.c_uint64), ("capacity", _C.c_uint64),
+                ("lp_cut_gain", _C.c_uint64), ("lp_cut_loss", _C.c_uint64),
+                ("rebalance_cut_gain", _C.c_uint64), ("rebalance_cut_loss", _C.c_uint64),
+                ("group_cut_gain", _C.c_uint64), ("group_accepted", _C.c_uint64),
+                ("seconds", _C.c_double), ("kernel_launches", _C.c_uint64)]
 
 
 class _Level(_C.Structure):
@@ -327,6 +339,20 @@ class Context:
                                       _C.c_uint32(seed), _C.c_uint32(flags), _ptr(labels), _C.byref(stats)))
         return labels, Stats._from(stats)
 
+    def refine(self, graph: Graph, labels, k: int, epsilon: float = 1.03, max_rounds: int = 32,
+               exchange_rounds: int = 2, flags: int = FLAG_QUIET):
+        """gp_refine (the reference's refine_partition): one level of refinement
+        of `labels` on `graph`; returns (refined labels, dict of RefineStats)."""
+        out = _np.array(labels, dtype=_np.int32, copy=True)
+        if out.shape != (graph.n,):
+            raise GpartError(1, "refinement partition has the wrong length")
+        stats = _RefineStats()
+        g = graph.as_c()
+        _check(self._lib.gp_refine(self._handle, _C.byref(g), _C.c_int32(k), _C.c_double(epsilon),
+                                   _C.c_int32(max_rounds), _C.c_int32(exchange_rounds), _C.c_uint32(flags),
+                                   _ptr(out), _C.byref(stats)))
+        return out, {name: getattr(stats, name) for name, _ in _RefineStats._fields_ if name != "reserved"}
+
     def load_csr_int64(self, indptr_path: str, indices_path: str) -> tuple[int, int]:
         """gp_load_csr_int64: the reference's int64 files streamed into device memory; returns (n, m)."""
         n, m = _C.c_int64(), _C.c_int64()
@@ -453,7 +479,7 @@ def evaluate_device_static(offsets_ptr: int, neighbors_ptr: int, n: int, m: int,
 
     For callers that must not let the library allocate device memory (a
     framework allocator that owns the memory budget, an allocation-free
-    serving loop).  Scratch is a fixed 611 KB device array shared by all
+    serving loop).  Scratch is a fixed 616 KB device array shared by all
     calls on a device; overlapping calls race, k must be <= 128, and the
     first call on a device should precede any stream capture.  Does not wait
     for the results.

@@ -169,6 +169,8 @@ struct gp_server {
                     if (labels_dev) cudaFree(labels_dev);
                     labels_dev = nullptr;
                     if (cudaMalloc(&labels_dev, sizeof(int32_t) * static_cast<size_t>(g.n)) != cudaSuccess) {
+                        cudaGetLastError();  // handled: this request reports GP_OUT_OF_MEMORY
+                        labels_dev = nullptr;
                         labels_cap = 0;
                         r.status = GP_OUT_OF_MEMORY;
                     } else {
@@ -232,7 +234,11 @@ extern "C" gp_status gp_server_add_graph(gp_server* server, const gp_csr* graph,
     cudaSetDevice(server->device);
     auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
         if (!src) return true;
-        if (cudaMalloc(dst, bytes ? bytes : 4) != cudaSuccess) return false;
+        if (cudaMalloc(dst, bytes ? bytes : 4) != cudaSuccess) {
+            cudaGetLastError();  // handled: gp_server_add_graph reports it
+            *dst = nullptr;
+            return false;
+        }
         return !bytes || cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
     };
     const bool ok = upload(reinterpret_cast<void**>(&g.off), graph->offsets, sizeof(int32_t) * (g.n + 1)) &&
@@ -280,14 +286,21 @@ extern "C" gp_status gp_server_wait(gp_server* server, uint64_t ticket, double t
     std::unique_lock<std::mutex> lock(server->mu);
     auto it = server->jobs.find(ticket);
     if (it == server->jobs.end()) { set_error("unknown ticket"); return GP_INVALID_ARGUMENT; }
-    auto finished = [&] { return server->jobs.at(ticket).done; };
+    // Another thread waiting on the same ticket may erase it first.
+    auto finished = [&] {
+        auto j = server->jobs.find(ticket);
+        return j == server->jobs.end() || j->second.done;
+    };
     if (timeout_seconds < 0) {
         server->done_cv.wait(lock, finished);
     } else if (!server->done_cv.wait_for(lock, std::chrono::duration<double>(timeout_seconds), finished)) {
         set_error("request still running");
         return GP_DEVICE_TIMEOUT;
     }
-    server->jobs.erase(ticket);
+    if (server->jobs.erase(ticket) == 0) {
+        set_error("unknown ticket (another wait already collected it)");
+        return GP_INVALID_ARGUMENT;
+    }
     return GP_OK;
 }
 

@@ -24,12 +24,18 @@ struct Failure : std::runtime_error {
 };
 [[noreturn]] inline void fail(gp_status s, const std::string& m) { throw Failure(s, m); }
 
+// A failed runtime call becomes a gp_status.  The failure is handled here,
+// so its error is also taken off the thread's last-error slot (a no-op for
+// sticky device faults, which stay set): a later launch check must not
+// report it again.
 #define GP_CUDA(call)                                                                          \
     do {                                                                                       \
         const cudaError_t gp_err__ = (call);                                                   \
-        if (gp_err__ != cudaSuccess)                                                           \
+        if (gp_err__ != cudaSuccess) {                                                         \
+            cudaGetLastError();                                                                \
             ::gp::fail(gp_err__ == cudaErrorMemoryAllocation ? GP_OUT_OF_MEMORY : GP_CUDA_ERROR, \
                        std::string(#call) + ": " + cudaGetErrorString(gp_err__));             \
+        }                                                                                      \
     } while (0)
 
 // Number of kernels this library launched; every launch goes through launch().
@@ -76,10 +82,9 @@ inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem
     if (timed) g_profiler->before(stream);
     // A launch that did not start (bad configuration, missing shared-memory
     // opt-in) must fail the call, not leave its results silently unwritten.
-    // The error left by an earlier call whose failure was already handled (an
-    // allocation the caller reported as out of memory) is cleared first;
-    // device faults stay set and are still reported.
-    cudaGetLastError();
+    // This library clears the error of every failure it has handled where it
+    // handles it (GP_CUDA, the server's own allocations), so what is pending
+    // here belongs to this launch or to an unhandled fault.
     kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
     if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess)
         ::gp::fail(GP_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));

@@ -124,10 +124,30 @@ struct RefineOutcome {
     u64 max_load = 0;
     int levels_refined = 0;
 };
+// Round budgets of one level's refinement (RefineOptions::max_rounds and
+// exchange_rounds, include/refine.hpp:13-26; the pipeline uses 32 and 2).
+struct RefineBudget {
+    int rounds = 32;
+    int exchange_rounds = 2;
+};
+// What one level's refinement did (the RefineStats fields of
+// include/refine.hpp:28-53 that describe the moves, not the layout).
+struct LevelStats {
+    int rounds = 0, admission_iterations = 0, checkpoint_updates = 0;
+    bool repair_failed = false;
+    u64 proposals = 0, accepted = 0, initial_cut = 0, final_cut = 0, final_max_load = 0;
+    u64 lp_gain = 0, lp_loss = 0, rebalance_gain = 0, rebalance_loss = 0, group_gain = 0, group_accepted = 0;
+};
 // Refines from the coarsest level down to level 0 (refine_hierarchy_impl,
 // src/refine.cu:483-730); `labels` (device, level-0 sized) receives the result.
 RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coarse_labels, int k, double eps,
                         int* labels, bool log, bool verify, const Mapping& mapping);
+
+// Refines one graph from `labels` (device, n entries, values in [0,k)) in
+// place: refine_partition (src/refine.cu:470-481) on a device-resident graph
+// whose metadata coarsen() has filled.  The part loads are measured first.
+LevelStats refine_single(Context& ctx, const DGraph& g, int* labels, int k, double eps, const RefineBudget& budget,
+                         bool log, bool verify, const Mapping& mapping);
 
 // Device edge cut of labels (directed sum / 2); throws on an odd sum.
 u64 device_cut(Context& ctx, const DGraph& g, const int* labels);

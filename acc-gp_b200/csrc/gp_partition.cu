@@ -198,11 +198,16 @@ u64 algorithmic_bytes(const Hierarchy& h) {
     return bytes;
 }
 
-gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, double eps, uint32_t seed,
-              uint32_t flags, int* labels_out, void* user_stream, gp_stats* stats) {
-    Context& ctx = handle->ctx;
-    if (!in || !labels_out) fail(GP_INVALID_ARGUMENT, "graph and labels must not be NULL");
-    if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(GP_INVALID_ARGUMENT, "invalid partition capacity options");
+// The input graph on the device: host arrays copied into the persist arena
+// (or caller device arrays used in place), unit vertex weights materialised,
+// then the shape checks of validate_weighted_shape (src/graph.cpp:118-155)
+// on the device, which also give the total vertex weight and the directed
+// edge-weight sum.  Records ev[0] (before the copies) and ev[1] (after).
+struct Input {
+    DGraph g;
+    u64 total = 0, directed = 0;
+};
+Input prepare_input(Context& ctx, const gp_csr* in, bool device_input) {
     if (in->n <= 0) fail(GP_INVALID_ARGUMENT, "empty CSR indptr");
     if (in->n > std::numeric_limits<int>::max() || in->m > std::numeric_limits<int>::max() || in->m < 0)
         fail(GP_INVALID_ARGUMENT, "graph exceeds supported 32-bit CSR limits; dataset excluded");
@@ -213,18 +218,10 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
         if (!in->offsets || (in->m > 0 && !in->neighbors)) fail(GP_INVALID_ARGUMENT, "graph arrays must not be NULL");
         if (in->offsets[0] != 0 || in->offsets[in->n] != in->m) fail(GP_INVALID_ARGUMENT, "invalid weighted CSR shape");
     }
-    GP_CUDA(cudaSetDevice(ctx.device));
     cudaStream_t s = ctx.stream;
-    cudaStream_t caller = static_cast<cudaStream_t>(user_stream);
-    if (caller) {  // order after the caller's producers
-        GP_CUDA(cudaEventRecord(ctx.ev[7], caller));
-        GP_CUDA(cudaStreamWaitEvent(s, ctx.ev[7], 0));
-    }
-    const u64 launches0 = g_launches;
-    ctx.persist.release({0, 0});
-    ctx.scratch.release({0, 0});
     const i64 n = in->n, m = in->m;
-    DGraph g;
+    Input out;
+    DGraph& g = out.g;
     g.n = n;
     g.m = m;
     GP_CUDA(cudaEventRecord(ctx.ev[0], s));
@@ -253,8 +250,6 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     }
     g.implicit_unit = g.ew == nullptr;
     GP_CUDA(cudaEventRecord(ctx.ev[1], s));
-    // Device-side validation: it also yields the total weight and the
-    // directed edge-weight sum the reference checks at the end.
     ctx.clear_scalars(5);
     launch(k_validate_vertices, std::min(blocks_for(n, 256), 148 * 16), 256, 0, s, n, m, g.off, g.vw, ctx.dev_scalars);
     launch(k_validate_edges, std::min(blocks_for(m, 256), 148 * 16), 256, 0, s, n, m, g.nbr, g.ew, ctx.dev_scalars);
@@ -262,7 +257,31 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     if (vs[0]) fail(GP_INVALID_ARGUMENT, "weighted CSR offsets are not monotone");
     if (vs[1]) fail(GP_INVALID_ARGUMENT, "weighted CSR contains an invalid neighbor");
     if (vs[2]) fail(GP_INVALID_ARGUMENT, "vertex weights must be positive");
-    const u64 total = vs[3], directed = vs[4];
+    out.total = vs[3];
+    out.directed = vs[4];
+    return out;
+}
+
+gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, double eps, uint32_t seed,
+              uint32_t flags, int* labels_out, void* user_stream, gp_stats* stats) {
+    Context& ctx = handle->ctx;
+    if (!in || !labels_out) fail(GP_INVALID_ARGUMENT, "graph and labels must not be NULL");
+    if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(GP_INVALID_ARGUMENT, "invalid partition capacity options");
+    if (in->n <= 0) fail(GP_INVALID_ARGUMENT, "empty CSR indptr");
+    GP_CUDA(cudaSetDevice(ctx.device));
+    cudaStream_t s = ctx.stream;
+    cudaStream_t caller = static_cast<cudaStream_t>(user_stream);
+    if (caller) {  // order after the caller's producers
+        GP_CUDA(cudaEventRecord(ctx.ev[7], caller));
+        GP_CUDA(cudaStreamWaitEvent(s, ctx.ev[7], 0));
+    }
+    const u64 launches0 = g_launches;
+    ctx.persist.release({0, 0});
+    ctx.scratch.release({0, 0});
+    const i64 n = in->n;
+    Input input = prepare_input(ctx, in, device_input);
+    DGraph& g = input.g;
+    const u64 total = input.total, directed = input.directed;
     uint64_t capacity = 0;
     if (gp_status st = capacity_of(total, k, eps, &capacity); st != GP_OK) fail(st, last_error());
 
@@ -333,6 +352,77 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
         stats->d2h_seconds = device_input ? 0.0 : elapsed(ctx.ev[4], ctx.ev[5]) * 1e-3;
         stats->kernel_launches = g_launches - launches0;
         stats->algorithmic_bytes = algorithmic_bytes(h);
+    }
+    return GP_OK;
+}
+
+// refine_partition (src/refine.cu:470-481, include/refine.hpp:84-88): one
+// graph refined from the caller's labels with the pipeline's refinement and
+// the caller's round budgets.
+gp_status run_refine(gp_context* handle, const gp_csr* in, int k, double eps, int rounds, int exchange_rounds,
+                     uint32_t flags, int* labels, gp_refine_stats* out) {
+    Context& ctx = handle->ctx;
+    if (!in || !labels) fail(GP_INVALID_ARGUMENT, "graph and labels must not be NULL");
+    if (k < 2 || k > kMaxParts || rounds < 0 || rounds > 64 || exchange_rounds < 0 || exchange_rounds > 8 ||
+        !std::isfinite(eps) || eps < 1.0 || in->n <= 0)
+        fail(GP_INVALID_ARGUMENT, "invalid refinement options");
+    for (i64 v = 0; v < in->n; ++v)
+        if (labels[v] < 0 || labels[v] >= k) fail(GP_INVALID_ARGUMENT, "refinement partition has an invalid part id");
+    GP_CUDA(cudaSetDevice(ctx.device));
+    cudaStream_t s = ctx.stream;
+    const u64 launches0 = g_launches;
+    ctx.persist.release({0, 0});
+    ctx.scratch.release({0, 0});
+    Input input = prepare_input(ctx, in, false);
+    uint64_t capacity = 0;
+    if (gp_status st = capacity_of(input.total, k, eps, &capacity); st != GP_OK) fail(st, last_error());
+    if (flags & GP_FLAG_REQUIRE_BALANCED) {  // allow_initial_imbalance = false
+        std::vector<u64> loads(static_cast<size_t>(k), 0);
+        for (i64 v = 0; v < in->n; ++v) loads[labels[v]] += in->vertex_weights ? in->vertex_weights[v] : 1u;
+        if (*std::max_element(loads.begin(), loads.end()) > capacity)
+            fail(GP_INVALID_ARGUMENT, "initial refinement partition is imbalanced");
+    }
+    CoarsenOptions o;  // metadata of the input level only (no coarsening)
+    o.parts = k;
+    o.max_levels = 0;
+    o.log = false;
+    o.verify = (flags & GP_FLAG_VERIFY) != 0;
+    o.mapping = handle->mapping;
+    if (o.verify) verify_csr(ctx, input.g, true, GP_INVALID_ARGUMENT);
+    Hierarchy h = coarsen(ctx, input.g, o);
+    int* dev_labels = ctx.persist.alloc<int>(in->n);
+    GP_CUDA(cudaMemcpyAsync(dev_labels, labels, sizeof(int) * in->n, cudaMemcpyHostToDevice, s));
+    RefineBudget budget;
+    budget.rounds = rounds;
+    budget.exchange_rounds = exchange_rounds;
+    GP_CUDA(cudaEventRecord(ctx.ev[2], s));
+    const LevelStats st = refine_single(ctx, h.levels[0], dev_labels, k, eps, budget, !(flags & GP_FLAG_QUIET),
+                                        o.verify, handle->mapping);
+    GP_CUDA(cudaEventRecord(ctx.ev[3], s));
+    if (st.repair_failed) fail(GP_CAPACITY_INFEASIBLE, "initial refinement capacity repair failed");
+    if (o.verify && device_cut(ctx, h.levels[0], dev_labels) != st.final_cut)
+        fail(GP_INTERNAL, "final cut differs from CSR scan");
+    GP_CUDA(cudaMemcpyAsync(labels, dev_labels, sizeof(int) * in->n, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->rounds = st.rounds;
+        out->admission_iterations = st.admission_iterations;
+        out->checkpoint_updates = st.checkpoint_updates;
+        out->proposals = st.proposals;
+        out->accepted = st.accepted;
+        out->initial_cut = st.initial_cut;
+        out->final_cut = st.final_cut;
+        out->final_max_part_weight = st.final_max_load;
+        out->capacity = capacity;
+        out->lp_cut_gain = st.lp_gain;
+        out->lp_cut_loss = st.lp_loss;
+        out->rebalance_cut_gain = st.rebalance_gain;
+        out->rebalance_cut_loss = st.rebalance_loss;
+        out->group_cut_gain = st.group_gain;
+        out->group_accepted = st.group_accepted;
+        out->seconds = elapsed(ctx.ev[2], ctx.ev[3]) * 1e-3;
+        out->kernel_launches = g_launches - launches0;
     }
     return GP_OK;
 }
@@ -426,6 +516,12 @@ gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k, d
                               uint32_t flags, int32_t* labels_out_device, void* stream, gp_stats* stats) {
     if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
     return guarded([&] { return run(ctx, graph, true, k, epsilon, seed, flags, labels_out_device, stream, stats); });
+}
+
+gp_status gp_refine(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon, int32_t max_rounds,
+                    int32_t exchange_rounds, uint32_t flags, int32_t* labels, gp_refine_stats* stats) {
+    if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
+    return guarded([&] { return run_refine(ctx, graph, k, epsilon, max_rounds, exchange_rounds, flags, labels, stats); });
 }
 
 // load_weighted_graph + make_device_weighted (src/graph.cpp:47-116,205-218)
@@ -626,6 +722,10 @@ gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
     else if (key == "build_short" && value >= 8 && value <= 2048) ctx->mapping.build_short = static_cast<int>(value);
     else if (key == "rebuild_divisor" && value >= 1 && value <= 100000) ctx->mapping.rebuild_divisor = static_cast<int>(value);
     else if (key == "on_demand_degree" && value >= 0 && value <= 32) ctx->mapping.on_demand_degree = static_cast<int>(value);
+    else if (key == "arena_chunk_mb" && value >= 1 && value <= (int64_t{1} << 24)) {
+        ctx->ctx.persist.set_chunk_bytes(static_cast<size_t>(value) << 20);
+        ctx->ctx.scratch.set_chunk_bytes(static_cast<size_t>(value) << 20);
+    }
     else { set_error("unknown option or value out of range: " + key); return GP_INVALID_ARGUMENT; }
     return GP_OK;
 }

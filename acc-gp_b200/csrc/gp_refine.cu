@@ -2132,11 +2132,12 @@ template <class T>
 class LevelRefiner {
 public:
     LevelRefiner(Context& c, const DGraph& g, int k, double eps, int* labels, u64* loads, u64 total, bool log,
-                 bool verify, const Mapping& mapping)
+                 bool verify, const Mapping& mapping, const RefineBudget& budget = RefineBudget{})
         : ctx(c), g(g), k(k), eps(eps), labels(labels), loads(loads), total(total), log(log), verify(verify),
-          mapping(mapping) {}
+          mapping(mapping), budget(budget) {}
 
     LevelResult run(bool has_known, u64 known);
+    LevelStats stats;
 
 private:
     Context& ctx;
@@ -2149,6 +2150,7 @@ private:
     bool log;
     bool verify;
     const Mapping& mapping;
+    RefineBudget budget;
     T* check_A = nullptr;       // verify: independent rebuild of the cache
     T* check_totals = nullptr;
 
@@ -2370,7 +2372,11 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     const i64 count = static_cast<i64>(ctx.host_scalars[1]);
     const long long delta = settled_delta(ctx.host_scalars + 2);
     max_load_host = ctx.host_scalars[3];
+    stats.proposals += static_cast<u64>(count);
     if (count) {
+        stats.accepted += static_cast<u64>(count);
+        if (delta >= 0) stats.lp_gain += static_cast<u64>(delta);
+        else stats.lp_loss += static_cast<u64>(-delta);
         account(delta);
         ++revision;
         check_state("incremental cut differs from CSR scan");
@@ -2523,6 +2529,9 @@ bool LevelRefiner<T>::repair() {
                     GP_CUDA(cudaStreamSynchronize(s()));
                     delta = settled_delta(ctx.host_scalars);
                     max_load_host = ctx.host_scalars[1];
+                    stats.accepted += static_cast<u64>(placed);
+                    if (delta >= 0) stats.rebalance_gain += static_cast<u64>(delta);
+                    else stats.rebalance_loss += static_cast<u64>(-delta);
                     account(delta);
                     ++revision;
                     check_state("GPU rebalance cut mismatch");
@@ -2533,6 +2542,7 @@ bool LevelRefiner<T>::repair() {
             launch(k_reset_targets, blocks_for(dcount, kThreads), kThreads, 0, s(), dcount,
                    static_cast<const u32*>(donors), targets);
         ++iterations;
+        ++stats.admission_iterations;
         const bool feasible = max_load_host <= C;
         if (feasible || placed == 0 || iterations >= 2 * k + 4) return feasible;
     }
@@ -2590,7 +2600,7 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
                static_cast<const JointMove*>(in), out);
     };
     int empty = 0;
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < budget.exchange_rounds; ++pass) {
         const size_t match_smem = sizeof(double) * k * k;
         // One value for every k: the limit belongs to the kernel for the whole
         // process, and concurrent worker contexts must not lower it under
@@ -2654,6 +2664,8 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         ++revision;
         check_state("incremental cut differs from CSR scan");
         if (delta <= 0) fail(GP_INTERNAL, "non-improving boundary group batch");
+        stats.group_gain += static_cast<u64>(delta);
+        stats.group_accepted += static_cast<u64>(count);
         if (max_load_host > C || cut >= best_cut) fail(GP_INTERNAL, "capacity exchange violated cut/capacity");
         best_cut = cut;
     }
@@ -2744,10 +2756,14 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
         cut = ctx.host_scalars[4] / 2;
     }
     LevelResult res;
+    stats.initial_cut = cut;
     if (max_load_host > C) {
         if (!repair()) {
             res.cut = cut;
             res.repair_failed = true;
+            stats.repair_failed = true;
+            stats.final_cut = cut;
+            stats.final_max_load = max_load_host;
             return res;
         }
     }
@@ -2784,7 +2800,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
         filter = ctx.read_scalars(1)[0] <= 1 ? 0.25 : 0.75;
     }
     int stale = 0, empty = 0, rounds = 0;
-    for (int phase = 0; phase < 32 && stale < 3; ++phase) {
+    for (int phase = 0; phase < budget.rounds && stale < 3; ++phase) {
         ++rounds;
         if (samples) GP_CUDA(cudaMemsetAsync(samples, 0, sizeof(Sample) * k, s()));
         const i64 count = lp_round(filter);
@@ -2799,6 +2815,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
             GP_CUDA(cudaMemcpyAsync(saved_labels, labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
             GP_CUDA(cudaMemcpyAsync(saved_loads, loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
             best_revision = revision;
+            ++stats.checkpoint_updates;
         }
     }
     const bool restored = revision != best_revision;
@@ -2813,7 +2830,7 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
         max_load_host = ctx.host_scalars[0];
     }
     cut = best;
-    if (n <= 65536) {
+    if (budget.rounds > 0 && budget.exchange_rounds > 0 && n <= 65536) {
         if (restored) build();
         exchange(best);
     }
@@ -2824,6 +2841,9 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
                     static_cast<unsigned long long>(feasible_start), static_cast<unsigned long long>(cut), rounds,
                     static_cast<long long>(repair_iterations), static_cast<long long>(repair_donors),
                     static_cast<unsigned long long>(g.maximum_degree), on_demand ? "on_demand" : "dense");
+    stats.rounds = rounds;
+    stats.final_cut = cut;
+    stats.final_max_load = max_load_host;
     res.cut = cut;
     res.refined = true;
     return res;
@@ -2922,6 +2942,29 @@ RefineOutcome uncoarsen(Context& ctx, Hierarchy& h, const std::vector<int>& coar
     out.cut = last_cut;
     out.max_load = maxload;
     return out;
+}
+
+// refine_partition (src/refine.cu:470-481): one graph, its labels measured,
+// one run_incremental_refinement with the caller's round budgets.
+LevelStats refine_single(Context& ctx, const DGraph& g, int* labels, int k, double eps, const RefineBudget& budget,
+                         bool log, bool verify, const Mapping& mapping) {
+    cudaStream_t s = ctx.stream;
+    u64* loads = ctx.persist.alloc<u64>(k);
+    GP_CUDA(cudaMemsetAsync(loads, 0, sizeof(u64) * k, s));
+    launch(k_loads, std::min(blocks_for(g.n, 256), 148 * 4), 256, sizeof(u64) * k, s, g.n, k,
+           static_cast<const int*>(labels), g.vw, loads);
+    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, loads, sizeof(u64) * k, cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    u64 total = 0;
+    for (int p = 0; p < k; ++p) total += ctx.host_scalars[p];
+    if (g.incident_bound <= 0xffffffffULL) {
+        LevelRefiner<u32> r(ctx, g, k, eps, labels, loads, total, log, verify, mapping, budget);
+        r.run(false, 0);
+        return r.stats;
+    }
+    LevelRefiner<u64> r(ctx, g, k, eps, labels, loads, total, log, verify, mapping, budget);
+    r.run(false, 0);
+    return r.stats;
 }
 
 }  // namespace gp

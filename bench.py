@@ -14,9 +14,10 @@ graph in pinned host memory (host->device copy and label read-back inside the
 timed region).  Multi-GPU runs are independent replicas (one graph per rank,
 no collective on the data path): weak scaling.
 
---impl reference times the reference partitioner's own build
-(oracle/_ref/gpart_partition_standard, compiled for sm_100a from its unmodified
-sources) on the same graph, metric and config.
+--impl reference times the reference partitioner's own build, warm, in one
+process (oracle/_ref/gpart_ref_bench: the reference's unmodified objects
+compiled for sm_100a, driven through its public API) on the same graph,
+metric and config; that process loads none of this repository's libraries.
 """
 from __future__ import annotations
 
@@ -122,21 +123,53 @@ class ClockSampler:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def cpu_baseline(gp, seconds_budget=30.0):
-    """The serial CPU restatement (oracle/) on a bounded sample: R-MAT scale 19
-    with the workload's generator parameters and k; graphs/s is scaled to the
-    full workload by directed entries (linear in edges)."""
+def cpu_baseline(gp, full_m, scale=20):
+    """The serial CPU restatement (oracle/) on a bounded sample: R-MAT scale
+    20 with the workload's generator parameters and k (about 15 s on one
+    core); graphs/s is scaled to the full workload by directed entries (the
+    V-cycle's work is linear in them)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # noqa: E402  (test infrastructure; CPU baseline leg only)
-    sample = gp.rmat(19, 16, 0.57, 0.19, 0.19, 0)
+    sample = gp.rmat(scale, 16, 0.57, 0.19, 0.19, 0)
     t = time.perf_counter()
     oracle.partition(sample, WORKLOAD["k"], WORKLOAD["epsilon"], WORKLOAD["seed"])
     seconds = time.perf_counter() - t
-    full_m = 125_000_000  # directed entries of the R-MAT scale-22 workload (approximate)
     value = (1.0 / seconds) * (sample.m / full_m)
     return {"value": value, "unit": "graphs/s", "cores": 1, "kind": "port",
-            "sample": f"R-MAT scale 19 (n={sample.n}, m={sample.m}) k=64 in {seconds:.2f}s on 1 core; "
-                      f"graphs/s scaled to the scale-22 workload by directed entries"}
+            "sample": f"R-MAT scale {scale} (n={sample.n}, m={sample.m}) k=64 in {seconds:.2f}s on 1 core; "
+                      f"graphs/s scaled to the scale-22 workload (m={full_m}) by directed entries"}
+
+
+def cpu_parts(gp, g, labels, metis_seconds):
+    """The reference's own CPU code on the workload, on the box's host cores:
+    its METIS step (the same METIS library call; our line's initial stage) and
+    its verifier tools/verify_csr.cpp (oracle/_ref/gpart_verify_csr, OpenMP,
+    all cores) on the full graph and the labels just produced."""
+    import platform
+    out = {"host_cores": os.cpu_count(), "cpu_model": platform.processor() or None,
+           "metis_step_ms": metis_seconds * 1e3}
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    out["cpu_model"] = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    verifier = os.path.join(ROOT, "oracle", "_ref", "gpart_verify_csr")
+    if os.path.exists(verifier):
+        with tempfile.TemporaryDirectory() as tmp:
+            ip, ix, part = (os.path.join(tmp, x) for x in ("g.indptr", "g.indices", "g.part"))
+            gp.write_csr_int64(g, ip, ix)
+            labels.astype("int32").tofile(part)
+            env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+            t = time.perf_counter()
+            r = subprocess.run([verifier, ip, ix, str(WORKLOAD["k"]), part, "binary"], capture_output=True,
+                               text=True, env=env)
+            out["reference_verifier_ms"] = (time.perf_counter() - t) * 1e3
+            out["reference_verifier_threads"] = os.cpu_count()
+            out["reference_verifier_ok"] = r.returncode == 0
+    return out
 
 
 def run_ours(args):
@@ -232,7 +265,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism=f"replicas{world}", l2="inputs larger than L2 (0.52 GB CSR)"),
+        "config": config_for(world),
         "partition_ms": elapsed / args.steps * 1e3, "cut": int(stats[-1].edge_cut),
         "verifier": {"cut": verdict["cut"], "max_load": verdict["max_load"], "capacity": verdict["capacity"],
                      "capacity_ok": verdict["capacity_ok"]},
@@ -245,7 +278,8 @@ def run_ours(args):
         "gpu_launches": launches, "roofline": roof, "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(gp)
+        line["cpu_baseline"] = cpu_baseline(gp, m)
+        line["cpu_parts"] = cpu_parts(gp, g, labels, stats[-1].initial_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -267,54 +301,81 @@ def traffic_ratio():
     return None
 
 
+def config_for(world):
+    """The `config` object of both arms' lines (identical, so the two lines
+    describe one workload)."""
+    return dict(WORKLOAD, parallelism=f"replicas{world}", l2="inputs larger than L2 (0.52 GB CSR)")
+
+
 def run_reference(args):
+    """The reference's own build of this path, timed warm in one process.
+
+    The reference implements the partitioner in CUDA only (its CPU parts are
+    the METIS step and the verifier), so its arm is its sm_100a build:
+    oracle/_ref/gpart_ref_bench links the reference's unmodified objects,
+    generates the same seeded R-MAT graph in-process (a test checks it equals
+    the library's generator byte for byte), and runs the reference's public
+    pipeline exactly as app/partition_main.cu does, `warmup` + `steps` times.
+    `value` is steps / summed algorithm_total_seconds (the CLI's timing scope:
+    input resident to labels resident); `e2e` adds each step's own
+    input_prepare_seconds (host validation + upload) and label download.
+    This process loads none of the repository's libraries.  One cold run of
+    the reference CLI on the same graph is reported beside it."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     if rank != 0:
         return
-    binary = os.path.join(ROOT, "oracle", "_ref", "gpart_partition_standard")
-    if not os.path.exists(binary):
+    harness = os.path.join(ROOT, "oracle", "_ref", "gpart_ref_bench")
+    cli = os.path.join(ROOT, "oracle", "_ref", "gpart_partition_standard")
+    if not os.path.exists(harness):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
         return
-    gp = load_package()
-    g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
-    times, cuts, e2e_times = [], [], []
-    with tempfile.TemporaryDirectory() as tmp:
-        ip, ix, part = os.path.join(tmp, "g.indptr"), os.path.join(tmp, "g.indices"), os.path.join(tmp, "g.part")
-        gp.write_csr_int64(g, ip, ix)
-        walls = []
-        for i in range(args.warmup + args.steps):
-            w0 = time.perf_counter()
-            proc = subprocess.run([binary, ip, ix, str(WORKLOAD["k"]), part, repr(WORKLOAD["epsilon"]),
-                                   str(WORKLOAD["seed"])], capture_output=True, text=True)
-            w1 = time.perf_counter()
-            if proc.returncode != 0:
-                print(json.dumps({"impl": "reference", "unavailable": "reference run failed: " +
-                                  proc.stderr.strip()[-200:]}))
-                return
-            if i >= args.warmup:
-                field = lambda key: float(re.search(key + r"=([0-9.eE+-]+)", proc.stdout).group(1))
-                times.append(field("algorithm_total_seconds"))
-                # Through the host-buffer path: validation + upload, the
-                # algorithm, and the label download (the same span as our e2e).
-                e2e_times.append(field("input_prepare_seconds") + field("algorithm_total_seconds") +
-                                 field("final_partition_d2h_seconds"))
-                cuts.append(int(re.search(r"final_edge_cut=(\d+)", proc.stdout).group(1)))
-                walls.append(w1 - w0)
-    elapsed = sum(times)
-    value = len(times) / elapsed
+    gen = ["22", "16", "0.57", "0.19", "0.19", "0"]
+    clocks = ClockSampler()
+    clocks.start()
+    proc = subprocess.run([harness, "rmat", *gen, str(WORKLOAD["k"]), repr(WORKLOAD["epsilon"]),
+                           str(WORKLOAD["seed"]), str(args.warmup), str(args.steps)], capture_output=True, text=True)
+    clk = clocks.stop(0)
+    if proc.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "reference run failed: " + proc.stderr.strip()[-200:]}))
+        return
+    found = [line for line in proc.stdout.splitlines() if line.startswith("REF_BENCH_JSON ")]
+    res = json.loads(found[-1][len("REF_BENCH_JSON "):])
+    algo = res["algorithm_total_seconds"]
+    e2e = [a + b + c for a, b, c in zip(res["input_prepare_seconds"], algo, res["final_partition_d2h_seconds"])]
+    value = len(algo) / sum(algo)
+    n, m = res["vertices"], res["edges"]
+    cold = None
+    if not args.no_cold_cli and os.path.exists(cli):
+        with tempfile.TemporaryDirectory() as tmp:
+            ip, ix, part = (os.path.join(tmp, x) for x in ("g.indptr", "g.indices", "g.part"))
+            w = subprocess.run([harness, "write-rmat", *gen, ip, ix], capture_output=True, text=True)
+            if w.returncode == 0:
+                w0 = time.perf_counter()
+                c = subprocess.run([cli, ip, ix, str(WORKLOAD["k"]), part, repr(WORKLOAD["epsilon"]),
+                                    str(WORKLOAD["seed"])], capture_output=True, text=True)
+                wall = time.perf_counter() - w0
+                if c.returncode == 0:
+                    field = lambda key: float(re.search(key + r"=([0-9.eE+-]+)", c.stdout).group(1))
+                    cold = {"process_wall_s": wall, "algorithm_total_seconds": field("algorithm_total_seconds"),
+                            "input_prepare_seconds": field("input_prepare_seconds"),
+                            "wall_total_seconds": field("wall_total_seconds"),
+                            "final_edge_cut": int(re.search(r"final_edge_cut=(\d+)", c.stdout).group(1))}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "graphs/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / len(times) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(algo) / len(algo) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism="replicas1"), "cut": cuts[-1],
-        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": os.cpu_count(), "kind": "reference",
-                         "sample": "full workload through the reference's own build (app/partition_main.cu compiled "
-                                   "for sm_100a from its sources), one process per step, its algorithm_total_seconds"},
-        "e2e": {"value": len(e2e_times) / sum(e2e_times), "unit": "graphs/s",
-                "h2d_bytes_per_step": 4 * (g.n + 1) + 4 * g.m, "d2h_bytes_per_step": 4 * g.n,
-                "ms_per_step": sum(e2e_times) / len(e2e_times) * 1e3,
-                "scope": "input_prepare_seconds + algorithm_total_seconds + final_partition_d2h_seconds"},
-        "process_wall_s_per_step": sum(walls) / len(walls),
+        "config": config_for(world), "cut": res["final_cut"],
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": 1, "kind": "reference",
+                         "sample": "the reference implements this path only in CUDA: this is its own sm_100a build "
+                                   "(unmodified objects, public coarsen / initial_partition_metis / uncoarsen API) "
+                                   "driven by one host thread, full workload, warm, one process; its CPU parts "
+                                   "(METIS, verifier) are timed in our line's cpu_parts"},
+        "e2e": {"value": len(e2e) / sum(e2e), "unit": "graphs/s", "h2d_bytes_per_step": 4 * (n + 1) + 4 * m,
+                "d2h_bytes_per_step": 4 * n, "ms_per_step": sum(e2e) / len(e2e) * 1e3,
+                "scope": "input_prepare_seconds + algorithm_total_seconds + final_partition_d2h_seconds, warm"},
+        "per_step_ms": [round(a * 1e3, 3) for a in algo], "cli_cold": cold, "clocks": clk,
+        "harness": "oracle/_ref/gpart_ref_bench (oracle/ref/ref_bench.cu)",
     }
     print(json.dumps(line), flush=True)
 
@@ -502,6 +563,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cold-cli", action="store_true", help="--impl reference: skip the cold CLI run")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
     ap.add_argument("--side", type=int, default=256, help="mesh side of --launch-list --workload m3")

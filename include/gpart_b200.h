@@ -15,6 +15,7 @@
  *   gp_partition_device     the same pipeline on caller-owned device buffers
  *                           (the reference's resident DeviceWeightedGraph path,
  *                           include/graph.hpp:148-171)
+ *   gp_refine               refine_partition (include/refine.hpp:84-88)
  *   gp_read_csr_int64       load_weighted_graph (include/graph.hpp:173, src/graph.cpp:47)
  *   gp_write_csr_int64      the on-disk int64 CSR format that loader reads
  *   gp_partition_capacity   partition_capacity (include/partition_capacity.hpp:14)
@@ -83,6 +84,8 @@ typedef struct gp_stats {
 #define GP_FLAG_NO_SEED_MATCHING 0x4u /* GPART_HEM_COARSEN=0 (app/partition_main.cu:57)    */
 #define GP_FLAG_QUIET            0x8u /* no per-level key=value log lines on stdout        */
 #define GP_FLAG_COARSEN_ONLY     0x10u /* stop after coarsening (levels kept, no labels)   */
+#define GP_FLAG_REQUIRE_BALANCED 0x20u /* gp_refine: reject an over-capacity start
+                                          (RefineOptions::allow_initial_imbalance = false) */
 
 typedef struct gp_context gp_context;
 
@@ -98,7 +101,9 @@ const char* gp_version(void);
  * "capacity_safe_fast_path" (GPART_REGRET_FORCE_FULL), "cluster_size_factor"
  * (GPART_COARSE_BETA, 0 = default rule), "progressive_fine_factor"
  * (GPART_FINE_FACTOR), "progressive_capacity_growth" (GPART_CAPACITY_GROWTH),
- * "heavy_edge_degree_limit" (GPART_HEM_DEGREE_LIMIT). */
+ * "heavy_edge_degree_limit" (GPART_HEM_DEGREE_LIMIT).  Also "arena_chunk_mb"
+ * (1..2^24, default 256): the smallest block the context's grow-only device
+ * arenas request from cudaMalloc at a time. */
 gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value);
 
 /* Partition a host CSR.  Copies the graph to the device, runs the V-cycle,
@@ -115,12 +120,47 @@ gp_status gp_partition_device(gp_context* ctx, const gp_csr* graph, int32_t k,
                               int32_t* labels_out_device, void* stream,
                               gp_stats* stats);
 
+/* What one gp_refine call did: the RefineStats fields of the reference
+ * (include/refine.hpp:28-53) that describe its moves. */
+typedef struct gp_refine_stats {
+    int32_t rounds;               /* label-propagation rounds run                     */
+    int32_t admission_iterations; /* capacity-repair iterations                       */
+    int32_t checkpoint_updates;   /* rounds that improved the best cut                */
+    int32_t reserved;
+    uint64_t proposals;           /* label-propagation movers, summed over rounds     */
+    uint64_t accepted;            /* vertices moved: propagation, repair, exchange    */
+    uint64_t initial_cut, final_cut, final_max_part_weight, capacity;
+    uint64_t lp_cut_gain, lp_cut_loss;             /* cut change of propagation batches */
+    uint64_t rebalance_cut_gain, rebalance_cut_loss;/* cut change of repair batches   */
+    uint64_t group_cut_gain, group_accepted;        /* capacity exchange batches      */
+    double seconds;               /* device time of the refinement                    */
+    uint64_t kernel_launches;
+} gp_refine_stats;
+
+/* refine_partition (include/refine.hpp:84-88, src/refine.cu:470-481): refines
+ * the host labelling `labels` (n int32 in [0,k), overwritten with the result)
+ * of the host graph with one level of the pipeline's refinement — capacity
+ * repair of an over-capacity start, up to max_rounds (0..64; the pipeline
+ * uses 32) label-propagation rounds with priority filtering and exact
+ * updates, then on graphs of at most 65,536 vertices up to exchange_rounds
+ * (0..8; the pipeline uses 2) capacity-exchange batches.  Capacity repair
+ * orders donors and receiver tickets deterministically (the reference orders
+ * them by atomic arrival).  Flags: GP_FLAG_VERIFY, GP_FLAG_QUIET,
+ * GP_FLAG_REQUIRE_BALANCED.  A start whose repair cannot restore capacity
+ * returns GP_CAPACITY_INFEASIBLE and leaves `labels` unchanged. */
+gp_status gp_refine(gp_context* ctx, const gp_csr* graph, int32_t k, double epsilon,
+                    int32_t max_rounds, int32_t exchange_rounds, uint32_t flags,
+                    int32_t* labels, gp_refine_stats* stats);
+
 /* Cut and part loads of a labelling of a device-resident graph
  * (refine_cut_kernel + accumulate_part_weights_kernel, src/refine.cu:63-126).
  * graph pointers, labels (n int32 in [0,k)), cut_out (1 uint64) and
  * loads_out (k uint64) are device memory; cut_out receives the directed
  * cut / 2.  Ordered on `stream` (NULL: the context stream); returns after the
- * results are written.  Per-block partial sums live in the context arena. */
+ * results are written.  Per-block partial sums live in the context arena.
+ * Labels outside [0,k), neighbours outside [0,n) and offsets outside [0,m]
+ * are skipped, never dereferenced, and make the call return
+ * GP_INVALID_ARGUMENT. */
 gp_status gp_evaluate_device(gp_context* ctx, const gp_csr* graph, const int32_t* labels,
                              int32_t k, uint64_t* cut_out, uint64_t* loads_out,
                              void* stream);
@@ -131,13 +171,18 @@ gp_status gp_evaluate_device(gp_context* ctx, const gp_csr* graph, const int32_t
  * serving loop that must not call cudaMalloc/cudaFree (which can synchronise
  * the device) once it is running.  It calls no cudaMalloc, cudaFree or other
  * allocating routine and needs no context: the per-block partial sums live
- * in one fixed file-scope device array of 592 x 129 uint64 (611 KB) that every
+ * in one fixed file-scope device array of 592 x 130 uint64 (616 KB) that every
  * GPU loading this library holds until the process exits.  k is limited to
  * 1..128 (the array's capacity); larger k returns GP_INVALID_ARGUMENT.
  * Runs on the current device and `stream` (NULL: the legacy default stream)
- * and returns without waiting for the results.  The first call on each
+ * and returns without waiting for the results, so it cannot report bad
+ * device data as a status: labels outside [0,k), neighbours outside [0,n) and
+ * offsets outside [0,m] are skipped, never dereferenced, and *cut_out then
+ * receives UINT64_MAX (no real cut reaches it).  The first call on each
  * device looks up the array's device address (cudaGetSymbolAddress) and
- * caches it; make that first call before any stream capture.  All calls on a
+ * caches it; make that first call before any stream capture.  The cache
+ * assumes the device's primary context for the life of the process (no
+ * cudaDeviceReset, no other driver-API context current).  All calls on a
  * device share the one array and it keeps the last call's contents: calls
  * whose work overlaps on the GPU (different streams, or different host
  * threads) race on it and must be serialised by the caller. */

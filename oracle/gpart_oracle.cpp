@@ -632,6 +632,7 @@ struct Refiner {
     std::vector<Sample> samples;
     u64 cut = 0;
     u64 revision = 0;
+    orc_refine_stats stats{};  // RefineStats (include/refine.hpp:28-53)
 
     Refiner(const Graph& graph, int parts, std::vector<int32_t>& lab, std::vector<u64> ld, u64 capacity)
         : g(graph), k(parts), C(capacity), labels(lab), loads(std::move(ld)), n(graph.n) {}
@@ -847,9 +848,13 @@ struct Refiner {
             if (!movers.empty()) {
                 delta = apply(movers, false, priced);
                 ++revision;
+                stats.accepted += movers.size();
+                if (delta >= 0) stats.rebalance_cut_gain += static_cast<u64>(delta);
+                else stats.rebalance_cut_loss += static_cast<u64>(-delta);
             }
             if (gain_sum && delta > 0) *gain_sum += static_cast<u64>(delta);
             ++iterations;
+            ++stats.admission_iterations;
             for (int32_t v : movers) flags[v] = 0;
             const bool feasible = max_load() <= C;
             if (feasible || movers.empty() || iterations >= 2 * k + 4) return feasible;
@@ -903,9 +908,13 @@ struct Refiner {
             if (keep) movers.push_back(static_cast<int32_t>(v));
         }
         for (int32_t v : movers) flags[v] = 1;
+        stats.proposals += movers.size();
         if (!movers.empty()) {
-            apply(movers, true, false);
+            const i64 delta = apply(movers, true, false);
             ++revision;
+            stats.accepted += movers.size();
+            if (delta >= 0) stats.lp_cut_gain += static_cast<u64>(delta);
+            else stats.lp_cut_loss += static_cast<u64>(-delta);
         }
         for (int32_t v : movers) flags[v] = 0;
         return static_cast<i64>(movers.size());
@@ -1059,6 +1068,8 @@ struct Refiner {
             if (delta <= 0) fail(5, "non-improving boundary group batch");
             if (max_load() > C || cut >= best_cut) fail(5, "capacity exchange violated cut/capacity");
             best_cut = cut;
+            stats.group_cut_gain += static_cast<u64>(delta);
+            stats.group_accepted += movers.size();
         }
     }
 
@@ -1223,11 +1234,13 @@ struct Refiner {
     }
 };
 
-struct LevelResult { u64 cut = 0; bool refined = false; bool repair_failed = false; };
+struct LevelResult { u64 cut = 0; bool refined = false; bool repair_failed = false; orc_refine_stats stats{}; };
 
-// run_incremental_refinement_typed (incremental.cuh:660-1051).
+// run_incremental_refinement_typed (incremental.cuh:660-1051); `rounds` and
+// `exchange_rounds` are RefineOptions::max_rounds and exchange_rounds (the
+// pipeline passes 32 and 2, app/partition_main.cu:111-118, refine.hpp:18).
 LevelResult refine_level(const Graph& g, int k, double eps, std::vector<int32_t>& labels, std::vector<u64>& loads,
-                         bool has_known, u64 known) {
+                         bool has_known, u64 known, int rounds = 32, int exchange_rounds = 2) {
     u64 total = 0;
     for (u64 w : loads) total += w;
     const u64 C = partition_capacity(total, k, eps);
@@ -1242,12 +1255,17 @@ LevelResult refine_level(const Graph& g, int k, double eps, std::vector<int32_t>
     r.priced = total > static_cast<u64>(n);
     r.build();
     r.cut = has_known ? known : cut_of(g, labels);
+    r.stats.initial_cut = r.cut;
+    r.stats.capacity = C;
     LevelResult res;
     if (r.max_load() > C) {
         if (!r.repair()) {
             res.cut = r.cut;
             res.repair_failed = true;
             loads = r.loads;
+            r.stats.final_cut = r.cut;
+            r.stats.final_max_part_weight = r.max_load();
+            res.stats = r.stats;
             return res;
         }
     }
@@ -1260,7 +1278,8 @@ LevelResult refine_level(const Graph& g, int k, double eps, std::vector<int32_t>
     for (u32 w : g.ew) max_edge = std::max(max_edge, w);
     const double filter = max_edge <= 1 ? 0.25 : 0.75;
     int stale = 0, empty = 0;
-    for (int phase = 0; phase < 32 && stale < 3; ++phase) {
+    for (int phase = 0; phase < rounds && stale < 3; ++phase) {
+        r.stats.rounds = phase + 1;
         std::fill(r.samples.begin(), r.samples.end(), Refiner::Sample{});
         const i64 count = r.lp_round(filter);
         if (!count) { if (++empty >= 2) break; ++stale; continue; }
@@ -1277,14 +1296,15 @@ LevelResult refine_level(const Graph& g, int k, double eps, std::vector<int32_t>
             saved_labels = labels;
             saved_loads = r.loads;
             best_revision = r.revision;
+            ++r.stats.checkpoint_updates;
         }
     }
     const bool restored = r.revision != best_revision;
     if (restored) { labels = saved_labels; r.loads = saved_loads; }
     r.cut = best;
-    if (n <= 65536) {
+    if (rounds > 0 && exchange_rounds > 0 && n <= 65536) {
         if (restored) r.build();
-        r.exchange(2, best);
+        r.exchange(exchange_rounds, best);
     }
     if (std::getenv("ORC_TRACE"))
         std::fprintf(stderr, "refine n=%lld start=%llu best=%llu final=%llu repairs=%d restored=%d\n", (long long)n,
@@ -1293,6 +1313,9 @@ LevelResult refine_level(const Graph& g, int k, double eps, std::vector<int32_t>
     loads = r.loads;
     res.cut = r.cut;
     res.refined = true;
+    r.stats.final_cut = r.cut;
+    r.stats.final_max_part_weight = r.max_load();
+    res.stats = r.stats;
     return res;
 }
 
@@ -1306,9 +1329,9 @@ struct State {
 };
 thread_local State g_state;
 
-int run(const orc_csr* in, int32_t k, double eps, uint32_t seed, uint32_t flags, int32_t* labels_out, uint64_t* cut_out) {
-    if (!in || in->n <= 0 || in->m < 0 || !in->offsets) fail(1, "invalid graph");
-    if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(1, "invalid partition capacity options");
+// The caller's CSR as an oracle graph, with load_weighted_graph's and
+// validate_weighted_shape's checks (src/graph.cpp:47-155).
+Graph to_graph(const orc_csr* in) {
     Graph g;
     g.n = in->n;
     g.m = in->m;
@@ -1321,8 +1344,16 @@ int run(const orc_csr* in, int32_t k, double eps, uint32_t seed, uint32_t flags,
     if (g.off[0] != 0 || g.off[g.n] != g.m) fail(1, "invalid weighted CSR shape");
     for (i64 v = 0; v < g.n; ++v) if (g.off[v] > g.off[v + 1]) fail(1, "weighted CSR offsets are not monotone");
     for (i64 e = 0; e < g.m; ++e) if (g.nbr[e] < 0 || g.nbr[e] >= g.n) fail(1, "weighted CSR contains an invalid neighbor");
+    for (u32 w : g.vw) if (!w) fail(1, "vertex weights must be positive");
+    return g;
+}
+
+int run(const orc_csr* in, int32_t k, double eps, uint32_t seed, uint32_t flags, int32_t* labels_out, uint64_t* cut_out) {
+    if (!in || in->n <= 0 || in->m < 0 || !in->offsets) fail(1, "invalid graph");
+    if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(1, "invalid partition capacity options");
+    Graph g = to_graph(in);
     u64 total = 0;
-    for (u32 w : g.vw) { if (!w) fail(1, "vertex weights must be positive"); total += w; }
+    for (u32 w : g.vw) total += w;
     partition_capacity(total, k, eps);
     Options o;
     o.parts = k;
@@ -1392,6 +1423,34 @@ int orc_partition(const orc_csr* graph, int32_t k, double epsilon, uint32_t seed
                   int32_t* labels_out, uint64_t* cut_out) {
     try {
         return run(graph, k, epsilon, seed, flags, labels_out, cut_out);
+    } catch (const Fail& f) {
+        g_error = f.what();
+        return f.status;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 5;
+    }
+}
+
+int orc_refine(const orc_csr* in, int32_t k, double epsilon, int32_t max_rounds, int32_t exchange_rounds,
+               int32_t* labels, orc_refine_stats* stats) {
+    try {
+        if (!in || in->n <= 0 || in->m < 0 || !in->offsets || !labels || k < 2 || k > kMaxParts ||
+            max_rounds < 0 || max_rounds > 64 || exchange_rounds < 0 || exchange_rounds > 8 ||
+            !std::isfinite(epsilon) || epsilon < 1.0)
+            fail(1, "invalid refinement options");
+        Graph g = to_graph(in);
+        std::vector<int32_t> lab(labels, labels + in->n);
+        std::vector<u64> loads(static_cast<size_t>(k), 0);
+        for (i64 v = 0; v < g.n; ++v) {
+            if (lab[v] < 0 || lab[v] >= k) fail(1, "refinement partition has an invalid part id");
+            loads[lab[v]] += g.vw[v];
+        }
+        const LevelResult r = refine_level(g, k, epsilon, lab, loads, false, 0, max_rounds, exchange_rounds);
+        if (stats) *stats = r.stats;
+        if (r.repair_failed) fail(2, "initial refinement capacity repair failed");
+        std::copy(lab.begin(), lab.end(), labels);
+        return 0;
     } catch (const Fail& f) {
         g_error = f.what();
         return f.status;

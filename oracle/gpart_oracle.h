@@ -7,8 +7,10 @@
  * the reference's own CUDA build (tests/golden/*.json, produced by
  * tests/golden/make_golden.py on a B200).  Refinement is the reference's LP,
  * priority filter, exact update and capacity exchange restated serially, with
- * the repair step in the deterministic (bucket, vertex id) order that the
- * GPU path also uses (the reference ranks repair donors by atomic arrival).
+ * the repair step in the deterministic (bucket, repair hash, id) order that
+ * the GPU path also uses (the reference ranks repair donors by atomic
+ * arrival).  Single-level refinement without repair batches is pinned against
+ * the reference's refine_partition (tests/golden/refine_cases.json).
  */
 #ifndef GPART_ORACLE_H
 #define GPART_ORACLE_H
@@ -41,6 +43,19 @@ int orc_level_copy(int32_t level, int32_t* offsets, int32_t* neighbors,
                    uint32_t* edge_weights, uint32_t* vertex_weights, int32_t* map,
                    uint64_t* metadata);
 int orc_initial_labels(int32_t* labels, int64_t capacity);
+/* RefineStats of include/refine.hpp:28-53 (the fields describing moves). */
+typedef struct orc_refine_stats {
+    int32_t rounds, admission_iterations, checkpoint_updates, reserved;
+    uint64_t proposals, accepted, initial_cut, final_cut, final_max_part_weight, capacity;
+    uint64_t lp_cut_gain, lp_cut_loss, rebalance_cut_gain, rebalance_cut_loss;
+    uint64_t group_cut_gain, group_accepted;
+} orc_refine_stats;
+
+/* refine_partition (include/refine.hpp:84-88): one level of refinement of
+ * `labels` (in/out) with the given round and exchange budgets. */
+int orc_refine(const orc_csr* graph, int32_t k, double epsilon, int32_t max_rounds,
+               int32_t exchange_rounds, int32_t* labels, orc_refine_stats* stats);
+
 /* Refined labels of every level (level order as in the hierarchy). */
 int orc_level_labels(int32_t level, int32_t* labels);
 /* Cut after refinement of a level, and whether that level was refined. */

@@ -59,6 +59,30 @@ def partition(graph, k, epsilon=1.03, seed=0, flags=0):
     return labels, cut.value
 
 
+class _RefineStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("admission_iterations", C.c_int32), ("checkpoint_updates", C.c_int32),
+                ("reserved", C.c_int32), ("proposals", C.c_uint64), ("accepted", C.c_uint64),
+                ("initial_cut", C.c_uint64), ("final_cut", C.c_uint64), ("final_max_part_weight", C.c_uint64),
+                ("capacity", C.c_uint64), ("lp_cut_gain", C.c_uint64), ("lp_cut_loss", C.c_uint64),
+                ("rebalance_cut_gain", C.c_uint64), ("rebalance_cut_loss", C.c_uint64),
+                ("group_cut_gain", C.c_uint64), ("group_accepted", C.c_uint64)]
+
+
+def refine(graph, labels, k, epsilon=1.03, max_rounds=32, exchange_rounds=2):
+    """refine_partition restated: one level of refinement of `labels`;
+    returns (refined labels, dict of RefineStats)."""
+    L = lib()
+    g = _Csr(graph.n, graph.m, _p(graph.offsets), _p(graph.neighbors), _p(graph.vertex_weights),
+             _p(graph.edge_weights))
+    out = np.array(labels, dtype=np.int32, copy=True)
+    st = _RefineStats()
+    status = L.orc_refine(C.byref(g), C.c_int32(k), C.c_double(epsilon), C.c_int32(max_rounds),
+                          C.c_int32(exchange_rounds), _p(out), C.byref(st))
+    if status != 0:
+        raise OracleError(status, L.orc_last_error().decode())
+    return out, {name: getattr(st, name) for name, _ in _RefineStats._fields_ if name != "reserved"}
+
+
 def levels():
     L = lib()
     out = []

@@ -7,6 +7,17 @@ weights and fine-to-coarse map, then the METIS labels of the coarsest graph
 and the final cut.  Needs a CUDA GPU (the reference is GPU code).
 
     python tests/golden/make_golden.py [--out DIR] [--cases a,b,...] [--baseline]
+    python tests/golden/make_golden.py --refine [--out DIR]
+    python tests/golden/make_golden.py --digests-only --cases rmat22_k64,m3_k128
+
+--refine runs the reference's single-level refinement (oracle/_ref/
+gpart_ref_refine: its run_incremental_refinement on a one-level resident
+hierarchy) on every case of cases.REFINE_CASES and writes refine_cases.json:
+per case the SHA-256 of the refined labels, the part loads, and the
+RefineStats fields the reference reports for that run (-1 where it reports
+none).  --digests-only records hierarchy
+digests and the METIS digest without the final-label checks (for the
+headline-size cases, whose full arrays are too large to keep).
 
 --baseline additionally times the unmodified reference CLI on R-MAT scale 22
 (k=64, seeds 0-2) and writes baseline_rmat22.json.
@@ -41,7 +52,13 @@ def load_package():
 
 gp = load_package()
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from cases import CASES, build_case  # noqa: E402
+from cases import CASES, REFINE_CASES, build_case, refine_start  # noqa: E402
+
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+STAT_FIELDS = ["rounds", "proposals", "accepted", "initial_cut", "final_cut", "final_max_part_weight",
+               "admission_iterations", "admission_fallbacks", "lp_cut_gain", "lp_cut_loss", "rebalance_cut_gain",
+               "rebalance_cut_loss", "checkpoint_updates", "group_cut_gain", "group_accepted",
+               "frontier_vertices_initial"]
 
 
 def digest(array) -> str:
@@ -112,6 +129,58 @@ def summarise(name, spec, dump, graph):
                 reference_seconds=dump["seconds"])
 
 
+def write_inputs(graph, workdir):
+    ip, ix = os.path.join(workdir, "g.indptr"), os.path.join(workdir, "g.indices")
+    gp.write_csr_int64(graph, ip, ix)
+    vw = ew = "-"
+    if graph.vertex_weights is not None:
+        vw = os.path.join(workdir, "g.vw"); graph.vertex_weights.tofile(vw)
+    if graph.edge_weights is not None:
+        ew = os.path.join(workdir, "g.ew"); graph.edge_weights.tofile(ew)
+    return ip, ix, vw, ew
+
+
+def refine_goldens(out_dir, names, arrays_dir=None):
+    """The reference's refine_partition on every refinement case."""
+    import oracle
+    records = {}
+    graphs = {}
+    for name in names:
+        spec = REFINE_CASES[name]
+        g = graphs.get(spec["graph"])
+        if g is None:
+            g = graphs[spec["graph"]] = build_case(gp, CASES[spec["graph"]])
+        start = refine_start(gp, oracle, spec, g)
+        with tempfile.TemporaryDirectory() as tmp:
+            ip, ix, vw, ew = write_inputs(g, tmp)
+            lp = os.path.join(tmp, "start.i32")
+            start.astype(np.int32).tofile(lp)
+            out = os.path.join(tmp, "refined.dump")
+            proc = subprocess.run([os.path.join(REF, "gpart_ref_refine"), ip, ix, vw, ew, lp, str(spec["k"]),
+                                   repr(spec["eps"]), str(spec["rounds"]), str(spec["exchange"]), out],
+                                  capture_output=True, text=True)
+            if proc.returncode != 0:
+                records[name] = dict(spec=spec, error=proc.stderr.strip()[-400:])
+                print(name, "REFERENCE FAILED", proc.stderr.strip()[-300:], flush=True)
+                continue
+            data = open(out, "rb").read()
+        assert data[:8] == b"GPREF002"
+        n = int(np.frombuffer(data, np.int64, 1, 8)[0])
+        labels = np.frombuffer(data, np.int32, n, 16)
+        fields = np.frombuffer(data, np.int64, 16, 16 + 4 * n)
+        stats = {key: int(v) for key, v in zip(STAT_FIELDS, fields)}
+        w = np.ones(n, np.uint64) if g.vertex_weights is None else g.vertex_weights.astype(np.uint64)
+        loads = np.bincount(labels, weights=w, minlength=spec["k"]).astype(np.uint64)
+        records[name] = dict(spec=spec, start=digest(start.astype(np.int32)), labels=digest(labels),
+                             loads=[int(x) for x in loads], cut=gp.edge_cut(g, labels), stats=stats)
+        if arrays_dir:
+            np.save(os.path.join(arrays_dir, f"refine_{name}.npy"), labels)
+        print(name, "cut", stats["initial_cut"], "->", stats["final_cut"], "rounds", stats["rounds"],
+              "repair_iterations", stats["admission_iterations"], flush=True)
+    with open(os.path.join(out_dir, "refine_cases.json"), "w") as f:
+        json.dump(records, f, indent=1, sort_keys=True)
+
+
 def baseline(out_dir):
     g = gp.rmat(22, 16, 0.57, 0.19, 0.19, 0)
     rows = []
@@ -140,8 +209,16 @@ def main():
     ap.add_argument("--cases", default="")
     ap.add_argument("--baseline", action="store_true")
     ap.add_argument("--keep-arrays", action="store_true", help="also save full small-level arrays (npz)")
+    ap.add_argument("--refine", action="store_true", help="refinement goldens (refine_cases.json)")
+    ap.add_argument("--arrays-dir", default="", help="--refine: also save each refined labelling here (.npy)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    if args.refine:
+        names = [c for c in args.cases.split(",") if c] or list(REFINE_CASES)
+        if args.arrays_dir:
+            os.makedirs(args.arrays_dir, exist_ok=True)
+        refine_goldens(args.out, names, args.arrays_dir or None)
+        return
     names = [c for c in args.cases.split(",") if c] or list(CASES)
     for name in names:
         spec = CASES[name]

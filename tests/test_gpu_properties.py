@@ -213,3 +213,21 @@ def test_kept_hierarchy_written_like_write_hierarchy(gp, ctx, tmp_path):
             np.testing.assert_array_equal(w[name], k[name].astype(np.int32), err_msg=f"level {i} {name}")
         if i:
             np.testing.assert_array_equal(w["map_from_previous"], kept[i - 1]["map"])
+
+
+def test_out_of_memory_request_does_not_fail_the_next(gp):
+    """A request whose device allocation fails reports GP_OUT_OF_MEMORY and
+    leaves no error behind: the next request on the same context succeeds
+    with the same labels as a fresh context.  The failure is a real
+    cudaMalloc refusal (a 4 TB arena block), not a fault."""
+    g = gp.grid2d(96, 80)
+    with gp.Context(0) as fresh:
+        expected, _ = fresh.partition(g, 8, 1.03, 0)
+    with gp.Context(0) as c:
+        c.set_option("arena_chunk_mb", 1 << 22)
+        with pytest.raises(gp.GpartError) as e:
+            c.partition(g, 8, 1.03, 0)
+        assert e.value.status == 3
+        c.set_option("arena_chunk_mb", 256)
+        labels, st = c.partition(g, 8, 1.03, 0)
+    np.testing.assert_array_equal(labels, expected)

@@ -36,6 +36,39 @@ def test_static_scratch_entry_matches_allocating_entry(gp):
             assert int(cut_b.item()) == int(cut_a.item()) > 0
             np.testing.assert_array_equal(loads_b.cpu().numpy(), loads_a.cpu().numpy())
             assert int(loads_b.sum().item()) == int(g.vertex_weights.sum())
+            # And against the host verifier, which shares no code with either.
+            verdict = gp.verify(g, labels.cpu().numpy(), k, 2.0)
+            assert int(cut_b.item()) == verdict["cut"]
+            assert [int(x) for x in loads_b.cpu().numpy()] == verdict["loads"]
+
+
+def test_out_of_range_labels_are_skipped_not_dereferenced(gp):
+    """A label outside [0,k) is never used as an index: the allocating entry
+    returns GP_INVALID_ARGUMENT, the static entry (which does not wait for
+    its results) writes UINT64_MAX as the cut, and both stay usable."""
+    import torch
+    g = gp.grid2d(40, 30)
+    k = 6
+    off = torch.from_numpy(g.offsets).cuda()
+    nbr = torch.from_numpy(g.neighbors).cuda()
+    good = (np.arange(g.n) % k).astype(np.int32)
+    bad = good.copy()
+    bad[[3, 500, 1199]] = [k, -1, 1 << 20]
+    cut = torch.zeros(1, dtype=torch.int64, device="cuda")
+    loads = torch.zeros(k, dtype=torch.int64, device="cuda")
+    with gp.Context(0) as ctx:
+        for labels, ok in ((bad, False), (good, True)):
+            d = torch.from_numpy(labels).cuda()
+            ptrs = (off.data_ptr(), nbr.data_ptr(), g.n, g.m, None, None, d.data_ptr(), k)
+            gp.evaluate_device_static(*ptrs, cut.data_ptr(), loads.data_ptr())
+            torch.cuda.synchronize()
+            if ok:
+                assert int(cut.item()) == gp.verify(g, labels, k, 2.0)["cut"]
+            else:
+                assert int(cut.item()) == -1  # UINT64_MAX read as int64
+                with pytest.raises(gp.GpartError) as e:
+                    ctx.evaluate_device(*ptrs, cut.data_ptr(), loads.data_ptr())
+                assert e.value.status == 1 and "out of range" in e.value.message
 
 
 def test_static_scratch_entry_rejects_k_beyond_capacity(gp):
