@@ -855,16 +855,28 @@ __device__ __forceinline__ long long update_entries(int v, int s, int t, int fir
     return gain;
 }
 
+// Compulsory DRAM bytes of updating one moved row of `entries` entries: the
+// mover id, its two offsets, its own label and target, per entry the
+// neighbour id (and edge weight) and the read and write of the two cache
+// counters it changes.  The neighbours' label, flag and target gathers are
+// not counted: those three n-word arrays stay resident in L2.
+template <class C>
+__device__ __forceinline__ u64 update_row_bytes(int entries, bool weighted, bool cached) {
+    return 20ULL + static_cast<u64>(entries) * (4ULL + (weighted ? 4ULL : 0ULL) + (cached ? 4ULL * sizeof(C) : 0ULL));
+}
+
 // incremental_update_cache_and_cut (incremental.cuh:440-506): exact cut delta
 // and dense cache updates; optional repair samples per source part.  A warp
 // takes four movers at a time: rows of up to kUpdateShort entries are done by
 // eight lanes each, longer ones (up to heavy_min) by the whole warp after
-// them, so a warp's memory chains cover four short rows at once.
+// them, so a warp's memory chains cover four short rows at once.  With
+// `work`, the compulsory bytes of the rows it updated are added there.
 constexpr int kUpdateShort = 16;
 template <class C>
 __global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
                          const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
-                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold, int heavy_min) {
+                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold, int heavy_min,
+                         u64* work) {
     constexpr int W = 8, G = 32 / W;
     __shared__ WarpSum delta_sum;
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
@@ -875,12 +887,14 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
     for (int g = 0; g < G; ++g) leaders |= 1u << (g * W);
     const i64 warps = (static_cast<i64>(gridDim.x) * blockDim.x) >> 5;
     long long total = 0;
+    u64 bytes = 0;
     for (i64 base = ((static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * G; base < count;
          base += warps * G) {
         const i64 i = base + gid;
         const int v = i < count ? movers[i] : -1;
         const int begin = v >= 0 ? off[v] : 0, end = v >= 0 ? off[v + 1] : 0;
         const bool light = v >= 0 && end - begin <= heavy_min;  // heavier rows: k_update_chunks
+        if (work && sub == 0 && light) bytes += update_row_bytes<C>(end - begin, ew != nullptr, A != nullptr);
         const int s = light ? labels[v] : 0, t = light ? targets[v] : 0;
         long long gain = light && end - begin <= kUpdateShort
                              ? update_entries(v, s, t, begin + sub, end, W, nbr, ew, labels, targets, flags, k, A)
@@ -905,16 +919,23 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
         }
     }
     delta_sum.finish(static_cast<u64>(warp_sum(total)), reinterpret_cast<u64*>(delta));
+    if (work) {
+        bytes = warp_sum(bytes);
+        if (lane == 0 && bytes) atomicAdd(reinterpret_cast<unsigned long long*>(work), bytes);
+    }
 }
 
 // Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,
 // incremental.cuh:508-530); a row moves when its flag is set.
 template <class C>
 __global__ void k_update_chunks(DGraph g, const int* labels, const int* targets, const int* flags, int k, C* A,
-                                long long* delta, Sample* samples, const u64* gate, u64 threshold) {
+                                long long* delta, Sample* samples, const u64* gate, u64 threshold, u64* work) {
     if (gate && *gate > threshold) return;
     const int c = blockIdx.x, v = g.chunk_row[c];
     if (!flags[v]) return;
+    if (work && threadIdx.x == 0)  // the chunk's entries, its row, begin and row id (no per-row mover id)
+        atomicAdd(reinterpret_cast<unsigned long long*>(work),
+                  update_row_bytes<C>(chunk_end(g, c, v) - g.chunk_begin[c], g.ew != nullptr, true) - 8ULL);
     const int s = labels[v], t = targets[v];
     long long gain = 0;
     for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
@@ -2253,12 +2274,13 @@ private:
         else
             launch(k_update<T>, grid_for(host_count * 8, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
                    g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
-                   sample ? samples : static_cast<Sample*>(nullptr), gate, threshold, g.heavy_min);
+                   sample ? samples : static_cast<Sample*>(nullptr), gate, threshold, g.heavy_min,
+                   work_counter(k_update<T>));
         if (g.chunks)
             launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
                    static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
                    reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr), gate,
-                   threshold);
+                   threshold, work_counter(k_update_chunks<T>));
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags,
                static_cast<const u32*>(rposition), rlabels);

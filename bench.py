@@ -36,20 +36,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 WORKLOAD = dict(workload="rmat22_k64", graph="R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, seed 0",
                 k=64, epsilon=1.03, seed=0, vertices=4194304)
 METRIC = "partition ms & batched graphs/s at k=64 ε=1.03; cut vs ref; HBM GB/s"
-# Kernel whose roofline fraction is reported: the affinity-cache build of the
-# refinement, the largest share of device time in the ncu launch list of this
-# workload (profiles/).  One build is three launches, all matched by this
-# pattern: k_build (rows up to 64 entries, heavy rows as zeros), k_build_long
-# (65..2048 entries, a warp per row) and k_build_chunks (the heavy rows'
-# 2048-entry chunks).  Each reports its algorithmic bytes from the device when
-# it runs (a build the update path made unnecessary adds nothing): offsets,
-# neighbours and label gathers of its rows, the k-wide cache rows and totals
-# it writes, each row's own label.
-DOMINANT_KERNEL = "k_build"
-DOMINANT_LABEL = "affinity-cache build (k_build + k_build_long + k_build_chunks)"
-# ncu DRAM bytes (read + write) per algorithmic byte of that build, from the
-# capture summarised in this file ("traffic_per_algorithmic_byte: x").
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "cache_build_rmat20_k64.md")
+# Kernels whose roofline fraction is reported.  The dominant operation is the
+# incremental affinity-cache update of the refinement (k_update for rows up to
+# the level's heavy-row threshold, k_update_chunks for the heavy rows' chunks;
+# the pattern matches both): the largest share of device time in this
+# workload's launch list (profiles/).  The second entry is the cache build
+# (k_build, k_build_long, k_build_chunks), the largest streaming operation.
+# Both report their compulsory bytes from the device when they run; the
+# update's model counts, per moved row, its id, offsets, label and target and,
+# per entry, the neighbour id and the read and write of the two cache
+# counters it changes (the neighbours' label, flag and target gathers hit the
+# L2-resident n-word arrays and are not compulsory DRAM traffic).
+ROOFLINES = (("k_update", "incremental cache update (k_update + k_update_chunks)"),
+             ("k_build", "affinity-cache build (k_build + k_build_long + k_build_chunks)"))
+# ncu DRAM bytes (read + write) per algorithmic byte of each operation, from
+# the full-size captures summarised beside this file's entries.
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
 
 
 def load_package():
@@ -208,7 +210,7 @@ def run_ours(args):
     clocks.start()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ctx.profile_begin(DOMINANT_KERNEL)
+    ctx.profile_begin(ROOFLINES[0][0])
     launches = 0
     stats = []
     start.record(stream)
@@ -247,19 +249,14 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
     e2e_value = world * len(e2e_times) / e2e_elapsed
-    # Roofline of the dominant kernel: algorithmic bytes per launch / duration.
-    peak, peak_kind = measured_peak_hbm()
-    roof = None
-    if dom_launches and dom_ms > 0:
-        per_launch_ms = dom_ms / dom_launches
-        alg = dom_bytes / dom_launches
-        achieved = alg / (per_launch_ms * 1e-3) / 1e9
-        ratio = traffic_ratio()
-        roof = {"bound": "hbm", "kernel": DOMINANT_LABEL, "achieved": achieved, "peak": peak,
-                "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": alg * ratio if ratio else None,
-                "algorithmic_bytes_per_launch": alg, "launches": dom_launches, "avg_launch_ms": per_launch_ms,
-                "share_of_step": dom_ms / (elapsed * 1e3 / world) if elapsed > 0 else None}
+    # Roofline of the dominant operation, timed live in the timed region, and
+    # of the cache build, timed the same way over one more partition.
+    ctx.profile_begin(ROOFLINES[1][0])
+    step()
+    torch.cuda.synchronize()
+    second = ctx.profile_end()
+    roof = roofline(ROOFLINES[0], (dom_launches, dom_ms, dom_bytes), elapsed * 1e3)
+    roof2 = roofline(ROOFLINES[1], second, None)
     vcycle_bytes = stats[-1].algorithmic_bytes
     line = {
         "metric": METRIC, "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
@@ -275,7 +272,7 @@ def run_ours(args):
                        "achieved_gbs": vcycle_bytes / (elapsed / args.steps) / 1e9},
         "e2e": {"value": e2e_value, "unit": "graphs/s", "h2d_bytes_per_step": 4 * (n + 1) + 4 * m,
                 "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_elapsed / len(e2e_times) * 1e3},
-        "gpu_launches": launches, "roofline": roof, "clocks": clk,
+        "gpu_launches": launches, "roofline": roof, "roofline_build": roof2, "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(gp, m)
@@ -287,18 +284,36 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def traffic_ratio():
-    """DRAM bytes per algorithmic byte of the dominant kernel, as measured by
-    ncu on the capture described in TRAFFIC_PROFILE (None if absent)."""
+def traffic_ratios():
+    """DRAM bytes per algorithmic byte of each reported operation, measured by
+    ncu on the captures recorded in TRAFFIC_FILE ({} if absent)."""
     try:
-        with open(TRAFFIC_PROFILE) as f:
-            for line in f:
-                m = re.search(r"traffic_per_algorithmic_byte:\s*([0-9.]+)", line)
-                if m:
-                    return float(m.group(1))
-    except OSError:
-        pass
-    return None
+        with open(TRAFFIC_FILE) as f:
+            return {key: float(entry["dram_bytes_per_algorithmic_byte"]) for key, entry in json.load(f).items()
+                    if isinstance(entry, dict) and "dram_bytes_per_algorithmic_byte" in entry}
+    except (OSError, ValueError, KeyError):
+        return {}
+
+
+def roofline(which, profiled, region_ms):
+    """roofline object of one operation: algorithmic bytes per launch over its
+    average CUDA-event launch time, against the measured copy bandwidth."""
+    pattern, label = which
+    launches, ms, alg_total = profiled
+    if not launches or ms <= 0:
+        return None
+    peak, peak_kind = measured_peak_hbm()
+    per_launch_ms = ms / launches
+    alg = alg_total / launches
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    ratio = traffic_ratios().get(pattern)
+    out = {"bound": "hbm", "kernel": label, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+           "unit": "GB/s", "frac": achieved / peak, "traffic": alg * ratio if ratio else None,
+           "algorithmic_bytes_per_launch": alg, "launches": launches, "avg_launch_ms": per_launch_ms,
+           "dram_frac": achieved * ratio / peak if ratio else None}
+    if region_ms:
+        out["share_of_step"] = ms / region_ms
+    return out
 
 
 def config_for(world):

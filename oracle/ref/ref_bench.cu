@@ -115,7 +115,7 @@ int main(int argc, char** argv) {
             std::cout << "vertices=" << g.vertices() << " edges=" << g.edges() << '\n';
             return 0;
         }
-        if (mode != "rmat" || argc != 14) {
+        if (mode != "rmat" || argc != 13) {
             std::cerr << "usage: gpart_ref_bench rmat SCALE EF A B C GSEED K EPS SEED WARMUP STEPS\n"
                          "       gpart_ref_bench write-rmat SCALE EF A B C GSEED indptr indices\n";
             return 2;
