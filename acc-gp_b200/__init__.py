@@ -60,7 +60,8 @@ class _Stats(_C.Structure):
                 ("coarsen_seconds", _C.c_double), ("initial_seconds", _C.c_double),
                 ("uncoarsen_seconds", _C.c_double), ("algorithm_seconds", _C.c_double),
                 ("h2d_seconds", _C.c_double), ("d2h_seconds", _C.c_double),
-                ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64)]
+                ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64),
+                ("device_peak_bytes", _C.c_uint64)]
 
 
 class _RefineStats(_C.Structure):
@@ -298,6 +299,7 @@ class Stats:
     d2h_seconds: float
     kernel_launches: int
     algorithmic_bytes: int
+    device_peak_bytes: int = 0
 
     @classmethod
     def _from(cls, s: _Stats) -> "Stats":
@@ -390,10 +392,11 @@ class Context:
                                       _C.c_uint32(seed), _C.c_uint32(flags), _C.c_void_p(labels_ptr), _C.byref(stats)))
         return Stats._from(stats)
 
-    def partition_batch(self, jobs, concurrency: int = 8, flags: int = FLAG_QUIET):
+    def partition_batch(self, jobs, concurrency: int = 8, flags: int = FLAG_QUIET, devices=None):
         """gp_partition_batch over (graph, k, epsilon, seed) tuples; returns a
         list of (labels, Stats, run_seconds) in input order.  Raises on the
-        first failed request."""
+        first failed request.  With `devices` (device ordinals), the graphs
+        are placed over those GPUs (gp_partition_batch_devices)."""
         jobs = list(jobs)
         requests = (_Request * max(1, len(jobs)))()
         keep = []
@@ -406,7 +409,13 @@ class Context:
             r.graph = g
             r.k, r.epsilon, r.seed, r.flags = k, eps, seed, flags
             r.labels_out = labels.ctypes.data_as(_C.c_void_p)
-        _check(self._lib.gp_partition_batch(self._handle, requests, _C.c_int32(len(jobs)), _C.c_int32(concurrency)))
+        if devices is None:
+            _check(self._lib.gp_partition_batch(self._handle, requests, _C.c_int32(len(jobs)),
+                                                _C.c_int32(concurrency)))
+        else:
+            devs = (_C.c_int32 * len(devices))(*devices)
+            _check(self._lib.gp_partition_batch_devices(self._handle, devs, _C.c_int32(len(devices)), requests,
+                                                        _C.c_int32(len(jobs)), _C.c_int32(concurrency)))
         return [(outs[i], Stats._from(requests[i].stats), requests[i].run_seconds) for i in range(len(jobs))]
 
     def evaluate_device(self, offsets_ptr: int, neighbors_ptr: int, n: int, m: int, vertex_weights_ptr,
@@ -490,17 +499,47 @@ def evaluate_device_static(offsets_ptr: int, neighbors_ptr: int, n: int, m: int,
                                                _C.c_void_p(stream_ptr) if stream_ptr else None))
 
 
+def batch_work(graph: Graph) -> int:
+    """The batched form's placement estimate of one partition (bytes of one
+    CSR sweep with its neighbour gathers)."""
+    return 4 * (graph.n + 1) + 8 * graph.m + (4 * graph.m if graph.edge_weights is not None else 0)
+
+
+def plan_placement(work, devices: int):
+    """gp_plan_placement: longest-processing-time placement of work items on
+    `devices` devices; returns (device_of, device_work) as numpy arrays."""
+    work = _np.ascontiguousarray(work, dtype=_np.uint64)
+    device_of = _np.empty(work.shape[0], _np.int32)
+    device_work = _np.empty(devices, _np.uint64)
+    _check(library().gp_plan_placement(_ptr(work), _C.c_int32(work.shape[0]), _C.c_int32(devices),
+                                       _ptr(device_of), _ptr(device_work)))
+    return device_of, device_work
+
+
 class Server:
     """gp_server_*: worker contexts taking requests as they arrive, admitted
-    by estimated device footprint; resident graphs via add_graph."""
+    by estimated device footprint; resident graphs via add_graph.  `device`
+    may be a list of device ordinals (gp_server_create_devices; `workers`
+    per device, `hbm_budget_bytes` per device)."""
 
-    def __init__(self, device: int = 0, workers: int = 8, hbm_budget_bytes: int = 0):
+    def __init__(self, device=0, workers: int = 8, hbm_budget_bytes: int = 0):
         self._lib = library()
         self._handle = _C.c_void_p()
         self._pending = {}
-        _check(self._lib.gp_server_create(_C.c_int(device), _C.c_int32(workers), _C.c_uint64(hbm_budget_bytes),
-                                          _C.byref(self._handle)))
+        if isinstance(device, (list, tuple)):
+            devs = (_C.c_int32 * len(device))(*device)
+            _check(self._lib.gp_server_create_devices(devs, _C.c_int32(len(device)), _C.c_int32(workers),
+                                                      _C.c_uint64(hbm_budget_bytes), _C.byref(self._handle)))
+        else:
+            _check(self._lib.gp_server_create(_C.c_int(device), _C.c_int32(workers), _C.c_uint64(hbm_budget_bytes),
+                                              _C.byref(self._handle)))
         self._graphs = []
+
+    def footprint(self, graph_id: int, k: int) -> int:
+        """gp_server_footprint: the admission estimate of a request, in bytes."""
+        out = _C.c_uint64()
+        _check(self._lib.gp_server_footprint(self._handle, _C.c_int32(graph_id), _C.c_int32(k), _C.byref(out)))
+        return out.value
 
     def add_graph(self, graph: Graph) -> int:
         gid = _C.c_int32()

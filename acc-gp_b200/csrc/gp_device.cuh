@@ -127,6 +127,7 @@ public:
             if (c.top + bytes <= c.size) {
                 void* p = c.base + c.top;
                 c.top += bytes;
+                note_use();
                 return p;
             }
             if (current_ + 1 < chunks_.size()) { ++current_; chunks_[current_].top = 0; continue; }
@@ -138,16 +139,27 @@ public:
         c.top = bytes;
         chunks_.push_back(c);
         current_ = chunks_.size() - 1;
+        note_use();
         return c.base;
     }
     void set_chunk_bytes(size_t b) { chunk_bytes_ = b; }
     size_t reserved() const { size_t s = 0; for (auto& c : chunks_) s += c.size; return s; }
+    // Largest number of bytes held at once since reset_peak() (the measured
+    // footprint of the work in between).
+    size_t peak() const { return peak_; }
+    void reset_peak() { peak_ = 0; note_use(); }
 
 private:
+    void note_use() {
+        size_t used = 0;
+        for (size_t i = 0; i <= current_ && i < chunks_.size(); ++i) used += chunks_[i].top;
+        if (used > peak_) peak_ = used;
+    }
     struct Chunk { char* base = nullptr; size_t size = 0, top = 0; };
     std::vector<Chunk> chunks_;
     size_t current_ = 0;
     size_t chunk_bytes_ = size_t{256} << 20;
+    size_t peak_ = 0;
 };
 
 // Scoped release of an arena region.

@@ -278,6 +278,8 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     const u64 launches0 = g_launches;
     ctx.persist.release({0, 0});
     ctx.scratch.release({0, 0});
+    ctx.persist.reset_peak();
+    ctx.scratch.reset_peak();
     const i64 n = in->n;
     Input input = prepare_input(ctx, in, device_input);
     DGraph& g = input.g;
@@ -352,6 +354,7 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
         stats->d2h_seconds = device_input ? 0.0 : elapsed(ctx.ev[4], ctx.ev[5]) * 1e-3;
         stats->kernel_launches = g_launches - launches0;
         stats->algorithmic_bytes = algorithmic_bytes(h);
+        stats->device_peak_bytes = ctx.persist.peak() + ctx.scratch.peak();
     }
     return GP_OK;
 }

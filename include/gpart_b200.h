@@ -76,6 +76,8 @@ typedef struct gp_stats {
     double d2h_seconds;           /* device → host copy of the labels (gp_partition) */
     uint64_t kernel_launches;     /* kernels this library launched during the call   */
     uint64_t algorithmic_bytes;   /* compulsory HBM traffic model of the V-cycle     */
+    uint64_t device_peak_bytes;   /* most device memory the call held at once in the
+                                     context's arenas (its measured footprint)       */
 } gp_stats;
 
 /* Flags for gp_partition / gp_partition_device. */
@@ -220,18 +222,52 @@ typedef struct gp_request {
  * request (per-request status in requests[i].status). */
 gp_status gp_partition_batch(gp_context* ctx, gp_request* requests, int32_t count, int32_t concurrency);
 
+/* The batched form over several GPUs of this node (graph-level placement,
+ * no collective: each graph runs wholly on one device and its labels are
+ * copied to its host buffer).  Graphs are placed by gp_plan_placement over
+ * `devices` (device ordinals); on each device up to `concurrency` graphs run
+ * at a time, largest first.  Every result is identical to gp_partition of
+ * the same request alone.  Status as gp_partition_batch. */
+gp_status gp_partition_batch_devices(gp_context* ctx, const int32_t* devices, int32_t device_count,
+                                     gp_request* requests, int32_t count, int32_t concurrency);
+
+/* Longest-processing-time placement of `count` work items on `devices`
+ * devices: items in decreasing work (ties: lower index first), each to the
+ * device with the least work placed so far (ties: lower device).  Writes
+ * device_of[count] (0..devices-1) and, if non-NULL, device_work[devices].
+ * Deterministic, so every process of a job computes the same plan.  The
+ * batched form uses work = 4(n+1) + 8m (+4m with edge weights) bytes, one
+ * CSR sweep with its neighbour gathers.  Needs no device. */
+gp_status gp_plan_placement(const uint64_t* work, int32_t count, int32_t devices, int32_t* device_of,
+                            uint64_t* device_work);
+
 /* A partition server: `workers` threads, each with its own context on
  * `device`, take requests as they arrive.  A request is admitted when its
  * estimated device footprint fits in what is left of hbm_budget_bytes
  * (0: no limit) among the requests running; smaller requests may pass a
- * waiting larger one.  Graphs added with gp_server_add_graph stay resident
- * on the device and are partitioned without an upload.  With a budget, a
- * worker whose device arenas hold more than budget/workers after a request
- * releases them.  No counterpart in the reference. */
+ * waiting larger one, and an idle device always admits the next request.
+ * The estimate of a request on a resident graph that has run before is that
+ * graph's measured footprint (the largest device_peak_bytes of its requests,
+ * less the k-wide affinity cache) plus the cache of the request's k and an
+ * eighth more; otherwise a static estimate from n, m and k.  Graphs added
+ * with gp_server_add_graph stay resident on the device and are partitioned
+ * without an upload.  With a budget, a worker whose device arenas hold more
+ * than budget/workers after a request releases them.  No counterpart in the
+ * reference. */
 typedef struct gp_server gp_server;
 gp_status gp_server_create(int device, int32_t workers, uint64_t hbm_budget_bytes, gp_server** out);
-/* Uploads a host CSR once; requests name it by *graph_id. */
+/* The same server over several GPUs: `workers_per_device` workers on each of
+ * `devices`, an HBM budget per device, resident graphs copied to every
+ * device; a request runs on the first device with a free worker whose budget
+ * admits it (graph-level placement; no collective). */
+gp_status gp_server_create_devices(const int32_t* devices, int32_t device_count, int32_t workers_per_device,
+                                   uint64_t hbm_budget_bytes, gp_server** out);
+/* Uploads a host CSR once (to every device of the server); requests name it
+ * by *graph_id. */
 gp_status gp_server_add_graph(gp_server* server, const gp_csr* graph, int32_t* graph_id);
+/* The admission estimate, in bytes, of a request of part count k on a
+ * resident graph. */
+gp_status gp_server_footprint(gp_server* server, int32_t graph_id, int32_t k, uint64_t* bytes);
 /* Queues a request (graph_id -1: request->graph is a host CSR).  The request
  * and its buffers must stay valid until gp_server_wait returns for it. */
 gp_status gp_server_submit(gp_server* server, gp_request* request, int32_t graph_id, uint64_t* ticket);

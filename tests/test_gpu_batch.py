@@ -94,3 +94,39 @@ def test_batch_mixed_part_counts_equal_single_calls(gp, ctx):
     alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
     for labels_batched, expect in zip(ctx.partition_batch(jobs, concurrency=12), alone):
         np.testing.assert_array_equal(labels_batched[0], expect)
+
+
+def test_batch_over_devices_equals_single_calls(gp, ctx):
+    """gp_partition_batch_devices places the graphs over the listed devices
+    by longest processing time.  One GPU is listed twice here (two workers'
+    pools on it), so the placement, the per-device queues and the gather run
+    as they would on two GPUs; every result equals the graph alone."""
+    jobs = mixed_graphs(gp)
+    alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
+    out = ctx.partition_batch(jobs, concurrency=3, devices=[0, 0])
+    for (labels, st, run_s), expect in zip(out, alone):
+        np.testing.assert_array_equal(labels, expect)
+
+
+def test_server_over_devices_and_measured_footprint(gp, ctx):
+    """A server over a device list (the one GPU twice) gives the same labels
+    as single calls, and after a resident graph has run its admission
+    estimate comes from the measured device peak of that request."""
+    jobs = mixed_graphs(gp)
+    alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
+    with gp.Server([0, 0], workers=2, hbm_budget_bytes=64 << 30) as server:
+        gid = server.add_graph(jobs[3][0])
+        static = server.footprint(gid, 128)
+        tickets = [server.submit(gid if i == 3 else g, k, eps, seed) for i, (g, k, eps, seed) in enumerate(jobs)]
+        peaks = {}
+        for i, t in enumerate(tickets):
+            labels, st, _, _ = server.wait(t)
+            np.testing.assert_array_equal(labels, alone[i])
+            peaks[i] = st.device_peak_bytes
+        g = jobs[3][0]
+        measured = server.footprint(gid, 128)
+        assert peaks[3] > 0 and measured != static
+        used, cache = peaks[3] + 4 * g.n, 4 * g.n * 128
+        base = used - cache if used > cache else used
+        expected = base + cache + 4 * g.n
+        assert measured == expected + expected // 8
