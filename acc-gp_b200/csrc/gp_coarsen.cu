@@ -1769,6 +1769,7 @@ void build_chunks(Context& ctx, DGraph& g, int heavy_min, Arena* storage) {
     Arena& out = storage ? *storage : ctx.persist;
     g.heavy_min = heavy_min;
     g.heavy = nullptr;
+    g.heavy_chunk0 = nullptr;
     g.heavy_count = 0;
     g.chunks = 0;
     g.heavy_entries = 0;
@@ -1784,8 +1785,9 @@ void build_chunks(Context& ctx, DGraph& g, int heavy_min, Arena* storage) {
     g.chunk_row = out.alloc<int>(g.chunks);
     g.chunk_hidx = out.alloc<int>(g.chunks);
     g.chunk_begin = out.alloc<int>(g.chunks);
+    g.heavy_chunk0 = out.alloc<int>(g.heavy_count);
+    int* chunk_off = g.heavy_chunk0;
     ArenaScope scope(ctx.scratch);
-    int* chunk_off = ctx.scratch.alloc<int>(g.heavy_count);
     select_if(ctx.scratch, s, g.n, IsHeavyRow{g.off, heavy_min}, WriteIndex{g.heavy}, static_cast<u32*>(nullptr));
     exclusive_scan<int>(ctx.scratch, s, g.heavy_count, ChunkCount{g.heavy, g.off}, chunk_off, static_cast<int*>(nullptr));
     launch(k_emit_chunks, blocks_for(g.heavy_count, kThreads), kThreads, 0, s, g.heavy_count, g.heavy, g.off,

@@ -34,6 +34,7 @@ struct DGraph {
     int* chunk_row = nullptr;
     int* chunk_hidx = nullptr;  // index of the chunk's row in `heavy`
     int* chunk_begin = nullptr;
+    int* heavy_chunk0 = nullptr;  // first chunk of each heavy row (chunks of a row are consecutive)
     i64 chunks = 0;
     i64 heavy_entries = 0;  // CSR entries in heavy rows
     int heavy_min = kHeavyRow;  // rows longer than this are the heavy (chunked) rows

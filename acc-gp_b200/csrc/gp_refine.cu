@@ -550,22 +550,29 @@ __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q, const int
 
 // Correction of candidate v (part s to t, gain `gain`) from the entries
 // first, first + stride, ... < end: the moves of its higher-priority
-// neighbours.  Two entries per lane at a time; the neighbour's target, gain
-// and label are gathered together.
+// neighbours.  Four entries per lane at a time: their neighbour ids first,
+// then every neighbour's target, gain and label, all in flight together.
 __device__ __forceinline__ long long filter_entries(const LpParams& q, int v, int s, int t, long long gain, int first,
                                                     int end, int stride) {
+    constexpr int U = 4;
     long long corr = 0;
-    for (int e0 = first; e0 < end; e0 += 2 * stride) {
-        const int e1 = e0 + stride;
-        const int u0 = q.nbr[e0], u1 = e1 < end ? q.nbr[e1] : v;
-        const int t0 = q.targets[u0], l0 = q.labels[u0];
-        const long long g0 = q.gains[u0];
-        const int t1 = u1 != v ? q.targets[u1] : -1, l1 = u1 != v ? q.labels[u1] : 0;
-        const long long g1 = u1 != v ? q.gains[u1] : 0;
-        if (u0 != v && t0 >= 0 && (g0 > gain || (g0 == gain && u0 < v)))
-            corr += static_cast<long long>(edge_w(q.ew, e0)) * ((t0 == t) - (t0 == s) - (l0 == t) + (l0 == s));
-        if (u1 != v && t1 >= 0 && (g1 > gain || (g1 == gain && u1 < v)))
-            corr += static_cast<long long>(edge_w(q.ew, e1)) * ((t1 == t) - (t1 == s) - (l1 == t) + (l1 == s));
+    for (int e0 = first; e0 < end; e0 += U * stride) {
+        int u[U], tu[U], lu[U];
+        long long gu[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) u[j] = e0 + j * stride < end ? q.nbr[e0 + j * stride] : v;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const bool real = u[j] != v;
+            tu[j] = real ? q.targets[u[j]] : -1;
+            lu[j] = real ? q.labels[u[j]] : 0;
+            gu[j] = real ? q.gains[u[j]] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (tu[j] >= 0 && (gu[j] > gain || (gu[j] == gain && u[j] < v)))
+                corr += static_cast<long long>(edge_w(q.ew, e0 + j * stride)) *
+                        ((tu[j] == t) - (tu[j] == s) - (lu[j] == t) + (lu[j] == s));
     }
     return corr;
 }
@@ -575,7 +582,7 @@ __device__ __forceinline__ long long filter_entries(const LpParams& q, int v, in
 // entries are read by eight lanes each, longer ones (up to heavy_min) by the
 // whole warp after them.
 constexpr int kFilterShort = 16;
-__global__ void k_filter(LpParams q) {
+__global__ void __launch_bounds__(kThreads, 6) k_filter(LpParams q) {
     constexpr int W = 8, G = 32 / W;
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
     const i64 count = static_cast<i64>(q.counters[0]);
@@ -715,11 +722,39 @@ __global__ void k_touch_rows(i64 count, const int* movers, const u64* live_count
         for (int e = off[v] + lane; e < off[v + 1]; e += 32) touch(f, nbr[e]);
     }
 }
-// The chunks of heavy rows whose vertex moves (flag set), a block per chunk.
-__global__ void k_touch_chunks(DGraph g, const int* flags, Frontier f) {
-    const int c = blockIdx.x, v = g.chunk_row[c];
-    if (!flags[v]) return;
-    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) touch(f, g.nbr[e]);
+// The chunks of heavy rows of a list (k_heavy_chunk_list) of movers, a block
+// per chunk.
+__global__ void k_touch_chunks(DGraph g, const int* work, const u64* work_count, Frontier f) {
+    const i64 count = static_cast<i64>(*work_count);
+    for (i64 w = blockIdx.x; w < count; w += gridDim.x) {
+        const int c = work[w], v = g.chunk_row[c];
+        for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) touch(f, g.nbr[e]);
+    }
+}
+
+// The chunks of the heavy rows (more than heavy_min entries) among a list of
+// vertices, appended to `work` (at most g.chunks entries; count at
+// *work_count, cleared by the caller), so that the chunk kernels visit the
+// rows that take part in a batch instead of every chunk of the level.  The
+// order of the list does not matter: the chunk kernels only add exact
+// integer contributions.
+__global__ void k_heavy_chunk_list(i64 count, const int* list, const u64* live_count, DGraph g, int* work,
+                                   u64* work_count) {
+    if (live_count) count = static_cast<i64>(*live_count);
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = list[i];
+        const int d = g.off[v + 1] - g.off[v];
+        if (d <= g.heavy_min) continue;
+        i64 lo = 0, hi = g.heavy_count;  // g.heavy is ascending: find v
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if (g.heavy[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        const int c0 = g.heavy_chunk0[lo], chunks = (d + kChunk - 1) / kChunk;
+        const u64 base = atomicAdd(reinterpret_cast<unsigned long long*>(work_count), static_cast<unsigned long long>(chunks));
+        for (int j = 0; j < chunks; ++j) work[base + static_cast<u64>(j)] = c0 + j;
+    }
 }
 // The initial frontier of an on-demand level: rows whose connection to their
 // own part is below their total weight (the proposal's boundary test).
@@ -768,26 +803,21 @@ __global__ void k_reset_targets(i64 count, const u32* donors, int* targets) {
 // Heavy candidates: partial corrections per chunk, then the decision
 // (incremental_heavy_priority / incremental_finish_heavy_priority,
 // incremental.cuh:395-438).
-__global__ void k_filter_chunks(DGraph g, LpParams q, long long* corr_acc) {
-    const int c = blockIdx.x, v = g.chunk_row[c];
-    const int t = q.targets[v];
-    if (t < 0) return;
-    const int s = q.labels[v];
-    const long long gain = q.gains[v];
-    long long corr = 0;
-    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
-        const int u = g.nbr[e];
-        if (u == v) continue;
-        const int tu = q.targets[u];
-        if (tu < 0) continue;
-        const long long gu = q.gains[u];
-        if (!(gu > gain || (gu == gain && u < v))) continue;
-        const int lu = q.labels[u];
-        corr += static_cast<long long>(edge_w(g.ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+__global__ void k_filter_chunks(DGraph g, LpParams q, long long* corr_acc, const int* work, const u64* work_count) {
+    const i64 count = static_cast<i64>(*work_count);
+    for (i64 w = blockIdx.x; w < count; w += gridDim.x) {
+        const int c = work[w], v = g.chunk_row[c];
+        const int t = q.targets[v];
+        if (t < 0) continue;
+        const int s = q.labels[v];
+        const long long gain = q.gains[v];
+        // q.nbr and q.ew are g's arrays: four entries per thread in flight.
+        long long corr = filter_entries(q, v, s, t, gain, g.chunk_begin[c] + static_cast<int>(threadIdx.x),
+                                        chunk_end(g, c, v), static_cast<int>(blockDim.x));
+        corr = warp_sum(corr);
+        if ((threadIdx.x & 31) == 0 && corr)
+            atomicAdd(reinterpret_cast<u64*>(corr_acc + g.chunk_hidx[c]), static_cast<u64>(corr));
     }
-    corr = warp_sum(corr);
-    if ((threadIdx.x & 31) == 0 && corr)
-        atomicAdd(reinterpret_cast<u64*>(corr_acc + g.chunk_hidx[c]), static_cast<u64>(corr));
 }
 __global__ void k_filter_finish(i64 count, const int* heavy, const long long* corr_acc, LpParams q) {
     const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -817,39 +847,52 @@ __global__ void k_compact_movers(LpParams q) {
     }
 }
 
+// Packed per-vertex state read by the cache update: bits 0-7 the label,
+// bits 8-15 the target and bit 16 set while the vertex is in the batch being
+// applied.  One 4-byte gather per neighbour replaces the label, flag and
+// target gathers.  k_state_init writes the labels, k_mark_movers adds the
+// batch's targets and bits, k_commit leaves each mover's new label.
+constexpr u32 kMovingBit = 1u << 16;
+__device__ __forceinline__ int state_label(u32 st) { return static_cast<int>(st & 0xffu); }
+__device__ __forceinline__ int state_next(u32 st) {  // the label after this batch
+    return static_cast<int>((st & kMovingBit) ? (st >> 8) & 0xffu : st & 0xffu);
+}
+
+__global__ void k_state_init(i64 n, const int* labels, u32* state) {
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x)
+        state[v] = static_cast<u32>(labels[v]);
+}
+
 // Cut change and cache updates of the entries first, first + stride, ... <
-// end of mover v (part s to part t); two entries per lane at a time, so that
-// their gathers are in flight together.  An edge whose both ends move is
-// counted by its larger endpoint's partner rule.
+// end of mover v (part s to part t); four entries per lane at a time, their
+// neighbour, weight and state loads all issued before any is used.  An edge
+// whose both ends move is counted by its larger endpoint's partner rule.
 template <class C>
 __device__ __forceinline__ long long update_entries(int v, int s, int t, int first, int end, int stride, const int* nbr,
-                                                    const u32* ew, const int* labels, const int* targets,
-                                                    const int* flags, int k, C* A) {
+                                                    const u32* ew, const u32* state, int k, C* A) {
+    constexpr int U = 4;
     long long gain = 0;
-    for (int e0 = first; e0 < end; e0 += 2 * stride) {
-        const int e1 = e0 + stride;
-        const int u0 = nbr[e0], u1 = e1 < end ? nbr[e1] : v;
-        const int old0 = labels[u0], f0 = flags[u0], t0 = targets[u0];
-        const int old1 = u1 != v ? labels[u1] : 0, f1 = u1 != v ? flags[u1] : 0, t1 = u1 != v ? targets[u1] : 0;
-        if (u0 != v) {
-            const u32 w = edge_w(ew, e0);
-            const bool moves = f0 != 0;
-            const int nw = moves ? t0 : old0;
-            if (A) {  // no cache with on-demand affinities
-                atomicAdd(A + static_cast<i64>(u0) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                atomicAdd(A + static_cast<i64>(u0) * k + t, static_cast<C>(w));
-            }
-            if (!moves || u0 > v) gain += static_cast<long long>(w) * ((s != old0) - (t != nw));
+    for (int e0 = first; e0 < end; e0 += U * stride) {
+        int u[U];
+        u32 w[U], st[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int e = e0 + j * stride;
+            u[j] = e < end ? nbr[e] : v;
+            w[j] = e < end ? edge_w(ew, e) : 0u;
         }
-        if (u1 != v) {
-            const u32 w = edge_w(ew, e1);
-            const bool moves = f1 != 0;
-            const int nw = moves ? t1 : old1;
-            if (A) {
-                atomicAdd(A + static_cast<i64>(u1) * k + s, static_cast<C>(0) - static_cast<C>(w));
-                atomicAdd(A + static_cast<i64>(u1) * k + t, static_cast<C>(w));
+#pragma unroll
+        for (int j = 0; j < U; ++j) st[j] = u[j] != v ? state[u[j]] : 0u;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            if (u[j] == v) continue;  // past the row's end, or a self loop
+            if (A) {  // no cache with on-demand affinities
+                atomicAdd(A + static_cast<i64>(u[j]) * k + s, static_cast<C>(0) - static_cast<C>(w[j]));
+                atomicAdd(A + static_cast<i64>(u[j]) * k + t, static_cast<C>(w[j]));
             }
-            if (!moves || u1 > v) gain += static_cast<long long>(w) * ((s != old1) - (t != nw));
+            const bool moves = (st[j] & kMovingBit) != 0;
+            if (!moves || u[j] > v)
+                gain += static_cast<long long>(w[j]) * ((s != state_label(st[j])) - (t != state_next(st[j])));
         }
     }
     return gain;
@@ -873,10 +916,9 @@ __device__ __forceinline__ u64 update_row_bytes(int entries, bool weighted, bool
 // `work`, the compulsory bytes of the rows it updated are added there.
 constexpr int kUpdateShort = 16;
 template <class C>
-__global__ void k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
-                         const u32* ew, const u32* vw, const int* labels, const int* targets, const int* flags, int k,
-                         C* A, long long* delta, Sample* samples, const u64* gate, u64 threshold, int heavy_min,
-                         u64* work) {
+__global__ void __launch_bounds__(kThreads, 6) k_update(i64 count, const int* movers, const u64* live_count, const int* off, const int* nbr,
+                         const u32* ew, const u32* vw, const u32* state, int k, C* A, long long* delta,
+                         Sample* samples, const u64* gate, u64 threshold, int heavy_min, u64* work) {
     constexpr int W = 8, G = 32 / W;
     __shared__ WarpSum delta_sum;
     const int lane = threadIdx.x & 31, gid = lane / W, sub = lane % W;
@@ -895,9 +937,10 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
         const int begin = v >= 0 ? off[v] : 0, end = v >= 0 ? off[v + 1] : 0;
         const bool light = v >= 0 && end - begin <= heavy_min;  // heavier rows: k_update_chunks
         if (work && sub == 0 && light) bytes += update_row_bytes<C>(end - begin, ew != nullptr, A != nullptr);
-        const int s = light ? labels[v] : 0, t = light ? targets[v] : 0;
+        const u32 sv = light ? state[v] : 0u;
+        const int s = state_label(sv), t = static_cast<int>((sv >> 8) & 0xffu);
         long long gain = light && end - begin <= kUpdateShort
-                             ? update_entries(v, s, t, begin + sub, end, W, nbr, ew, labels, targets, flags, k, A)
+                             ? update_entries(v, s, t, begin + sub, end, W, nbr, ew, state, k, A)
                              : 0;
         for (unsigned rest = __ballot_sync(0xffffffffu, light && end - begin > kUpdateShort) & leaders; rest;
              rest &= rest - 1) {
@@ -905,7 +948,7 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
             const int vv = __shfl_sync(0xffffffffu, v, leader), ss = __shfl_sync(0xffffffffu, s, leader),
                       tt = __shfl_sync(0xffffffffu, t, leader), b = __shfl_sync(0xffffffffu, begin, leader),
                       e = __shfl_sync(0xffffffffu, end, leader);
-            const long long g = warp_sum(update_entries(vv, ss, tt, b + lane, e, 32, nbr, ew, labels, targets, flags, k, A));
+            const long long g = warp_sum(update_entries(vv, ss, tt, b + lane, e, 32, nbr, ew, state, k, A));
             if (lane == leader) gain += g;
         }
 #pragma unroll
@@ -926,46 +969,45 @@ __global__ void k_update(i64 count, const int* movers, const u64* live_count, co
 }
 
 // Heavy movers, chunk-parallel (incremental_heavy_update_cache_and_cut,
-// incremental.cuh:508-530); a row moves when its flag is set.
+// incremental.cuh:508-530): the chunks listed by k_heavy_chunk_list for the
+// batch, a block per chunk, each thread with four entries' loads in flight.
 template <class C>
-__global__ void k_update_chunks(DGraph g, const int* labels, const int* targets, const int* flags, int k, C* A,
+__global__ void k_update_chunks(DGraph g, const int* chunk_list, const u64* chunk_count, const u32* state, int k, C* A,
                                 long long* delta, Sample* samples, const u64* gate, u64 threshold, u64* work) {
     if (gate && *gate > threshold) return;
-    const int c = blockIdx.x, v = g.chunk_row[c];
-    if (!flags[v]) return;
-    if (work && threadIdx.x == 0)  // the chunk's entries, its row, begin and row id (no per-row mover id)
-        atomicAdd(reinterpret_cast<unsigned long long*>(work),
-                  update_row_bytes<C>(chunk_end(g, c, v) - g.chunk_begin[c], g.ew != nullptr, true) - 8ULL);
-    const int s = labels[v], t = targets[v];
-    long long gain = 0;
-    for (int e = g.chunk_begin[c] + threadIdx.x; e < chunk_end(g, c, v); e += blockDim.x) {
-        const int u = g.nbr[e];
-        if (u == v) continue;
-        const int old = labels[u];
-        const bool moves = flags[u] != 0;
-        const int nw = moves ? targets[u] : old;
-        const u32 w = edge_w(g.ew, e);
-        atomicAdd(A + static_cast<i64>(u) * k + s, static_cast<C>(0) - static_cast<C>(w));
-        atomicAdd(A + static_cast<i64>(u) * k + t, static_cast<C>(w));
-        if (!moves || u > v) gain += static_cast<long long>(w) * ((s != old) - (t != nw));
+    const i64 count = static_cast<i64>(*chunk_count);
+    for (i64 w = blockIdx.x; w < count; w += gridDim.x) {
+        const int c = chunk_list[w], v = g.chunk_row[c];
+        const u32 sv = state[v];
+        if (work && threadIdx.x == 0)  // the chunk's entries, its row, begin and row id (no per-row mover id)
+            atomicAdd(reinterpret_cast<unsigned long long*>(work),
+                      update_row_bytes<C>(chunk_end(g, c, v) - g.chunk_begin[c], g.ew != nullptr, true) - 8ULL);
+        const int s = state_label(sv), t = static_cast<int>((sv >> 8) & 0xffu);
+        long long gain = update_entries(v, s, t, g.chunk_begin[c] + static_cast<int>(threadIdx.x), chunk_end(g, c, v),
+                                        static_cast<int>(blockDim.x), g.nbr, g.ew, state, k, A);
+        gain = block_sum(gain);
+        if (threadIdx.x == 0 && gain) {
+            atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(gain));
+            if (samples) atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
+        }
+        if (samples && threadIdx.x == 0 && g.chunk_begin[c] == g.off[v])
+            atomicAdd(&samples[s].weight, static_cast<u64>(g.vw[v]));
     }
-    gain = block_sum(gain);
-    if (threadIdx.x == 0 && gain) {
-        atomicAdd(reinterpret_cast<u64*>(delta), static_cast<u64>(gain));
-        if (samples) atomicAdd(reinterpret_cast<u64*>(&samples[s].loss), static_cast<u64>(-gain));
-    }
-    if (samples && threadIdx.x == 0 && g.chunk_begin[c] == g.off[v])
-        atomicAdd(&samples[s].weight, static_cast<u64>(g.vw[v]));
 }
 
 // Entries of the rows of a mover list: decides between updating the cache
 // entry by entry and rebuilding it after the commit.
-__global__ void k_mover_entries(i64 count, const int* movers, const u64* live_count, const int* off, u64* out) {
+// Also marks the batch in the packed state (target and batch bit).
+__global__ void k_mark_movers(i64 count, const int* movers, const u64* live_count, const int* off, const int* targets,
+                              u32* state, u64* out) {
     if (live_count) count = static_cast<i64>(*live_count);
     u64 entries = 0;
-    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x)
-        entries += static_cast<u64>(off[movers[i] + 1] - off[movers[i]]);
-    block_atomic_add(out, entries);
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const int v = movers[i];
+        if (state) state[v] = (state[v] & 0xffu) | (static_cast<u32>(targets[v] & 0xff) << 8) | kMovingBit;
+        if (out) entries += static_cast<u64>(off[v + 1] - off[v]);
+    }
+    if (out) block_atomic_add(out, entries);
 }
 
 // incremental_commit (incremental.cuh:532-547) with per-block aggregation of
@@ -974,7 +1016,7 @@ __global__ void k_mover_entries(i64 count, const int* movers, const u64* live_co
 // v) current.
 __global__ void k_commit(i64 count, const int* movers, const u64* live_count, int* labels, const int* targets,
                          const u32* vw, int k, u64* loads, unsigned char* locks, int* flags, const u32* rposition,
-                         int* rlabels) {
+                         int* rlabels, u32* state) {
     extern __shared__ long long diff[];
     if (live_count) count = static_cast<i64>(*live_count);
     for (int p = threadIdx.x; p < k; p += blockDim.x) diff[p] = 0;
@@ -987,6 +1029,7 @@ __global__ void k_commit(i64 count, const int* movers, const u64* live_count, in
         atomicAdd(reinterpret_cast<u64*>(diff + t), static_cast<u64>(w));
         labels[v] = t;
         rlabels[rposition[v]] = t;
+        if (state) state[v] = static_cast<u32>(t);
         if (locks) locks[v] = 1;
     }
     __syncthreads();
@@ -2190,6 +2233,9 @@ private:
     u32* rorder = nullptr;
     u32* rposition = nullptr;  // place of each vertex in the repair order
     int* rlabels = nullptr;    // labels in repair order
+    u32* state = nullptr;      // packed label / target / batch bit per vertex (dense-cache levels)
+    int* chunk_work = nullptr;      // chunks of the heavy rows taking part in a batch (k_heavy_chunk_list)
+    u64* chunk_work_count = nullptr;
     u64* counters = nullptr;  // device: 0 cand, 1 movers, 2 delta, 3 max load, 4.. scratch
     long long* corr_acc = nullptr;  // per heavy row: priority-filter correction
     u64 cut = 0, revision = 0;
@@ -2204,6 +2250,16 @@ private:
 
     cudaStream_t s() const { return ctx.stream; }
     int grid_for(i64 items, int per_block) const { return static_cast<int>(std::min<i64>(blocks_for(items, per_block), 148 * 32)); }
+    // Blocks of the list-driven chunk kernels: enough to fill the GPU, never
+    // more than there are chunks.
+    int chunk_grid() const { return static_cast<int>(std::min<i64>(g.chunks, 148 * 16)); }
+    // The chunks of the heavy rows among `list` (count at `live`, or
+    // host_count) into chunk_work.
+    void list_heavy_chunks(const int* list, const u64* live, i64 host_count) {
+        GP_CUDA(cudaMemsetAsync(chunk_work_count, 0, sizeof(u64), s()));
+        launch(k_heavy_chunk_list, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g,
+               chunk_work, chunk_work_count);
+    }
 
     // Rebuilds the cache and row totals from the labels; with directed_cut
     // also sums the directed cut (device counter, cleared by the caller).
@@ -2260,9 +2316,9 @@ private:
         GP_CUDA(cudaMemsetAsync(counters + 6, 0, 2 * sizeof(u64), s()));
         const u64* gate = sample || on_demand ? nullptr : counters + 6;
         const u64 threshold = gate ? rebuild_entries : ~0ULL;
-        if (gate)
-            launch(k_mover_entries, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
-                   counters + 6);
+        if (gate || state)
+            launch(k_mark_movers, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
+                   static_cast<const int*>(targets), state, gate ? counters + 6 : static_cast<u64*>(nullptr));
         if (on_demand)
             with_row_size([&](auto d) {
                 launch(k_update_od<decltype(d)::value>, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list,
@@ -2273,22 +2329,25 @@ private:
             });
         else
             launch(k_update<T>, grid_for(host_count * 8, kThreads), kThreads, 0, s(), host_count, list, live, g.off, g.nbr,
-                   g.ew, g.vw, labels, targets, flags, k, A, reinterpret_cast<long long*>(counters + 2),
+                   g.ew, g.vw, static_cast<const u32*>(state), k, A, reinterpret_cast<long long*>(counters + 2),
                    sample ? samples : static_cast<Sample*>(nullptr), gate, threshold, g.heavy_min,
                    work_counter(k_update<T>));
-        if (g.chunks)
-            launch(k_update_chunks<T>, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(labels),
-                   static_cast<const int*>(targets), static_cast<const int*>(flags), k, A,
+        if (g.chunks) {
+            list_heavy_chunks(list, live, host_count);
+            launch(k_update_chunks<T>, chunk_grid(), 256, 0, s(), g, static_cast<const int*>(chunk_work),
+                   static_cast<const u64*>(chunk_work_count), static_cast<const u32*>(state), k, A,
                    reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr), gate,
                    threshold, work_counter(k_update_chunks<T>));
+        }
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags,
-               static_cast<const u32*>(rposition), rlabels);
+               static_cast<const u32*>(rposition), rlabels, state);
         if (frontier_on) {
             launch(k_touch_rows, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    g.nbr, g.heavy_min, frontier);
-            if (g.chunks)
-                launch(k_touch_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, static_cast<const int*>(flags), frontier);
+            if (g.chunks)  // the heavy movers' chunks listed for the update above
+                launch(k_touch_chunks, chunk_grid(), 256, 0, s(), g, static_cast<const int*>(chunk_work),
+                       static_cast<const u64*>(chunk_work_count), frontier);
         }
         launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
         if (gate) build(counters + 7, gate, threshold);
@@ -2383,7 +2442,9 @@ i64 LevelRefiner<T>::lp_round(double filter) {
         launch(k_filter, grid_for(n * 8, kThreads), kThreads, 0, s(), q);
     if (g.chunks) {
         GP_CUDA(cudaMemsetAsync(corr_acc, 0, sizeof(long long) * g.heavy_count, s()));
-        launch(k_filter_chunks, static_cast<int>(g.chunks), 256, 0, s(), g, q, corr_acc);
+        list_heavy_chunks(cand, counters, n);
+        launch(k_filter_chunks, chunk_grid(), 256, 0, s(), g, q, corr_acc, static_cast<const int*>(chunk_work),
+               static_cast<const u64*>(chunk_work_count));
         launch(k_filter_finish, blocks_for(g.heavy_count, kThreads), kThreads, 0, s(), g.heavy_count,
                static_cast<const int*>(g.heavy), static_cast<const long long*>(corr_acc), q);
     }
@@ -2735,6 +2796,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     movers = A_.alloc<int>(n);
     counters = A_.alloc<u64>(8);
     corr_acc = A_.alloc<long long>(g.heavy_count + 1);
+    if (g.chunks) {
+        chunk_work = A_.alloc<int>(g.chunks);
+        chunk_work_count = A_.alloc<u64>(1);
+    }
     int* saved_labels = A_.alloc<int>(n);
     u64* saved_loads = A_.alloc<u64>(k);
     GP_CUDA(cudaMemsetAsync(locks, 0, n, s()));
@@ -2764,6 +2829,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     rebuild_entries = (static_cast<u64>(n) * k * sizeof(T) + 8ULL * static_cast<u64>(g.m)) /
                       static_cast<u64>(std::max(1, mapping.rebuild_divisor));
     GP_CUDA(cudaMemsetAsync(counters + 7, 0, sizeof(u64), s()));
+    if (!on_demand) {
+        state = A_.alloc<u32>(n);
+        launch(k_state_init, grid_for(n, kThreads), kThreads, 0, s(), n, static_cast<const int*>(labels), state);
+    }
     build(has_known ? nullptr : counters + 7);
     launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 3, 5 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
@@ -2843,6 +2912,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     const bool restored = revision != best_revision;
     if (restored) {
         GP_CUDA(cudaMemcpyAsync(labels, saved_labels, sizeof(int) * n, cudaMemcpyDeviceToDevice, s()));
+        if (state)
+            launch(k_state_init, grid_for(n, kThreads), kThreads, 0, s(), n, static_cast<const int*>(labels), state);
         launch(k_repair_positions, blocks_for(n, kThreads), kThreads, 0, s(), n, static_cast<const u32*>(rorder),
                static_cast<const int*>(labels), rposition, rlabels);
         GP_CUDA(cudaMemcpyAsync(loads, saved_loads, sizeof(u64) * k, cudaMemcpyDeviceToDevice, s()));
