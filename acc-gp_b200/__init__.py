@@ -61,7 +61,7 @@ class _Stats(_C.Structure):
                 ("uncoarsen_seconds", _C.c_double), ("algorithm_seconds", _C.c_double),
                 ("h2d_seconds", _C.c_double), ("d2h_seconds", _C.c_double),
                 ("kernel_launches", _C.c_uint64), ("algorithmic_bytes", _C.c_uint64),
-                ("device_peak_bytes", _C.c_uint64)]
+                ("device_peak_bytes", _C.c_uint64), ("hierarchy_reused", _C.c_uint32), ("reserved", _C.c_uint32)]
 
 
 class _RefineStats(_C.Structure):
@@ -300,10 +300,11 @@ class Stats:
     kernel_launches: int
     algorithmic_bytes: int
     device_peak_bytes: int = 0
+    hierarchy_reused: int = 0
 
     @classmethod
     def _from(cls, s: _Stats) -> "Stats":
-        return cls(**{name: getattr(s, name) for name, _ in _Stats._fields_})
+        return cls(**{name: getattr(s, name) for name, _ in _Stats._fields_ if name != "reserved"})
 
 
 class Context:
@@ -534,6 +535,16 @@ class Server:
             _check(self._lib.gp_server_create(_C.c_int(device), _C.c_int32(workers), _C.c_uint64(hbm_budget_bytes),
                                               _C.byref(self._handle)))
         self._graphs = []
+
+    def keep_hierarchies(self, bytes_per_device: int) -> None:
+        """gp_server_keep_hierarchies: keep coarsened hierarchies of resident
+        graphs (per graph, k, seed) for later requests, within this budget."""
+        _check(self._lib.gp_server_keep_hierarchies(self._handle, _C.c_uint64(bytes_per_device)))
+
+    def kept_bytes(self) -> int:
+        out = _C.c_uint64()
+        _check(self._lib.gp_server_kept_bytes(self._handle, _C.byref(out)))
+        return out.value
 
     def footprint(self, graph_id: int, k: int) -> int:
         """gp_server_footprint: the admission estimate of a request, in bytes."""

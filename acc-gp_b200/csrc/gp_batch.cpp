@@ -198,6 +198,7 @@ struct gp_server {
         bool done = false;
     };
     std::vector<int> devices;
+    std::vector<HierarchyCache*> caches;  // per device index; empty until gp_server_keep_hierarchies
     uint64_t budget = 0;            // per device
     std::vector<uint64_t> in_use;   // per device index
     bool stopping = false;
@@ -285,7 +286,11 @@ struct gp_server {
                 }
                 if (r.status == GP_OK) {
                     const gp_csr dg{gn, gm, arrays.off, arrays.nbr, arrays.vw, arrays.ew};
-                    r.status = gp_partition_device(c, &dg, r.k, r.epsilon, r.seed, r.flags, labels_dev, nullptr, &r.stats);
+                    HierarchyCache* cache = caches.empty() ? nullptr : caches[static_cast<size_t>(d)];
+                    r.status = cache ? partition_resident(c, cache, static_cast<uint64_t>(job.graph), &dg, r.k, r.epsilon,
+                                                          r.seed, r.flags, labels_dev, &r.stats)
+                                     : gp_partition_device(c, &dg, r.k, r.epsilon, r.seed, r.flags, labels_dev, nullptr,
+                                                           &r.stats);
                 }
                 if (r.status == GP_OK &&
                     cudaMemcpy(r.labels_out, labels_dev, sizeof(int32_t) * static_cast<size_t>(gn),
@@ -397,6 +402,26 @@ extern "C" gp_status gp_server_add_graph(gp_server* server, const gp_csr* graph,
     return GP_OK;
 }
 
+extern "C" gp_status gp_server_keep_hierarchies(gp_server* server, uint64_t bytes_per_device) {
+    if (!server) { set_error("server is NULL"); return GP_INVALID_ARGUMENT; }
+    std::lock_guard<std::mutex> lock(server->mu);
+    if (!server->caches.empty() || !server->jobs.empty()) {
+        set_error("set the hierarchy budget once, before the first request");
+        return GP_INVALID_ARGUMENT;
+    }
+    if (!bytes_per_device) return GP_OK;
+    for (int device : server->devices) server->caches.push_back(hierarchy_cache_create(device, bytes_per_device));
+    return GP_OK;
+}
+
+extern "C" gp_status gp_server_kept_bytes(gp_server* server, uint64_t* bytes) {
+    if (!server || !bytes) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
+    uint64_t total = 0;
+    for (HierarchyCache* c : server->caches) total += hierarchy_cache_bytes(c);
+    *bytes = total;
+    return GP_OK;
+}
+
 extern "C" gp_status gp_server_footprint(gp_server* server, int32_t graph_id, int32_t k, uint64_t* bytes) {
     if (!server || !bytes) { set_error("NULL argument"); return GP_INVALID_ARGUMENT; }
     std::lock_guard<std::mutex> lock(server->mu);
@@ -463,6 +488,7 @@ extern "C" void gp_server_destroy(gp_server* server) {
     server->work_cv.notify_all();
     for (auto& t : server->threads) t.join();
     for (gp_context* c : server->contexts) gp_context_destroy(c);
+    for (HierarchyCache* c : server->caches) hierarchy_cache_destroy(c);
     for (auto& g : server->graphs)
         for (size_t d = 0; d < g.on.size(); ++d) {
             cudaSetDevice(server->devices[d]);

@@ -143,6 +143,13 @@ public:
         return c.base;
     }
     void set_chunk_bytes(size_t b) { chunk_bytes_ = b; }
+    // Exchanges the whole state (chunks included) with another arena.
+    void swap(Arena& o) noexcept {
+        chunks_.swap(o.chunks_);
+        std::swap(current_, o.current_);
+        std::swap(chunk_bytes_, o.chunk_bytes_);
+        std::swap(peak_, o.peak_);
+    }
     size_t reserved() const { size_t s = 0; for (auto& c : chunks_) s += c.size; return s; }
     // Largest number of bytes held at once since reset_peak() (the measured
     // footprint of the work in between).

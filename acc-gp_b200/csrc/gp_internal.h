@@ -25,4 +25,19 @@ size_t context_reserved(const gp_context* ctx);
 void context_trim(gp_context* ctx);
 void copy_options(const gp_context* from, gp_context* to);
 
+// Coarsened hierarchies of resident graphs kept on one device for later
+// requests (gp_partition.cu).  A hierarchy depends on the graph, k, the
+// seed and the coarsening options, not on epsilon, so requests that differ
+// only in epsilon (or repeat) reuse it.  Least recently used unreferenced
+// hierarchies are dropped beyond `budget_bytes`.
+struct HierarchyCache;
+HierarchyCache* hierarchy_cache_create(int device, uint64_t budget_bytes);
+void hierarchy_cache_destroy(HierarchyCache* cache);
+uint64_t hierarchy_cache_bytes(const HierarchyCache* cache);
+// gp_partition_device of a resident graph (graph_key names it) through the
+// cache; stats->hierarchy_reused tells whether the hierarchy came from it.
+gp_status partition_resident(gp_context* ctx, HierarchyCache* cache, uint64_t graph_key, const gp_csr* device_graph,
+                             int32_t k, double epsilon, uint32_t seed, uint32_t flags, int32_t* labels_device,
+                             gp_stats* stats);
+
 }  // namespace gp

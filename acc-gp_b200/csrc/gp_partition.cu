@@ -12,8 +12,12 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
+#include <tuple>
 
 struct gp_context {
     gp::Context ctx;
@@ -262,8 +266,90 @@ Input prepare_input(Context& ctx, const gp_csr* in, bool device_input) {
     return out;
 }
 
+}  // namespace
+
+// Kept hierarchies of resident graphs (see gp_internal.h).  An entry owns the
+// arena its levels live in; entries in use by a call are never dropped.
+struct HierarchyCache {
+    struct Key {
+        uint64_t graph;
+        int k;
+        uint32_t seed, flags;
+        bool operator<(const Key& o) const {
+            return std::tie(graph, k, seed, flags) < std::tie(o.graph, o.k, o.seed, o.flags);
+        }
+    };
+    struct Entry {
+        Arena storage;
+        Hierarchy h;
+        u64 total = 0, directed = 0;
+        int users = 0;
+        u64 last_use = 0;
+    };
+    int device = 0;
+    uint64_t budget = 0;
+    std::mutex mu;
+    std::map<Key, std::unique_ptr<Entry>> entries;
+    u64 clock = 0;
+
+    Entry* find(const Key& key) {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = entries.find(key);
+        if (it == entries.end()) return nullptr;
+        ++it->second->users;
+        it->second->last_use = ++clock;
+        return it->second.get();
+    }
+    // Keeps a complete `fresh` entry, in use by the caller, and drops least
+    // recently used idle entries while the total exceeds the budget.  When
+    // another call kept the same key first, `fresh` is still the caller's
+    // and is freed at its release.  Returns the caller's entry.
+    Entry* insert(const Key& key, std::unique_ptr<Entry> fresh) {
+        std::lock_guard<std::mutex> lock(mu);
+        fresh->users = 1;
+        fresh->last_use = ++clock;
+        Entry* out = fresh.get();
+        if (entries.count(key)) retired.push_back(std::move(fresh));
+        else entries.emplace(key, std::move(fresh));
+        evict();
+        return out;
+    }
+    void release(Entry* e) {
+        std::lock_guard<std::mutex> lock(mu);
+        --e->users;
+        evict();
+        free_retired();
+    }
+    uint64_t bytes() const {
+        uint64_t b = 0;
+        for (auto& kv : entries) b += kv.second->storage.reserved();
+        return b;
+    }
+
+private:
+    std::vector<std::unique_ptr<Entry>> retired;  // duplicates, freed once idle
+    void evict() {
+        while (bytes() > budget) {
+            auto victim = entries.end();
+            for (auto it = entries.begin(); it != entries.end(); ++it)
+                if (!it->second->users && (victim == entries.end() || it->second->last_use < victim->second->last_use))
+                    victim = it;
+            if (victim == entries.end()) break;  // everything is in use
+            cudaSetDevice(device);
+            entries.erase(victim);
+        }
+    }
+    void free_retired() {
+        for (auto& e : retired) if (e && !e->users) { cudaSetDevice(device); e.reset(); }
+        retired.erase(std::remove(retired.begin(), retired.end(), nullptr), retired.end());
+    }
+};
+
+namespace {
+
 gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, double eps, uint32_t seed,
-              uint32_t flags, int* labels_out, void* user_stream, gp_stats* stats) {
+              uint32_t flags, int* labels_out, void* user_stream, gp_stats* stats, HierarchyCache* cache = nullptr,
+              uint64_t graph_key = 0) {
     Context& ctx = handle->ctx;
     if (!in || !labels_out) fail(GP_INVALID_ARGUMENT, "graph and labels must not be NULL");
     if (k < 2 || k > kMaxParts || !std::isfinite(eps) || eps < 1.0) fail(GP_INVALID_ARGUMENT, "invalid partition capacity options");
@@ -281,7 +367,41 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     ctx.persist.reset_peak();
     ctx.scratch.reset_peak();
     const i64 n = in->n;
-    Input input = prepare_input(ctx, in, device_input);
+    // A kept hierarchy of a resident graph, or a fresh one.
+    HierarchyCache::Entry* kept = nullptr;
+    struct Release {
+        HierarchyCache* cache;
+        HierarchyCache::Entry*& entry;
+        ~Release() { if (cache && entry) cache->release(entry); }
+    } release{cache, kept};
+    const HierarchyCache::Key key{graph_key, k, seed, flags & GP_FLAG_NO_SEED_MATCHING};
+    if (cache) kept = cache->find(key);
+    Input input;
+    const bool reused = kept != nullptr;
+    // On a miss with a cache, the input's own arrays (unit vertex weights) and
+    // the levels go to a new entry's arena: it stands in for the persist
+    // arena until the hierarchy is complete.
+    std::unique_ptr<HierarchyCache::Entry> fresh;
+    struct Borrow {
+        Arena& persist;
+        Arena* lent = nullptr;
+        void end() { if (lent) persist.swap(*lent); lent = nullptr; }
+        ~Borrow() { end(); }
+    } borrow{ctx.persist};
+    if (reused) {  // validated and measured when it was kept
+        GP_CUDA(cudaEventRecord(ctx.ev[0], s));
+        GP_CUDA(cudaEventRecord(ctx.ev[1], s));
+        input.g = kept->h.levels.front();
+        input.total = kept->total;
+        input.directed = kept->directed;
+    } else {
+        if (cache) {
+            fresh = std::make_unique<HierarchyCache::Entry>();
+            ctx.persist.swap(fresh->storage);
+            borrow.lent = &fresh->storage;
+        }
+        input = prepare_input(ctx, in, device_input);
+    }
     DGraph& g = input.g;
     const u64 total = input.total, directed = input.directed;
     uint64_t capacity = 0;
@@ -305,8 +425,15 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
     o.mapping = handle->mapping;
     // --verify: the input must be bidirectional with equal reverse weights
     // (validate_weighted_csr, src/graph.cpp:157-182).
-    if (o.verify) verify_csr(ctx, g, true, GP_INVALID_ARGUMENT);
-    Hierarchy h = coarsen(ctx, g, o);
+    if (o.verify && !reused) verify_csr(ctx, g, true, GP_INVALID_ARGUMENT);
+    Hierarchy h = reused ? kept->h : coarsen(ctx, g, o);
+    if (fresh) {  // the entry is complete: the persist arena is the call's own again
+        borrow.end();
+        fresh->h = h;
+        fresh->total = total;
+        fresh->directed = directed;
+        kept = cache->insert(key, std::move(fresh));
+    }
     GP_CUDA(cudaEventRecord(ctx.ev[2], s));
     if (flags & GP_FLAG_KEEP_HIERARCHY) keep_levels(ctx, h);
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -355,6 +482,7 @@ gp_status run(gp_context* handle, const gp_csr* in, bool device_input, int k, do
         stats->kernel_launches = g_launches - launches0;
         stats->algorithmic_bytes = algorithmic_bytes(h);
         stats->device_peak_bytes = ctx.persist.peak() + ctx.scratch.peak();
+        stats->hierarchy_reused = reused ? 1u : 0u;
     }
     return GP_OK;
 }
@@ -451,6 +579,32 @@ gp_status guarded(F&& f) {
 
 namespace gp {
 Context& context_of(gp_context* ctx) { return ctx->ctx; }
+
+HierarchyCache* hierarchy_cache_create(int device, uint64_t budget_bytes) {
+    auto* c = new HierarchyCache;
+    c->device = device;
+    c->budget = budget_bytes;
+    return c;
+}
+void hierarchy_cache_destroy(HierarchyCache* cache) {
+    if (!cache) return;
+    cudaSetDevice(cache->device);
+    delete cache;
+}
+uint64_t hierarchy_cache_bytes(const HierarchyCache* cache) {
+    if (!cache) return 0;
+    auto* c = const_cast<HierarchyCache*>(cache);
+    std::lock_guard<std::mutex> lock(c->mu);
+    return c->bytes();
+}
+gp_status partition_resident(gp_context* ctx, HierarchyCache* cache, uint64_t graph_key, const gp_csr* device_graph,
+                             int32_t k, double epsilon, uint32_t seed, uint32_t flags, int32_t* labels_device,
+                             gp_stats* stats) {
+    if (!ctx) { set_error("context is NULL"); return GP_INVALID_ARGUMENT; }
+    return guarded([&] {
+        return run(ctx, device_graph, true, k, epsilon, seed, flags, labels_device, nullptr, stats, cache, graph_key);
+    });
+}
 }  // namespace gp
 
 using namespace gp;

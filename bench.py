@@ -564,7 +564,10 @@ def serving_form(gp, rate, requests, workers, pool_graphs, budget_gb, saturation
     capacity cannot hold the graph), epsilon in {1.01, 1.03, 1.05} and a
     seed.  Reports p50/p99 latency (submit -> labels in host memory) and
     throughput; a sample of results is checked against the same request
-    partitioned alone.  With saturation_requests, that many more requests are
+    partitioned alone.  The stream's (graph, k, seed) rarely repeats, so
+    hierarchies are not kept there; what keeping one saves is measured
+    apart, on the largest pool graph: a request, then the same request at
+    another epsilon reusing its kept hierarchy.  With saturation_requests, that many more requests are
     submitted at once afterwards: their completion rate is the server's
     saturation throughput."""
     import numpy as np
@@ -627,10 +630,28 @@ def serving_form(gp, rate, requests, workers, pool_graphs, budget_gb, saturation
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "throughput_req_s": len(reqs) / wall, "offered_rate_req_s": rate, "requests": len(reqs),
             "saturation_req_s": saturation, "workers": workers, "pool_graphs": len(pool),
+            "kept_hierarchy": kept_hierarchy(gp, max(pool, key=lambda g: g.m)),
             "pool_vertices": [int(g.n) for g in pool], "sample_identical_to_alone": same,
             "workload": "serving_poisson: resident R-MAT pool (n 1e4..4e6, weighted), k uniform 2..128, "
                         "eps in {1.01, 1.03, 1.05}; the survey's 200 req/s exceeds one B200, so the latency "
                         "phase offers a rate below saturation and saturation is measured separately"}
+
+
+def kept_hierarchy(gp, g, k=64, seed=0):
+    """Run time of a resident-graph request that coarsens, then of the same
+    (graph, k, seed) at another epsilon reusing the kept hierarchy (labels
+    checked against the request alone)."""
+    with gp.Server(0, workers=1) as server:
+        server.keep_hierarchies(16 << 30)
+        gid = server.add_graph(g)
+        server.wait(server.submit(gid, k, 1.03, seed + 1))  # warm the worker
+        _, first, _, fresh_s = server.wait(server.submit(gid, k, 1.03, seed))
+        labels, second, _, reused_s = server.wait(server.submit(gid, k, 1.05, seed))
+    with gp.Context(0) as ctx:
+        alone, _ = ctx.partition(g, k, 1.05, seed)
+    return {"graph_vertices": int(g.n), "graph_entries": int(g.m), "k": k, "fresh_ms": fresh_s * 1e3,
+            "reused_ms": reused_s * 1e3, "reused": bool(second.hierarchy_reused and not first.hierarchy_reused),
+            "identical_to_alone": bool((labels == alone).all())}
 
 
 def run_serving(args):

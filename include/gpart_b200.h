@@ -78,6 +78,8 @@ typedef struct gp_stats {
     uint64_t algorithmic_bytes;   /* compulsory HBM traffic model of the V-cycle     */
     uint64_t device_peak_bytes;   /* most device memory the call held at once in the
                                      context's arenas (its measured footprint)       */
+    uint32_t hierarchy_reused;    /* 1: a server request reused a kept hierarchy      */
+    uint32_t reserved;
 } gp_stats;
 
 /* Flags for gp_partition / gp_partition_device. */
@@ -268,6 +270,17 @@ gp_status gp_server_add_graph(gp_server* server, const gp_csr* graph, int32_t* g
 /* The admission estimate, in bytes, of a request of part count k on a
  * resident graph. */
 gp_status gp_server_footprint(gp_server* server, int32_t graph_id, int32_t k, uint64_t* bytes);
+/* Keeps the coarsened hierarchies of resident graphs on the device, up to
+ * bytes_per_device on each device of the server (0: none, the default).  A
+ * hierarchy depends on the graph, k, the seed and GP_FLAG_NO_SEED_MATCHING,
+ * not on epsilon, so a later request with the same four skips coarsening
+ * (stats.hierarchy_reused = 1) and yields exactly the labels a fresh call
+ * would.  Least recently used hierarchies not in use by a request are
+ * dropped beyond the budget, which is separate from hbm_budget_bytes.  Call
+ * once, before the first request. */
+gp_status gp_server_keep_hierarchies(gp_server* server, uint64_t bytes_per_device);
+/* Device bytes the kept hierarchies hold, summed over the devices. */
+gp_status gp_server_kept_bytes(gp_server* server, uint64_t* bytes);
 /* Queues a request (graph_id -1: request->graph is a host CSR).  The request
  * and its buffers must stay valid until gp_server_wait returns for it. */
 gp_status gp_server_submit(gp_server* server, gp_request* request, int32_t graph_id, uint64_t* ticket);

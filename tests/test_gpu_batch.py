@@ -130,3 +130,33 @@ def test_server_over_devices_and_measured_footprint(gp, ctx):
         base = used - cache if used > cache else used
         expected = base + cache + 4 * g.n
         assert measured == expected + expected // 8
+
+
+def test_server_keeps_hierarchies(gp, ctx):
+    """With kept hierarchies, a request that repeats a resident graph's
+    (k, seed) skips coarsening and still returns exactly the labels of the
+    request alone, whatever its epsilon; a different k or seed coarsens anew.
+    The unit-weight grid checks that the vertex weights the first request
+    materialised live with the kept hierarchy.  A one-byte budget keeps
+    nothing once the request that made a hierarchy is done."""
+    weighted = gp.with_weights(gp.rmat(15, 12, 0.57, 0.19, 0.19, 21), 3, (1, 8), (1, 20))
+    grid = gp.grid2d(200, 150)
+    plan = [(weighted, 32, 1.03, 5), (weighted, 32, 1.05, 5), (weighted, 32, 1.03, 5), (weighted, 16, 1.03, 5),
+            (weighted, 32, 1.03, 6), (grid, 8, 1.03, 0), (grid, 8, 1.01, 0)]
+    expect_reused = [0, 1, 1, 0, 0, 0, 1]
+    alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in plan]
+    with gp.Server(0, workers=2) as server:
+        server.keep_hierarchies(8 << 30)
+        ids = {id(weighted): server.add_graph(weighted), id(grid): server.add_graph(grid)}
+        for (g, k, eps, seed), expect, reused in zip(plan, alone, expect_reused):
+            labels, st, _, _ = server.wait(server.submit(ids[id(g)], k, eps, seed))
+            np.testing.assert_array_equal(labels, expect)
+            assert st.hierarchy_reused == reused
+        assert server.kept_bytes() > 0
+    with gp.Server(0, workers=1) as server:
+        server.keep_hierarchies(1)
+        gid = server.add_graph(weighted)
+        for eps in (1.03, 1.05):
+            labels, st, _, _ = server.wait(server.submit(gid, 32, eps, 5))
+            assert st.hierarchy_reused == 0
+        assert server.kept_bytes() == 0
