@@ -1191,6 +1191,8 @@ constexpr size_t kBigSortSmem = sizeof(int) * kBigSortRow * 2 + sizeof(u32) * (k
 
 // Rows above 8192 raw entries: records (row rank, target) -> global radix
 // sort.  Flat over records; the row of a record is found by binary search.
+// With vals == nullptr the record's weight rides in the low 32 bits of its
+// key word (key << 32 | weight), so the sort moves one 8-byte word per record.
 __global__ void k_large_records(i64 records, i64 count, const int* rows, const int* raw_off, const int* rec_off,
                                 const int* raw_t, const u32* raw_w, int tbits, u64* keys, u32* vals) {
     const u64 sentinel = (1ULL << tbits) - 1;
@@ -1201,8 +1203,13 @@ __global__ void k_large_records(i64 records, i64 count, const int* rows, const i
         const int j = lo;
         const int pos = raw_off[rows[j]] + static_cast<int>(r - rec_off[j]);
         const int t = raw_t[pos];
-        keys[r] = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
-        vals[r] = raw_w[pos];
+        const u64 key = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
+        if (vals) {
+            keys[r] = key;
+            vals[r] = raw_w[pos];
+        } else {
+            keys[r] = (key << 32) | raw_w[pos];
+        }
     }
 }
 struct LargeRowSize {
@@ -1215,25 +1222,29 @@ struct UniqueCount {
     i64 nc;
     __device__ int operator()(i64 i) const { return i < nc ? ucount[i] : 0; }
 };
+// Records are (key, weight) pairs, or packed key << 32 | weight words when
+// shift is 32 (vals unused).
 struct RecordHead {
     const u64* keys;
     u64 sentinel_mask;
+    int shift;
     __device__ u32 operator()(i64 i) const {
-        const u64 k = keys[i];
+        const u64 k = keys[i] >> shift;
         if ((k & sentinel_mask) == sentinel_mask) return 0;
-        return (i == 0 || keys[i - 1] != k) ? 1u : 0u;
+        return (i == 0 || (keys[i - 1] >> shift) != k) ? 1u : 0u;
     }
 };
-__global__ void k_large_write(i64 records, const u64* keys, const u32* vals, const u32* hpos, int tbits,
+__global__ void k_large_write(i64 records, const u64* keys, const u32* vals, int shift, const u32* hpos, int tbits,
                               const int* rows, const int* rec_off, const int* raw_off, int* raw_t, u32* raw_w) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= records) return;
-    const u64 k = keys[i];
+    const u64 k = keys[i] >> shift;
     const u64 tmask = (1ULL << tbits) - 1;
-    if ((k & tmask) == tmask || (i > 0 && keys[i - 1] == k)) return;
+    if ((k & tmask) == tmask || (i > 0 && (keys[i - 1] >> shift) == k)) return;
     const int j = static_cast<int>(k >> tbits);
     u64 sum = 0;
-    for (i64 r = i; r < records && keys[r] == k; ++r) sum += vals[r];
+    for (i64 r = i; r < records && (keys[r] >> shift) == k; ++r)
+        sum += shift ? (keys[r] & 0xffffffffULL) : vals[r];
     const int c = rows[j];
     const int pos = raw_off[c] + static_cast<int>(hpos[i] - hpos[rec_off[j]]);
     raw_t[pos] = static_cast<int>(k & tmask);
@@ -1715,19 +1726,24 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
                             static_cast<int*>(nullptr));
         const int tbits = bit_length(static_cast<u64>(nc));
         const int jbits = std::max(1, bit_length(static_cast<u64>(count[4] - 1)));
+        // (row, target) keys of up to 32 bits carry the weight in the same
+        // word: the sort then moves 8 bytes per record and pass, not 12.
+        const bool packed = tbits + jbits <= 32;
+        const int shift = packed ? 32 : 0;
         u64* keys = A.alloc<u64>(large_records);
         u64* keys_alt = A.alloc<u64>(large_records);
-        u32* vals = A.alloc<u32>(large_records);
-        u32* vals_alt = A.alloc<u32>(large_records);
+        u32* vals = packed ? nullptr : A.alloc<u32>(large_records);
+        u32* vals_alt = packed ? nullptr : A.alloc<u32>(large_records);
         launch(k_large_records, std::min(blocks_for(large_records, kThreads), 148 * 16), kThreads, 0, s,
                large_records, count[4], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
                vals);
-        radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, 0, tbits + jbits);
+        radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, shift, shift + tbits + jbits);
         u32* hpos = A.alloc<u32>(large_records);
         u32* heads_total = reinterpret_cast<u32*>(ctx.dev_scalars);
-        exclusive_scan<u32>(A, s, large_records, RecordHead{keys, (1ULL << tbits) - 1}, hpos, heads_total);
-        launch(k_large_write, blocks_for(large_records, kThreads), kThreads, 0, s, 
-            large_records, keys, vals, hpos, tbits, large, rec_off, raw_off, raw_t, raw_w);
+        exclusive_scan<u32>(A, s, large_records, RecordHead{keys, (1ULL << tbits) - 1, shift}, hpos, heads_total);
+        launch(k_large_write, blocks_for(large_records, kThreads), kThreads, 0, s, large_records,
+               static_cast<const u64*>(keys), static_cast<const u32*>(vals), shift, static_cast<const u32*>(hpos),
+               tbits, large, rec_off, raw_off, raw_t, raw_w);
         launch(k_large_counts, blocks_for(count[4], kThreads), kThreads, 0, s, count[4], large, rec_off, hpos,
                                                                                  heads_total, large_records, ucount);
     }

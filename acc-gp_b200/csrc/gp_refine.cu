@@ -1597,19 +1597,20 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                     const u64 t0 = tried[2 * i], t1 = tried[2 * i + 1];
                     const C* row = A + static_cast<i64>(v) * k;
                     u64 best = 0, room = 0;
-                    // Eight affinities loaded together, then scanned in part order.
-                    for (int p0 = 0; p0 < k; p0 += 8) {
-                        C c8[8];
+                    // Sixteen affinities loaded together (one round trip for
+                    // a 16-part slice), then scanned in part order.
+                    for (int p0 = 0; p0 < k; p0 += 16) {
+                        C c16[16];
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) c8[q] = p0 + q < k ? row[p0 + q] : C(0);
+                        for (int q = 0; q < 16; ++q) c16[q] = p0 + q < k ? row[p0 + q] : C(0);
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
+                        for (int q = 0; q < 16; ++q) {
                             const int p = p0 + q;
                             if (p >= k) break;
                             if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
                             const u64 avail = s_avail[p];
                             if (avail < w) continue;
-                            const u64 c = c8[q];
+                            const u64 c = c16[q];
                             if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
                         }
                     }
@@ -2546,14 +2547,19 @@ bool LevelRefiner<T>::repair() {
                 u32* open_count = reinterpret_cast<u32*>(counters + 5);
                 // Small sets of open donors finish all their attempts in one block.
                 auto finish_in_block = [&](int first_attempt) {
-                    with_row_size([&](auto d) {
+                    auto go = [&](auto d) {
                         launch(k_attempts<T, decltype(d)::value>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
                                static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
                                static_cast<const T*>(A), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
                                static_cast<const u32*>(g.ew), static_cast<const int*>(labels), g.vw, k,
                                static_cast<const int*>(targets), static_cast<const u64*>(slack), requests, tried, state,
                                targets, flags);
-                    });
+                    };
+                    // The row size matters only for on-demand affinities; a
+                    // dense level takes the smallest instantiation (fewest
+                    // registers: one block of 1024 threads has 64 each).
+                    if (on_demand) with_row_size(go);
+                    else go(std::integral_constant<int, 8>{});
                 };
                 if (acount <= kAttemptCap) {
                     select_if(A_, s(), acount, IsOpen{state}, WriteIdx{open}, open_count);
