@@ -82,7 +82,8 @@ class _Level(_C.Structure):
 class _Tuning(_C.Structure):
     _fields_ = [("medium_degree", _C.c_int32), ("large_narrow", _C.c_int32), ("build_short", _C.c_int32),
                 ("rebuild_divisor", _C.c_int32), ("on_demand_degree", _C.c_int32), ("default_ms", _C.c_double),
-                ("tuned_ms", _C.c_double), ("trials", _C.c_int32)]
+                ("tuned_ms", _C.c_double), ("trials", _C.c_int32), ("refine_heavy_small", _C.c_int32),
+                ("refine_heavy_mid", _C.c_int32), ("refine_heavy_large", _C.c_int32)]
 
 
 class _Request(_C.Structure):

@@ -62,6 +62,12 @@ struct Mapping {
     int build_short = 64;       // refinement: cache-build rows up to this, 8 lanes per row
     int rebuild_divisor = 100;  // refinement: rebuild the cache when moved entries exceed (n k size + 8 m) / this
     int on_demand_degree = 32;  // refinement: no cache when the maximum degree is at most this (0: never)
+    // Refinement rows above these entry counts go through the block-per-chunk
+    // kernels (2048-entry chunks) instead of a warp: on levels of at most
+    // 65,536 vertices, at most 2^20 vertices, and larger ones.
+    int refine_heavy_small = 256;
+    int refine_heavy_mid = 512;
+    int refine_heavy_large = 2048;
 };
 
 // Coarsening options, app/partition_main.cu:52-87 with no environment overrides.

@@ -846,6 +846,9 @@ gp_status gp_autotune(gp_context* ctx, const gp_csr* graph, int32_t k, double ep
             {&Mapping::build_short, {32, 64, 128}},
             {&Mapping::rebuild_divisor, {25, 50, 100, 200, 400}},
             {&Mapping::on_demand_degree, {0, 32}},
+            {&Mapping::refine_heavy_small, {128, 256, 512}},
+            {&Mapping::refine_heavy_mid, {256, 512, 1024}},
+            {&Mapping::refine_heavy_large, {1024, 2048, 4096}},
         };
         for (const Knob& knob : knobs) {
             const int kept = ctx->mapping.*knob.field;
@@ -860,7 +863,9 @@ gp_status gp_autotune(gp_context* ctx, const gp_csr* graph, int32_t k, double ep
         }
         restore.done = true;
         *out = gp_tuning{ctx->mapping.medium_degree, ctx->mapping.large_narrow, ctx->mapping.build_short,
-                         ctx->mapping.rebuild_divisor, ctx->mapping.on_demand_degree, default_ms, best_ms, trials};
+                         ctx->mapping.rebuild_divisor, ctx->mapping.on_demand_degree, default_ms, best_ms, trials,
+                         ctx->mapping.refine_heavy_small, ctx->mapping.refine_heavy_mid,
+                         ctx->mapping.refine_heavy_large};
         return GP_OK;
     });
 }
@@ -879,6 +884,9 @@ gp_status gp_set_option(gp_context* ctx, const char* name, int64_t value) {
     else if (key == "build_short" && value >= 8 && value <= 2048) ctx->mapping.build_short = static_cast<int>(value);
     else if (key == "rebuild_divisor" && value >= 1 && value <= 100000) ctx->mapping.rebuild_divisor = static_cast<int>(value);
     else if (key == "on_demand_degree" && value >= 0 && value <= 32) ctx->mapping.on_demand_degree = static_cast<int>(value);
+    else if (key == "refine_heavy_small" && value >= 64 && value <= 8192) ctx->mapping.refine_heavy_small = static_cast<int>(value);
+    else if (key == "refine_heavy_mid" && value >= 64 && value <= 8192) ctx->mapping.refine_heavy_mid = static_cast<int>(value);
+    else if (key == "refine_heavy_large" && value >= 64 && value <= 8192) ctx->mapping.refine_heavy_large = static_cast<int>(value);
     else if (key == "arena_chunk_mb" && value >= 1 && value <= (int64_t{1} << 24)) {
         ctx->ctx.persist.set_chunk_bytes(static_cast<size_t>(value) << 20);
         ctx->ctx.scratch.set_chunk_bytes(static_cast<size_t>(value) << 20);

@@ -2009,27 +2009,51 @@ __global__ void k_combine(int count, const JointMove* archive, const int* off, c
         return l;
     };
     const int begin = bound(lo - x.net, false), end = bound(hi - x.net, true);
-    long long best_gain = 0;
-    int best = -1, previous = -1;
+    // The (up to four) partner candidates, in the reference's probe order.
+    int cand[4];
+    int ncand = 0, previous = -1;
     for (int r = 0; r < 4 && begin < end; ++r) {
         const int j = begin + static_cast<int>((static_cast<long long>(end - begin - 1) * r) / 3);
         if (j == previous) continue;
         previous = j;
         if (j == i) continue;
-        const JointMove y = archive[j];
+        const JointMove& y = archive[j];
         if (y.a != x.a || y.b != x.b || x.size + y.size > 8) continue;
         bool overlap = false;
         for (int u = 0; u < x.size; ++u) for (int w = 0; w < y.size; ++w) overlap |= x.vertices[u] == y.vertices[w];
-        if (overlap) continue;
-        long long correction = 0;
+        if (!overlap) cand[ncand++] = j;
+    }
+    // One pass over x's rows corrects every candidate at once (each row is
+    // read once, not once per candidate).
+    long long correction[4] = {0, 0, 0, 0};
+    if (ncand) {
+        int yv[4][8], ysize[4];
+        for (int c = 0; c < ncand; ++c) {
+            const JointMove& y = archive[cand[c]];
+            ysize[c] = y.size;
+            for (int t = 0; t < 8; ++t) yv[c][t] = t < y.size ? y.vertices[t] : -1;
+        }
         for (int u = 0; u < x.size; ++u) {
             const int v = x.vertices[u];
-            for (int e = off[v] + lane; e < off[v + 1]; e += 32)
-                for (int t = 0; t < y.size; ++t)
-                    if (nbr[e] == y.vertices[t]) correction += (labels[v] == labels[nbr[e]] ? 2LL : -2LL) * edge_w(ew, e);
+            const int lv = labels[v];
+            for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
+                const int w = nbr[e];
+                bool hit = false;
+                for (int c = 0; c < ncand; ++c)
+                    for (int t = 0; t < ysize[c]; ++t) hit |= w == yv[c][t];
+                if (!hit) continue;
+                const long long contrib = (lv == labels[w] ? 2LL : -2LL) * edge_w(ew, e);
+                for (int c = 0; c < ncand; ++c)
+                    for (int t = 0; t < ysize[c]; ++t)
+                        if (w == yv[c][t]) correction[c] += contrib;
+            }
         }
-        correction = warp_sum(correction);
-        const long long gain = x.gain + y.gain + correction;
+    }
+    long long best_gain = 0;
+    int best = -1;
+    for (int c = 0; c < ncand; ++c) {
+        const int j = cand[c];
+        const long long gain = x.gain + archive[j].gain + warp_sum(correction[c]);
         if (gain > best_gain || (gain == best_gain && gain > 0 && j < best)) { best_gain = gain; best = j; }
     }
     if (!lane && best >= 0) {
@@ -2185,8 +2209,6 @@ struct Flagged {
 
 // ---------------------------------------------------------------- host side
 
-constexpr int kSmallLevelHeavyRow = 256;  // heavy-row threshold of levels of at most 65,536 vertices
-constexpr int kMidLevelHeavyRow = 512;    // and of levels of at most 2^20 vertices
 
 struct LevelResult {
     u64 cut = 0;
@@ -2426,13 +2448,16 @@ private:
             cut -= static_cast<u64>(delta);
         } else cut += static_cast<u64>(-delta);
     }
+    void enqueue_lp_round(double filter);
     i64 lp_round(double filter);
     bool repair();
     void exchange(u64& best);
 };
 
+// The device work of one label-propagation round, up to the read-back of its
+// counters (every launch is sized by the level, not by a count read back).
 template <class T>
-i64 LevelRefiner<T>::lp_round(double filter) {
+void LevelRefiner<T>::enqueue_lp_round(double filter) {
     GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
     LpParams q{n,     k,      C,     filter, g.off, g.nbr, g.ew,   g.vw,     labels, loads,
                prices, targets, gains, locks, flags, cand,  movers, counters, g.heavy_min};
@@ -2451,6 +2476,11 @@ i64 LevelRefiner<T>::lp_round(double filter) {
     }
     launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q);
     apply(movers, counters + 1, n, true, false);
+}
+
+template <class T>
+i64 LevelRefiner<T>::lp_round(double filter) {
+    enqueue_lp_round(filter);
     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters, 8 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
     GP_CUDA(cudaStreamSynchronize(s()));
     const i64 count = static_cast<i64>(ctx.host_scalars[1]);
@@ -2769,8 +2799,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     // Smaller levels: rows above a lower threshold (coarse hubs) go through
     // the block-per-chunk kernels instead of one warp each, which otherwise
     // set the time of every row-parallel pass of the level.
-    const int heavy_min = n <= 65536 ? kSmallLevelHeavyRow : n <= (1 << 20) ? kMidLevelHeavyRow : kHeavyRow;
-    if (heavy_min < kHeavyRow && g.maximum_degree > static_cast<u64>(heavy_min)) build_chunks(ctx, g, heavy_min, &A_);
+    const int heavy_min = n <= 65536 ? mapping.refine_heavy_small
+                          : n <= (1 << 20) ? mapping.refine_heavy_mid : mapping.refine_heavy_large;
+    if (heavy_min != g.heavy_min && (g.maximum_degree > static_cast<u64>(std::min(heavy_min, g.heavy_min)) || g.heavy_count))
+        build_chunks(ctx, g, heavy_min, &A_);
     uint64_t cap = 0;
     if (gp_status st = capacity_of(total, k, eps, &cap); st != GP_OK) fail(st, last_error());
     C = cap;

@@ -309,12 +309,16 @@ gp_status gp_profile_end(gp_context* ctx, uint64_t* launches, double* total_ms,
  *   large_narrow      [256, 2048] coarsening rows up to this: the smaller shared table
  *   build_short       [8, 2048]   cache-build rows up to this: 8 lanes per row
  *   rebuild_divisor   [1, 1e5]    cache rebuilt when moved entries exceed (n k w + 8 m) / this
- *   on_demand_degree  [0, 32]     no cache on levels whose maximum degree is at most this */
+ *   on_demand_degree  [0, 32]     no cache on levels whose maximum degree is at most this
+ *   refine_heavy_small / _mid / _large [64, 8192]  refinement rows longer than this go to the
+ *                     block-per-2048-entry-chunk kernels, on levels of at most 65,536
+ *                     vertices / at most 2^20 / larger (defaults 256 / 512 / 2048) */
 typedef struct gp_tuning {
     int32_t medium_degree, large_narrow, build_short, rebuild_divisor, on_demand_degree;
     double default_ms;  /* best partition time with the thresholds the call started from */
     double tuned_ms;    /* best partition time with the thresholds chosen */
     int32_t trials;     /* partitions timed */
+    int32_t refine_heavy_small, refine_heavy_mid, refine_heavy_large;
 } gp_tuning;
 
 /* Autotuner: partitions `graph` (host memory; uploaded once) `repeats` times

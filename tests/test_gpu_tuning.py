@@ -12,6 +12,9 @@ EXTREMES = {
     "build_short": [8, 32, 2048],
     "rebuild_divisor": [1, 100000],
     "on_demand_degree": [0, 8, 32],
+    "refine_heavy_small": [64, 8192],
+    "refine_heavy_mid": [64, 8192],
+    "refine_heavy_large": [64, 1024, 8192],
 }
 
 
@@ -36,7 +39,7 @@ def test_mapping_thresholds_do_not_change_labels(gp, graphs, name):
 
 def test_set_option_rejects_out_of_range(gp, ctx):
     for name, bad in [("medium_degree", 300), ("large_narrow", 4096), ("build_short", 4),
-                      ("rebuild_divisor", 0), ("on_demand_degree", 64)]:
+                      ("rebuild_divisor", 0), ("on_demand_degree", 64), ("refine_heavy_large", 32)]:
         with pytest.raises(gp.GpartError):
             ctx.set_option(name, bad)
 
@@ -49,6 +52,8 @@ def test_autotune_keeps_labels_and_reports(gp):
         assert t["medium_degree"] in (64, 128, 256) and t["large_narrow"] in (512, 1024, 2048)
         assert t["build_short"] in (32, 64, 128) and t["rebuild_divisor"] in (25, 50, 100, 200, 400)
         assert t["on_demand_degree"] in (0, 32)
-        assert t["trials"] == 12 and 0 < t["tuned_ms"] <= t["default_ms"]
+        assert t["refine_heavy_small"] in (128, 256, 512) and t["refine_heavy_mid"] in (256, 512, 1024)
+        assert t["refine_heavy_large"] in (1024, 2048, 4096)
+        assert t["trials"] == 18 and 0 < t["tuned_ms"] <= t["default_ms"]
         after, _ = c.partition(g, 64, 1.03, 0)  # the chosen thresholds stay on the context
         np.testing.assert_array_equal(after, before)
