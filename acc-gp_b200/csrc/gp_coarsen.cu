@@ -891,13 +891,21 @@ __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int*
 
 // Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 <= 8192, 4 larger;
 // sc[5] counts the records of class 4.
+constexpr int kRowClasses = 7;  // raw row sizes: <=128, <=512, <=1024, <=2048, <=4096, <=8192, larger
 __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u64* sc) {
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int r = c < nc ? raw[c] : 0;
-    const int cls = c >= nc ? -1 : r <= 128 ? 0 : r <= 512 ? 1 : r <= kBlockSortRow ? 2 : r <= kBigSortRow ? 3 : 4;
+    const int cls = c >= nc                  ? -1
+                    : r <= 128               ? 0
+                    : r <= 512               ? 1
+                    : r <= 1024              ? 2
+                    : r <= 2048              ? 3
+                    : r <= kBlockSortRow     ? 4
+                    : r <= kBigSortRow       ? 5
+                                             : 6;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) block_append(static_cast<int>(c), cls == k, lists + k * stride, sc + k);
-    block_atomic_add(sc + 5, cls == 4 ? static_cast<u64>(r) : 0ULL);
+    for (int k = 0; k < kRowClasses; ++k) block_append(static_cast<int>(c), cls == k, lists + k * stride, sc + k);
+    block_atomic_add(sc + kRowClasses, cls == kRowClasses - 1 ? static_cast<u64>(r) : 0ULL);
 }
 
 // contraction_warp_sort / contraction_sort_row (contraction_rows.cuh:40-116):
@@ -1110,25 +1118,23 @@ __device__ __forceinline__ void sort_row_in_smem(int* keys, u32* vals, u32 (*war
 // Rows of 513..4096 raw entries: stable LSD radix sort by target in shared
 // memory (8-bit digits over the bits of nc; dropped intra-cluster entries
 // take the key nc and sort last), then one thread per run of equal keys sums
-// it and writes the unique run back at the row's start.
+// it and writes the unique run back at the row's start.  One instantiation
+// per row class (Items = 4, 8, 16 per thread: rows up to 1024, 2048, 4096),
+// each launched on its own list, so the short classes run with their own
+// register count and shared memory and more blocks fit on an SM.
+template <int Items>
 __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
                                                          int* ucount, int nc, int bits) {
-    __shared__ int keys[kBlockSortRow];
-    __shared__ u32 vals[kBlockSortRow];
+    static_assert(Items * 256 <= kBlockSortRow, "row class above the block sort");
+    __shared__ int keys[Items * 256];
+    __shared__ u32 vals[Items * 256];
     __shared__ u32 warp_count[8][kRadix];
     __shared__ u32 local_base[kRadix];
     __shared__ u32 scan_u[33];
     __shared__ int scan_smem[33];
     const int c = rows[blockIdx.x];
     const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
-    // Items per thread by row length (uniform per block).
-    if (degree <= 1024)
-        sort_row_in_smem<4>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
-    else if (degree <= 2048)
-        sort_row_in_smem<8>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
-    else
-        sort_row_in_smem<kBlockSortRow / 256>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree,
-                                              nc, bits);
+    sort_row_in_smem<Items>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
     // keys/vals hold the sorted row; heads of runs and their exclusive scan.
     const int per = (degree + blockDim.x - 1) / blockDim.x;
     int local = 0;
@@ -1693,13 +1699,13 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
                    static_cast<const int*>(base), raw_t, raw_w);
     }
     // Row classes by raw size.
-    int* lists = A.alloc<int>(static_cast<size_t>(nc) * 5);
-    ctx.clear_scalars(6);
+    int* lists = A.alloc<int>(static_cast<size_t>(nc) * kRowClasses);
+    ctx.clear_scalars(kRowClasses + 1);
     launch(k_row_classes, blocks_for(nc, kThreads), kThreads, 0, s, nc, raw, lists, nc, ctx.dev_scalars);
-    const u64* cls = ctx.read_scalars(6);
-    const i64 count[5] = {static_cast<i64>(cls[0]), static_cast<i64>(cls[1]), static_cast<i64>(cls[2]),
-                          static_cast<i64>(cls[3]), static_cast<i64>(cls[4])};
-    const i64 large_records = static_cast<i64>(cls[5]);
+    const u64* cls = ctx.read_scalars(kRowClasses + 1);
+    i64 count[kRowClasses];
+    for (int c = 0; c < kRowClasses; ++c) count[c] = static_cast<i64>(cls[c]);
+    const i64 large_records = static_cast<i64>(cls[kRowClasses]);
     int* ucount = raw;  // raw sizes are no longer needed once the classes exist
     if (count[0])
         launch(k_sort_rows_warp<false>, blocks_for(count[0] * 32, kThreads), kThreads, 0, s, count[0], lists, raw_off,
@@ -1708,24 +1714,30 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         launch(k_sort_rows_warp<true>, blocks_for(count[1] * 32, kThreads), kThreads, 0, s, count[1], lists + nc,
                raw_off, raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     if (count[2])
-        launch(k_sort_rows_block, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
+        launch(k_sort_rows_block<4>, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
                ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
-    if (count[3]) {
+    if (count[3])
+        launch(k_sort_rows_block<8>, static_cast<int>(count[3]), 256, 0, s, lists + 3 * nc, raw_off, raw_t, raw_w,
+               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
+    if (count[4])
+        launch(k_sort_rows_block<16>, static_cast<int>(count[4]), 256, 0, s, lists + 4 * nc, raw_off, raw_t, raw_w,
+               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
+    if (count[5]) {
         // Set on every call (one fixed value): the attribute belongs to the
         // kernel, on whichever device is current.
         GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kBigSortSmem)));
-        launch(k_sort_rows_big, static_cast<int>(count[3]), kBigSortThreads, kBigSortSmem, s, lists + 3 * nc, raw_off,
+        launch(k_sort_rows_big, static_cast<int>(count[5]), kBigSortThreads, kBigSortSmem, s, lists + 5 * nc, raw_off,
                raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
     }
-    if (count[4]) {
+    if (count[6]) {
         ArenaScope ls(A);
-        const int* large = lists + 4 * nc;
-        int* rec_off = A.alloc<int>(count[4]);
-        exclusive_scan<int>(A, s, count[4], LargeRowSize{large, raw_off}, rec_off,
+        const int* large = lists + 6 * nc;
+        int* rec_off = A.alloc<int>(count[6]);
+        exclusive_scan<int>(A, s, count[6], LargeRowSize{large, raw_off}, rec_off,
                             static_cast<int*>(nullptr));
         const int tbits = bit_length(static_cast<u64>(nc));
-        const int jbits = std::max(1, bit_length(static_cast<u64>(count[4] - 1)));
+        const int jbits = std::max(1, bit_length(static_cast<u64>(count[6] - 1)));
         // (row, target) keys of up to 32 bits carry the weight in the same
         // word: the sort then moves 8 bytes per record and pass, not 12.
         const bool packed = tbits + jbits <= 32;
@@ -1735,7 +1747,7 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         u32* vals = packed ? nullptr : A.alloc<u32>(large_records);
         u32* vals_alt = packed ? nullptr : A.alloc<u32>(large_records);
         launch(k_large_records, std::min(blocks_for(large_records, kThreads), 148 * 16), kThreads, 0, s,
-               large_records, count[4], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
+               large_records, count[6], large, raw_off, static_cast<const int*>(rec_off), raw_t, raw_w, tbits, keys,
                vals);
         radix_sort_pairs(A, s, large_records, keys, vals, keys_alt, vals_alt, shift, shift + tbits + jbits);
         u32* hpos = A.alloc<u32>(large_records);
@@ -1744,7 +1756,7 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         launch(k_large_write, blocks_for(large_records, kThreads), kThreads, 0, s, large_records,
                static_cast<const u64*>(keys), static_cast<const u32*>(vals), shift, static_cast<const u32*>(hpos),
                tbits, large, rec_off, raw_off, raw_t, raw_w);
-        launch(k_large_counts, blocks_for(count[4], kThreads), kThreads, 0, s, count[4], large, rec_off, hpos,
+        launch(k_large_counts, blocks_for(count[6], kThreads), kThreads, 0, s, count[6], large, rec_off, hpos,
                                                                                  heads_total, large_records, ucount);
     }
     // Final offsets, then the compact copy into the level's own storage.
