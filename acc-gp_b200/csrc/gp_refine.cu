@@ -1709,6 +1709,22 @@ __device__ bool joint_same(const JointMove& x, const JointMove& y) {  // joint_s
     }
     return true;
 }
+// Sort keys of a joint move.  (k1, k2), compared as unsigned words in that
+// order, is a monotone projection of the comparator's leading fields: unequal
+// keys decide a comparison the same way the comparator does, and only equal
+// keys need the comparator itself.  A signed field enters as its value
+// clamped to [-2^53, 2^53) with one value for each side beyond, 55 bits; a
+// word that would need a field after a clamped one stops there (zero).
+struct MoveKey {
+    u64 k1, k2;
+};
+constexpr long long kKeyLimit = 1LL << 53;
+__device__ __forceinline__ u64 field_key(long long v, bool descending, bool& clamped) {
+    clamped = v < -kKeyLimit || v >= kKeyLimit;
+    const long long c = v < -kKeyLimit ? -kKeyLimit - 1 : v >= kKeyLimit ? kKeyLimit : v;
+    const u64 u = static_cast<u64>(c + kKeyLimit + 1);  // 0 .. 2^54
+    return descending ? (1ULL << 54) - u : u;
+}
 struct NetOrder {  // JointNetOrder (complementary_moves.cuh:5-14)
     __device__ bool operator()(const JointMove& x, const JointMove& y) const {
         if (x.a != y.a) return x.a < y.a;
@@ -1718,6 +1734,16 @@ struct NetOrder {  // JointNetOrder (complementary_moves.cuh:5-14)
         for (int j = 0; j < x.size; ++j) if (x.vertices[j] != y.vertices[j]) return x.vertices[j] < y.vertices[j];
         return x.id < y.id;
     }
+    // k1 = (a + 1, net ascending), k2 = (gain descending, size).
+    __device__ static MoveKey key(const JointMove& x) {
+        bool net_clamped, gain_clamped;
+        const u64 net = field_key(x.net, false, net_clamped);
+        const u64 gain = field_key(x.gain, true, gain_clamped);
+        MoveKey r;
+        r.k1 = (static_cast<u64>(x.a + 1) << 55) | net;
+        r.k2 = net_clamped ? 0 : (gain << 8) | (gain_clamped ? 0 : static_cast<u64>(x.size));
+        return r;
+    }
 };
 struct MoveOrder {  // JointOrder (exchange.cuh:29-36)
     __device__ bool operator()(const JointMove& x, const JointMove& y) const {
@@ -1726,11 +1752,34 @@ struct MoveOrder {  // JointOrder (exchange.cuh:29-36)
         if (x.gain != y.gain) return x.gain > y.gain;
         return x.id < y.id;
     }
+    // k1 = (empty, a + 1, gain descending), k2 = id.
+    __device__ static MoveKey key(const JointMove& x) {
+        bool gain_clamped;
+        const u64 gain = field_key(x.gain, true, gain_clamped);
+        MoveKey r;
+        r.k1 = (static_cast<u64>(x.size == 0) << 63) | (static_cast<u64>(x.a + 1) << 55) | gain;
+        r.k2 = gain_clamped ? 0 : static_cast<u64>(static_cast<long long>(x.id) + 2147483649LL);
+        return r;
+    }
 };
+template <class Cmp>
+__global__ void k_move_keys(int count, const JointMove* moves, MoveKey* keys) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) keys[i] = Cmp::key(moves[i]);
+}
+// Whether move b sorts before move a (both real entries).
+template <class Cmp>
+__device__ __forceinline__ bool move_before(const MoveKey& kb, const MoveKey& ka, const JointMove* moves, int b, int a,
+                                            Cmp cmp) {
+    if (kb.k1 != ka.k1) return kb.k1 < ka.k1;
+    if (kb.k2 != ka.k2) return kb.k2 < ka.k2;
+    return cmp(moves[b], moves[a]);
+}
 
 // One bitonic stage over an index permutation padded to a power of two.
 template <class Cmp>
-__global__ void k_bitonic(int size, int count, const JointMove* moves, int* idx, int kk, int jj, Cmp cmp) {
+__global__ void k_bitonic(int size, int count, const JointMove* moves, const MoveKey* keys, int* idx, int kk, int jj,
+                          Cmp cmp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= size) return;
     const int x = i ^ jj;
@@ -1740,39 +1789,76 @@ __global__ void k_bitonic(int size, int count, const JointMove* moves, int* idx,
     bool greater;
     if (a >= count) greater = b < count;
     else if (b >= count) greater = false;
-    else greater = cmp(moves[b], moves[a]);
+    else greater = move_before(keys[b], keys[a], moves, b, a, cmp);
     const bool up = (i & kk) == 0;
     if (greater == up) { idx[i] = b; idx[x] = a; }
 }
-// Bitonic stages on segments of kBitonicSegment indices held in shared
-// memory: for kk from kk_first to kk_last, every jj below the segment size
-// (the first kk starts at jj_first).  Same compare-exchange as k_bitonic.
-constexpr int kBitonicSegment = 4096;
+// One compare-exchange step (partner distance jj, direction block kk) over
+// the shared-memory segment that starts at permutation position `base`.
 template <class Cmp>
-__global__ void __launch_bounds__(1024) k_bitonic_local(int size, int count, const JointMove* moves, int* idx, int kk_first,
-                                                       int kk_last, int jj_first, Cmp cmp) {
-    __shared__ int s_idx[kBitonicSegment];
-    const int base = blockIdx.x * kBitonicSegment;
-    const int seg = min(kBitonicSegment, size - base);
-    for (int i = threadIdx.x; i < seg; i += blockDim.x) s_idx[i] = idx[base + i];
-    __syncthreads();
-    for (int kk = kk_first; kk <= kk_last; kk <<= 1) {
-        for (int jj = kk == kk_first ? jj_first : kk >> 1; jj; jj >>= 1) {
-            for (int p = threadIdx.x; p < seg / 2; p += blockDim.x) {
-                const int i = (p / jj) * 2 * jj + p % jj;
-                const int x = i + jj;
-                const int a = s_idx[i], b = s_idx[x];
-                bool greater;
-                if (a >= count) greater = b < count;
-                else if (b >= count) greater = false;
-                else greater = cmp(moves[b], moves[a]);
-                const bool up = ((base + i) & kk) == 0;
-                if (greater == up) { s_idx[i] = b; s_idx[x] = a; }
-            }
-            __syncthreads();
+__device__ __forceinline__ void bitonic_step_smem(int seg, int base, int count, int kk, int jj, const JointMove* moves,
+                                                  MoveKey* s_key, int* s_idx, Cmp cmp) {
+    for (int p = threadIdx.x; p < seg / 2; p += blockDim.x) {
+        const int i = (p / jj) * 2 * jj + p % jj;
+        const int x = i + jj;
+        const int a = s_idx[i], b = s_idx[x];
+        bool greater;
+        if (a >= count) greater = b < count;
+        else if (b >= count) greater = false;
+        else greater = move_before(s_key[x], s_key[i], moves, b, a, cmp);
+        const bool up = ((base + i) & kk) == 0;
+        if (greater == up) {
+            s_idx[i] = b;
+            s_idx[x] = a;
+            const MoveKey t = s_key[i];
+            s_key[i] = s_key[x];
+            s_key[x] = t;
         }
     }
+    __syncthreads();
+}
+// Bitonic stages on segments of kBitonicSegment indices held in shared
+// memory with their keys: for kk from kk_first to kk_last, every jj below the
+// segment size (the first kk starts at jj_first).  Same compare-exchange as
+// k_bitonic.
+constexpr int kBitonicSegment = 4096;
+constexpr size_t kBitonicEntryBytes = sizeof(MoveKey) + sizeof(int);
+template <class Cmp>
+__global__ void __launch_bounds__(1024) k_bitonic_local(int size, int count, const JointMove* moves, const MoveKey* keys,
+                                                       int* idx, int kk_first, int kk_last, int jj_first, Cmp cmp) {
+    extern __shared__ __align__(16) unsigned char bitonic_smem[];
+    MoveKey* s_key = reinterpret_cast<MoveKey*>(bitonic_smem);
+    int* s_idx = reinterpret_cast<int*>(s_key + kBitonicSegment);
+    const int base = blockIdx.x * kBitonicSegment;
+    const int seg = min(kBitonicSegment, size - base);
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) {
+        const int a = idx[base + i];
+        s_idx[i] = a;
+        if (a < count) s_key[i] = keys[a];
+    }
+    __syncthreads();
+    for (int kk = kk_first; kk <= kk_last; kk <<= 1)
+        for (int jj = kk == kk_first ? jj_first : kk >> 1; jj; jj >>= 1)
+            bitonic_step_smem(seg, base, count, kk, jj, moves, s_key, s_idx, cmp);
     for (int i = threadIdx.x; i < seg; i += blockDim.x) idx[base + i] = s_idx[i];
+}
+// A whole sort of up to kBitonicSegment moves in one block: keys, the full
+// network in shared memory (the same steps as k_bitonic_local over one
+// segment) and the gather of the sorted moves.
+template <class Cmp>
+__global__ void __launch_bounds__(1024) k_sort_moves_block(int size, int count, const JointMove* in, JointMove* out,
+                                                          Cmp cmp) {
+    extern __shared__ __align__(16) unsigned char bitonic_smem[];
+    MoveKey* s_key = reinterpret_cast<MoveKey*>(bitonic_smem);
+    int* s_idx = reinterpret_cast<int*>(s_key + size);
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        s_idx[i] = i;
+        if (i < count) s_key[i] = Cmp::key(in[i]);
+    }
+    __syncthreads();
+    for (int kk = 2; kk <= size; kk <<= 1)
+        for (int jj = kk >> 1; jj; jj >>= 1) bitonic_step_smem(size, 0, count, kk, jj, in, s_key, s_idx, cmp);
+    for (int i = threadIdx.x; i < count; i += blockDim.x) out[i] = in[s_idx[i]];
 }
 __global__ void k_iota(int n, int* idx) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2024,28 +2110,34 @@ __global__ void k_combine(int count, const JointMove* archive, const int* off, c
         if (!overlap) cand[ncand++] = j;
     }
     // One pass over x's rows corrects every candidate at once (each row is
-    // read once, not once per candidate).
+    // read once, not once per candidate).  The candidates' vertices sit in
+    // 32 fixed register slots (slot 8c + t: vertex t of candidate c, -1 when
+    // absent), so a neighbour is tested against all of them without local
+    // memory; a move's vertices are distinct, so a neighbour meets each
+    // candidate at most once.
     long long correction[4] = {0, 0, 0, 0};
     if (ncand) {
-        int yv[4][8], ysize[4];
-        for (int c = 0; c < ncand; ++c) {
-            const JointMove& y = archive[cand[c]];
-            ysize[c] = y.size;
-            for (int t = 0; t < 8; ++t) yv[c][t] = t < y.size ? y.vertices[t] : -1;
+        int yv[32];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const JointMove* y = c < ncand ? archive + cand[c] : nullptr;
+            const int size = y ? y->size : 0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) yv[8 * c + t] = t < size ? y->vertices[t] : -1;
         }
         for (int u = 0; u < x.size; ++u) {
             const int v = x.vertices[u];
             const int lv = labels[v];
             for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
                 const int w = nbr[e];
-                bool hit = false;
-                for (int c = 0; c < ncand; ++c)
-                    for (int t = 0; t < ysize[c]; ++t) hit |= w == yv[c][t];
+                unsigned hit = 0;
+#pragma unroll
+                for (int q = 0; q < 32; ++q) hit |= w == yv[q] ? 1u << (q >> 3) : 0u;
                 if (!hit) continue;
                 const long long contrib = (lv == labels[w] ? 2LL : -2LL) * edge_w(ew, e);
-                for (int c = 0; c < ncand; ++c)
-                    for (int t = 0; t < ysize[c]; ++t)
-                        if (w == yv[c][t]) correction[c] += contrib;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (hit & (1u << c)) correction[c] += contrib;
             }
         }
     }
@@ -2686,6 +2778,7 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
     JointMove* act = A_.alloc<JointMove>(pool_cap);
     JointMove* act_sorted = A_.alloc<JointMove>(pool_cap);
     int* idx = A_.alloc<int>(2 * pool_cap);
+    MoveKey* move_keys = A_.alloc<MoveKey>(pool_cap);
     int* owners = A_.alloc<int>(n);
     u64* events = A_.alloc<u64>(pool_cap);
     int* stops = A_.alloc<int>(k);
@@ -2699,20 +2792,38 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         return static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
     };
     auto sort_moves = [&](JointMove* in, JointMove* out, int count, auto cmp) {
+        using Cmp = decltype(cmp);
         int size = 1;
         while (size < count) size <<= 1;
+        // (Shared-memory limits are set on every call that needs more than
+        // the default: they belong to the kernel, on whichever device is
+        // current.)
+        if (size <= kBitonicSegment) {
+            const size_t smem = kBitonicEntryBytes * size;
+            if (smem > 48 * 1024)
+                GP_CUDA(cudaFuncSetAttribute(k_sort_moves_block<Cmp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+            launch(k_sort_moves_block<Cmp>, 1, 1024, smem, s(), size, count, static_cast<const JointMove*>(in), out,
+                   cmp);
+            return;
+        }
         launch(k_iota, blocks_for(size, kThreads), kThreads, 0, s(), size, idx);
+        launch(k_move_keys<Cmp>, blocks_for(count, kThreads), kThreads, 0, s(), count,
+               static_cast<const JointMove*>(in), move_keys);
         // Stages whose partner distance stays inside a segment run in shared
         // memory, the rest one launch per stage.
-        const int segments = std::max(1, size / kBitonicSegment);
+        const size_t smem = kBitonicEntryBytes * kBitonicSegment;
+        GP_CUDA(cudaFuncSetAttribute(k_bitonic_local<Cmp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        const int segments = size / kBitonicSegment;
         const JointMove* m = in;
-        launch(k_bitonic_local<decltype(cmp)>, segments, 1024, 0, s(), size, count, m, idx, 2,
-               std::min(size, kBitonicSegment), 1, cmp);
+        const MoveKey* mk = move_keys;
+        launch(k_bitonic_local<Cmp>, segments, 1024, smem, s(), size, count, m, mk, idx, 2, kBitonicSegment, 1, cmp);
         for (int kk = 2 * kBitonicSegment; kk <= size; kk <<= 1) {
             for (int jj = kk >> 1; jj >= kBitonicSegment; jj >>= 1)
-                launch(k_bitonic<decltype(cmp)>, blocks_for(size, kThreads), kThreads, 0, s(), size, count, m, idx, kk,
-                       jj, cmp);
-            launch(k_bitonic_local<decltype(cmp)>, segments, 1024, 0, s(), size, count, m, idx, kk, kk,
+                launch(k_bitonic<Cmp>, blocks_for(size, kThreads), kThreads, 0, s(), size, count, m, mk, idx, kk, jj,
+                       cmp);
+            launch(k_bitonic_local<Cmp>, segments, 1024, smem, s(), size, count, m, mk, idx, kk, kk,
                    kBitonicSegment / 2, cmp);
         }
         launch(k_gather_moves, blocks_for(count, kThreads), kThreads, 0, s(), count, static_cast<const int*>(idx),

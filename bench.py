@@ -406,6 +406,8 @@ def launch_list(args):
     gp = load_package()
     if args.workload == "m3":  # weighted 7-point mesh, side^3 vertices, k=128
         g, k = gp.mesh3d(args.side, args.side, args.side, weighted=True, seed=0), 128
+    elif args.workload == "g2":  # 2D grid, side^2 vertices, k=8
+        g, k = gp.grid2d(args.side, args.side), 8
     else:
         g, k = gp.rmat(args.scale, 16, 0.57, 0.19, 0.19, 0), WORKLOAD["k"]
     dev = torch.device("cuda", 0)
@@ -674,8 +676,8 @@ def main():
     ap.add_argument("--no-cold-cli", action="store_true", help="--impl reference: skip the cold CLI run")
     ap.add_argument("--launch-list", action="store_true",
                     help="run `--warmup` + one partition and exit (for the ncu launch list)")
-    ap.add_argument("--side", type=int, default=256, help="mesh side of --launch-list --workload m3")
-    ap.add_argument("--workload", choices=["rmat22", "batch", "serving", "m3", "tune"], default="rmat22",
+    ap.add_argument("--side", type=int, default=256, help="mesh or grid side of --launch-list --workload m3 / g2")
+    ap.add_argument("--workload", choices=["rmat22", "batch", "serving", "m3", "g2", "tune"], default="rmat22",
                     help="batch: the uneven 512-graph set, serial vs gp_partition_batch; "
                          "serving: Poisson requests against a gp_server")
     ap.add_argument("--requests", type=int, default=1000)
@@ -693,6 +695,8 @@ def main():
     ap.add_argument("--scale", type=int, default=22,
                     help="R-MAT scale of the --launch-list graph (smaller cases for ncu captures)")
     args = ap.parse_args()
+    if args.workload in ("m3", "g2") and not args.launch_list:
+        ap.error(f"--workload {args.workload} is a --launch-list case")
     if args.launch_list:
         launch_list(args)
     elif args.workload == "batch":
