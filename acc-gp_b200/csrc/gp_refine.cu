@@ -837,16 +837,6 @@ __global__ void k_filter_finish(i64 count, const int* heavy, const long long* co
     q.flags[v] = keep;
 }
 
-// Candidates with a kept move -> mover list (incremental_compact_candidates).
-__global__ void k_compact_movers(LpParams q) {
-    const i64 count = static_cast<i64>(q.counters[0]);
-    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < count; base += static_cast<i64>(gridDim.x) * blockDim.x) {
-        const i64 i = base + threadIdx.x;
-        const int v = i < count ? q.cand[i] : 0;
-        block_append(v, i < count && q.flags[v], q.movers, q.counters + 1);
-    }
-}
-
 // Packed per-vertex state read by the cache update: bits 0-7 the label,
 // bits 8-15 the target and bit 16 set while the vertex is in the batch being
 // applied.  One 4-byte gather per neighbour replaces the label, flag and
@@ -1010,14 +1000,38 @@ __global__ void k_mark_movers(i64 count, const int* movers, const u64* live_coun
     if (out) block_atomic_add(out, entries);
 }
 
+// Candidates with a kept move -> mover list (incremental_compact_candidates).
+// With `state`, also what k_mark_movers does for the list: marks each mover
+// in the packed state and adds its row's entries to *entries (the rebuild
+// gate), so the batch needs no separate marking launch.
+__global__ void k_compact_movers(LpParams q, u32* state, u64* entries) {
+    const i64 count = static_cast<i64>(q.counters[0]);
+    u64 mine = 0;
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < count; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 i = base + threadIdx.x;
+        const int v = i < count ? q.cand[i] : 0;
+        const bool keep = i < count && q.flags[v];
+        if (keep && state) {
+            state[v] = (state[v] & 0xffu) | (static_cast<u32>(q.targets[v] & 0xff) << 8) | kMovingBit;
+            mine += static_cast<u64>(q.off[v + 1] - q.off[v]);
+        }
+        block_append(v, keep, q.movers, q.counters + 1);
+    }
+    if (entries) block_atomic_add(entries, mine);
+}
+
 // incremental_commit (incremental.cuh:532-547) with per-block aggregation of
 // the part-load changes.
 // Also keeps rlabels (the labels in repair order, rposition[v] the place of
-// v) current.
+// v) current and clears each mover's flag.  The last block to finish (a
+// counter that every block increments once after its load changes; that
+// block resets it for the next launch) writes the largest part load to
+// *max_load, so no separate launch reads the loads back.
 __global__ void k_commit(i64 count, const int* movers, const u64* live_count, int* labels, const int* targets,
                          const u32* vw, int k, u64* loads, unsigned char* locks, int* flags, const u32* rposition,
-                         int* rlabels, u32* state) {
+                         int* rlabels, u32* state, u64* max_load, unsigned int* blocks_done) {
     extern __shared__ long long diff[];
+    __shared__ bool last;
     if (live_count) count = static_cast<i64>(*live_count);
     for (int p = threadIdx.x; p < k; p += blockDim.x) diff[p] = 0;
     __syncthreads();
@@ -1031,17 +1045,24 @@ __global__ void k_commit(i64 count, const int* movers, const u64* live_count, in
         rlabels[rposition[v]] = t;
         if (state) state[v] = static_cast<u32>(t);
         if (locks) locks[v] = 1;
+        flags[v] = 0;
     }
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x)
         if (diff[p]) atomicAdd(loads + p, static_cast<u64>(diff[p]));
-    (void)flags;
-}
-
-__global__ void k_clear_flags(i64 count, const int* movers, const u64* live_count, int* flags) {
-    if (live_count) count = static_cast<i64>(*live_count);
-    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x)
-        flags[movers[i]] = 0;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(blocks_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    u64 m = 0;
+    for (int p = threadIdx.x; p < k; p += 32) m = max(m, __ldcg(loads + p));
+    m = warp_max(m);
+    if (threadIdx.x == 0) {
+        *max_load = m;
+        *blocks_done = 0;
+    }
 }
 
 // ---------------------------------------------------------------- repair
@@ -2426,12 +2447,15 @@ private:
     // after the commit instead (identical values: the cache is an exact sum);
     // settle() then takes the new cut from the rebuild.  counters: 2 delta,
     // 3 max load, 6 mover entries, 7 directed cut of a rebuild.
-    void apply(const int* list, const u64* live, i64 host_count, bool lp, bool sample) {
-        GP_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(u64), s()));
-        GP_CUDA(cudaMemsetAsync(counters + 6, 0, 2 * sizeof(u64), s()));
+    // `marked`: the list's producer has zeroed counters[2..7] and done what
+    // k_mark_movers does (k_compact_movers for a label-propagation batch).
+    void apply(const int* list, const u64* live, i64 host_count, bool lp, bool sample, bool marked = false) {
+        // counters[2..7]: cut change, largest load, (free), rebuild gate
+        // entries and rebuild decision; [4] and [5] hold nothing across it.
+        if (!marked) GP_CUDA(cudaMemsetAsync(counters + 2, 0, 6 * sizeof(u64), s()));
         const u64* gate = sample || on_demand ? nullptr : counters + 6;
         const u64 threshold = gate ? rebuild_entries : ~0ULL;
-        if (gate || state)
+        if ((gate || state) && !marked)
             launch(k_mark_movers, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    static_cast<const int*>(targets), state, gate ? counters + 6 : static_cast<u64*>(nullptr));
         if (on_demand)
@@ -2456,7 +2480,8 @@ private:
         }
         launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags,
-               static_cast<const u32*>(rposition), rlabels, state);
+               static_cast<const u32*>(rposition), rlabels, state, counters + 3,
+               reinterpret_cast<unsigned int*>(counters + 8));
         if (frontier_on) {
             launch(k_touch_rows, grid_for(host_count * 32, kThreads), kThreads, 0, s(), host_count, list, live, g.off,
                    g.nbr, g.heavy_min, frontier);
@@ -2464,9 +2489,7 @@ private:
                 launch(k_touch_chunks, chunk_grid(), 256, 0, s(), g, static_cast<const int*>(chunk_work),
                        static_cast<const u64*>(chunk_work_count), frontier);
         }
-        launch(k_clear_flags, grid_for(host_count, kThreads), kThreads, 0, s(), host_count, list, live, flags);
         if (gate) build(counters + 7, gate, threshold);
-        launch(k_max_load, 1, 32, 0, s(), k, loads, counters + 3);
     }
     // Cut decrease of the last apply from host copies of counters[2..7].
     long long settled_delta(const u64* h) const {
@@ -2550,7 +2573,7 @@ private:
 // counters (every launch is sized by the level, not by a count read back).
 template <class T>
 void LevelRefiner<T>::enqueue_lp_round(double filter) {
-    GP_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(u64), s()));
+    GP_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(u64), s()));  // [0..1] here, [2..7] for apply
     LpParams q{n,     k,      C,     filter, g.off, g.nbr, g.ew,   g.vw,     labels, loads,
                prices, targets, gains, locks, flags, cand,  movers, counters, g.heavy_min};
     proposals(q);
@@ -2566,8 +2589,9 @@ void LevelRefiner<T>::enqueue_lp_round(double filter) {
         launch(k_filter_finish, blocks_for(g.heavy_count, kThreads), kThreads, 0, s(), g.heavy_count,
                static_cast<const int*>(g.heavy), static_cast<const long long*>(corr_acc), q);
     }
-    launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q);
-    apply(movers, counters + 1, n, true, false);
+    launch(k_compact_movers, grid_for(n, kThreads), kThreads, 0, s(), q, state,
+           on_demand ? static_cast<u64*>(nullptr) : counters + 6);
+    apply(movers, counters + 1, n, true, false, true);
 }
 
 template <class T>
@@ -2943,7 +2967,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     flags = A_.alloc<int>(n);
     cand = A_.alloc<int>(n);
     movers = A_.alloc<int>(n);
-    counters = A_.alloc<u64>(8);
+    counters = A_.alloc<u64>(9);  // [8]: k_commit's finished-block count, zero between launches
+    GP_CUDA(cudaMemsetAsync(counters + 8, 0, sizeof(u64), s()));
     corr_acc = A_.alloc<long long>(g.heavy_count + 1);
     if (g.chunks) {
         chunk_work = A_.alloc<int>(g.chunks);
