@@ -1579,8 +1579,33 @@ __global__ void k_merge_requests(int k, u64* requests, u64* added) {
 // attempt after attempt, without a round trip to the host.  open[j] (j <
 // *count, ascending) indexes the active donors, so the requests of one target
 // are admitted in repair order exactly as the device-wide path does.
+//
+// Everything an attempt reads about a donor (vertex, weight, part, state,
+// tried parts) sits in dynamic shared memory for the whole launch; state and
+// tried go back to global memory at the end.  A donor's choice is the
+// eligible part (not its own, not tried, room for its weight) of largest
+// (affinity, room, -part).  Parts only leave eligibility during a launch
+// (tried parts stay tried, rooms only shrink), so a full scan of the
+// donor's affinity row also keeps a shortlist: the four eligible parts of
+// largest (affinity, -part) and the largest affinity among the other
+// eligible parts.  A later attempt whose best listed part, still eligible,
+// has an affinity above that bound takes it without reading the row again
+// (no unlisted part can reach or tie it).  When the bound is 0 and no
+// eligible listed part has more, every eligible part has affinity 0 and the
+// choice is the eligible part of most room: the first one in the attempt's
+// order of parts by (room desc, part asc).  Otherwise the row is scanned
+// anew.  Admission turns the per-warp request sums of a chunk into per-part
+// prefixes once (a thread per part), so a request reads its start directly.
 constexpr int kAttemptThreads = 1024;
 constexpr int kAttemptCap = 2048;  // open donors handled by one block
+constexpr int kShortlist = 4;
+constexpr unsigned char kNoPart = 0xff;
+// Dynamic shared memory of k_attempts for `count` donors (cache type C).
+template <class C>
+constexpr size_t attempt_smem(int count) {
+    return static_cast<size_t>(count) * (2 * sizeof(u64) + (kShortlist + 1) * sizeof(C) + 2 * sizeof(u32) +
+                                         4 + kShortlist);
+}
 template <class C, int D>
 __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, const u32* count_ptr, int first_attempt,
                                                               const u32* active, const C* A, const int* off,
@@ -1590,53 +1615,171 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                                                               unsigned char* state, int* targets, int* flags) {
     constexpr int kWarps = kAttemptThreads / 32;
     __shared__ u64 s_slack[kMaxParts], s_requests[kMaxParts], s_base[kMaxParts], s_avail[kMaxParts];
-    __shared__ u64 s_warp[kWarps][kMaxParts];  // per-warp weight requested per part
+    __shared__ u64 s_warp[kMaxParts][kWarps];  // per part, the weight each warp requests
     __shared__ int s_want[kAttemptCap];
+    __shared__ unsigned char s_order[kMaxParts];  // parts by (room desc, part asc), per attempt
     __shared__ int s_any;
+    extern __shared__ __align__(16) unsigned char attempt_smem_raw[];
     const int count = static_cast<int>(*count_ptr);
+    // Per-donor arrays (j < count), widest first.
+    u64* d_tried = reinterpret_cast<u64*>(attempt_smem_raw);          // 2 per donor
+    C* d_list_c = reinterpret_cast<C*>(d_tried + 2 * count);           // kShortlist per donor
+    C* d_bound = d_list_c + kShortlist * count;                         // largest unlisted affinity
+    u32* d_v = reinterpret_cast<u32*>(d_bound + count);
+    u32* d_w = d_v + count;
+    unsigned char* d_src = reinterpret_cast<unsigned char*>(d_w + count);
+    unsigned char* d_state = d_src + count;
+    unsigned char* d_list_n = d_state + count;  // listed parts; kNoPart: no shortlist yet
+    unsigned char* d_bounded = d_list_n + count;  // 1 when some eligible part is unlisted
+    unsigned char* d_list_p = d_bounded + count;  // kShortlist per donor
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int p = threadIdx.x; p < k; p += blockDim.x) { s_slack[p] = slack[p]; s_requests[p] = requests[p]; }
+    for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        const u32 i = open[j];
+        const u32 v = active[i];
+        d_v[j] = v;
+        d_w[j] = vw[v];
+        d_src[j] = static_cast<unsigned char>(labels[v]);
+        d_state[j] = state[i];
+        d_tried[2 * j] = tried[2 * i];
+        d_tried[2 * j + 1] = tried[2 * i + 1];
+        d_list_n[j] = kNoPart;
+    }
     __syncthreads();
     for (int attempt = first_attempt; attempt < k; ++attempt) {
         if (threadIdx.x == 0) s_any = 0;
         for (int p = threadIdx.x; p < k; p += blockDim.x)
             s_avail[p] = s_requests[p] < s_slack[p] ? s_slack[p] - s_requests[p] : 0;
         __syncthreads();
+        if (attempt > 0 && A) {
+            // Rank of part p: the parts before it, counted by 8 lanes.
+            const int p = threadIdx.x >> 3, sub = threadIdx.x & 7;
+            int rank = 0;
+            if (p < k) {
+                const u64 a = s_avail[p];
+                for (int q = sub; q < k; q += 8) rank += s_avail[q] > a || (s_avail[q] == a && q < p);
+            }
+            rank += __shfl_xor_sync(0xffffffffu, rank, 1);
+            rank += __shfl_xor_sync(0xffffffffu, rank, 2);
+            rank += __shfl_xor_sync(0xffffffffu, rank, 4);
+            if (p < k && sub == 0) s_order[rank] = static_cast<unsigned char>(p);
+            __syncthreads();
+        }
         // Choice (k_choose).
         for (int j = threadIdx.x; j < count; j += blockDim.x) {
-            const u32 i = open[j];
             int target = -1;
-            if (!state[i]) {
-                const int v = static_cast<int>(active[i]);
+            if (!d_state[j]) {
+                const int v = static_cast<int>(d_v[j]);
+                const u64 w = d_w[j];
+                const u64 t0 = d_tried[2 * j], t1 = d_tried[2 * j + 1];
+                auto eligible = [&](int p) {
+                    return !(((p < 64 ? t0 : t1) >> (p & 63)) & 1) && s_avail[p] >= w;
+                };
                 if (attempt == 0) {
                     target = proposal[v];
                 } else if (!A) {  // on-demand affinities
-                    target = choose_od<D>(v, off, nbr, ew, labels, k, vw[v], tried[2 * i], tried[2 * i + 1], s_avail);
+                    target = choose_od<D>(v, off, nbr, ew, labels, k, w, t0, t1, s_avail);
                 } else {
-                    const u64 w = vw[v];
-                    const int src = labels[v];
-                    const u64 t0 = tried[2 * i], t1 = tried[2 * i + 1];
-                    const C* row = A + static_cast<i64>(v) * k;
-                    u64 best = 0, room = 0;
-                    // Sixteen affinities loaded together (one round trip for
-                    // a 16-part slice), then scanned in part order.
-                    for (int p0 = 0; p0 < k; p0 += 16) {
-                        C c16[16];
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) c16[q] = p0 + q < k ? row[p0 + q] : C(0);
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const int p = p0 + q;
-                            if (p >= k) break;
-                            if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+                    bool decided = false;
+                    const int listed = d_list_n[j];
+                    if (listed != kNoPart) {
+                        C best = 0;
+                        u64 room = 0;
+                        for (int q = 0; q < listed; ++q) {
+                            const int p = d_list_p[kShortlist * j + q];
+                            if (!eligible(p)) continue;
+                            const C c = d_list_c[kShortlist * j + q];
                             const u64 avail = s_avail[p];
-                            if (avail < w) continue;
-                            const u64 c = c16[q];
-                            if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                            if (target < 0 || c > best || (c == best && (avail > room || (avail == room && p < target)))) {
+                                target = p;
+                                best = c;
+                                room = avail;
+                            }
+                        }
+                        // Every eligible part listed: the best listed one
+                        // (or none) is the choice.  Otherwise the best must
+                        // beat every unlisted affinity.
+                        decided = !d_bounded[j] || (target >= 0 && best > d_bound[j]);
+                        if (!decided && d_bound[j] == 0 && (target < 0 || best == 0)) {
+                            // Every eligible part has affinity 0 (the unlisted
+                            // ones at most the bound, the listed ones at most
+                            // the best): the one with the most room, the
+                            // lowest part on equal room.
+                            const int src = d_src[j];
+                            target = -1;
+                            for (int r = 0; r < k; ++r) {
+                                const int p = s_order[r];
+                                if (s_avail[p] < w) break;  // the rest have less room
+                                if (p == src || (((p < 64 ? t0 : t1) >> (p & 63)) & 1)) continue;
+                                target = p;
+                                break;
+                            }
+                            decided = true;
                         }
                     }
+                    if (!decided) {
+                        // Full scan of the row: the choice and a new shortlist.
+                        const int src = d_src[j];
+                        const C* row = A + static_cast<i64>(v) * k;
+                        target = -1;
+                        C best = 0, bound = 0;
+                        u64 room = 0;
+                        int n_list = 0;
+                        bool bounded = false;
+                        int lp[kShortlist];
+                        C lc[kShortlist];
+                        // A slice of affinities loaded together (one round
+                        // trip for 64 bytes of the row), then scanned in part
+                        // order.
+                        constexpr int kSlice = 64 / static_cast<int>(sizeof(C));
+                        for (int p0 = 0; p0 < k; p0 += kSlice) {
+                            C slice[kSlice];
+#pragma unroll
+                            for (int q = 0; q < kSlice; ++q) slice[q] = p0 + q < k ? row[p0 + q] : C(0);
+#pragma unroll
+                            for (int q = 0; q < kSlice; ++q) {
+                                const int p = p0 + q;
+                                if (p >= k) break;
+                                if (p == src || !eligible(p)) continue;
+                                const C c = slice[q];
+                                const u64 avail = s_avail[p];
+                                if (target < 0 || c > best || (c == best && avail > room)) { target = p; best = c; room = avail; }
+                                // Shortlist by (affinity desc, part asc): parts
+                                // arrive in ascending order, so a part enters
+                                // only past a strictly smaller affinity.
+                                if (n_list == kShortlist && !(c > lc[kShortlist - 1])) {
+                                    bound = bounded ? (c > bound ? c : bound) : c;
+                                    bounded = true;
+                                    continue;
+                                }
+                                if (n_list == kShortlist) {
+                                    const C out = lc[kShortlist - 1];
+                                    bound = bounded ? (out > bound ? out : bound) : out;
+                                    bounded = true;
+                                } else {
+                                    ++n_list;
+                                }
+                                int at = n_list - 1;
+#pragma unroll
+                                for (int q2 = kShortlist - 1; q2 > 0; --q2)
+                                    if (q2 <= at && lc[q2 - 1] < c) { lc[q2] = lc[q2 - 1]; lp[q2] = lp[q2 - 1]; at = q2 - 1; }
+#pragma unroll
+                                for (int q2 = 0; q2 < kShortlist; ++q2)
+                                    if (q2 == at) { lc[q2] = c; lp[q2] = p; }
+                            }
+                        }
+#pragma unroll
+                        for (int q = 0; q < kShortlist; ++q)
+                            if (q < n_list) {
+                                d_list_p[kShortlist * j + q] = static_cast<unsigned char>(lp[q]);
+                                d_list_c[kShortlist * j + q] = lc[q];
+                            }
+                        d_list_n[j] = static_cast<unsigned char>(n_list);
+                        d_bounded[j] = bounded;
+                        d_bound[j] = bound;
+                    }
                 }
-                if (target < 0) state[i] = 2;
+                if (target < 0) d_state[j] = 2;
                 else s_any = 1;
             }
             s_want[j] = target;
@@ -1648,12 +1791,11 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
         // requests (earlier chunks, earlier warps, earlier lanes).
         for (int p = threadIdx.x; p < k; p += blockDim.x) s_base[p] = s_requests[p];
         for (int chunk = 0; chunk < count; chunk += blockDim.x) {
-            for (int x = threadIdx.x; x < kWarps * k; x += blockDim.x) s_warp[x / k][x % k] = 0;
+            for (int x = threadIdx.x; x < kWarps * k; x += blockDim.x) s_warp[x / kWarps][x % kWarps] = 0;
             __syncthreads();
             const int j = chunk + threadIdx.x;
             const int t = j < count ? s_want[j] : -1;
-            const u32 i = j < count ? open[j] : 0;
-            const u64 w = t >= 0 ? vw[active[i]] : 0;
+            const u64 w = t >= 0 ? d_w[j] : 0;
             const unsigned peers = __match_any_sync(0xffffffffu, t);
             u64 before = 0, sum = 0;
             for (unsigned rest = peers; rest; rest &= rest - 1) {
@@ -1662,23 +1804,34 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
                 sum += o;
                 if (l < lane) before += o;
             }
-            if (t >= 0 && lane == __ffs(peers) - 1) s_warp[warp][t] = sum;
+            if (t >= 0 && lane == __ffs(peers) - 1) s_warp[t][warp] = sum;
             __syncthreads();
-            if (t >= 0) {
-                u64 begin = s_base[t] + before;
-                for (int w2 = 0; w2 < warp; ++w2) begin += s_warp[w2][t];
-                tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
-                if (begin <= s_slack[t] && w <= s_slack[t] - begin) {
-                    targets[active[i]] = t;
-                    flags[active[i]] = 1;
-                    state[i] = 1;
+            // Per part, the weight requested before each warp (from the
+            // running base), and the base for the next chunk: warp `warp`
+            // scans the parts warp, warp + 32, ... across its lanes (lane l
+            // holds warp l's sum).
+            static_assert(kWarps == 32, "one lane per warp of the block");
+            for (int p = warp; p < k; p += kWarps) {
+                const u64 x = s_warp[p][lane], base = s_base[p];
+                u64 inc = x;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u64 o = __shfl_up_sync(0xffffffffu, inc, d);
+                    if (lane >= d) inc += o;
                 }
+                s_warp[p][lane] = base + inc - x;
+                __syncwarp();
+                if (lane == 31) s_base[p] = base + inc;
             }
             __syncthreads();
-            for (int p = threadIdx.x; p < k; p += blockDim.x) {
-                u64 add = 0;
-                for (int w2 = 0; w2 < kWarps; ++w2) add += s_warp[w2][p];
-                s_base[p] += add;
+            if (t >= 0) {
+                const u64 begin = s_warp[t][warp] + before;
+                d_tried[2 * j + (t >> 6)] |= 1ULL << (t & 63);
+                if (begin <= s_slack[t] && w <= s_slack[t] - begin) {
+                    targets[d_v[j]] = t;
+                    flags[d_v[j]] = 1;
+                    d_state[j] = 1;
+                }
             }
             __syncthreads();
         }
@@ -1686,6 +1839,12 @@ __global__ void __launch_bounds__(kAttemptThreads) k_attempts(const u32* open, c
         __syncthreads();
     }
     for (int p = threadIdx.x; p < k; p += blockDim.x) requests[p] = s_requests[p];
+    for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        const u32 i = open[j];
+        state[i] = d_state[j];
+        tried[2 * i] = d_tried[2 * j];
+        tried[2 * i + 1] = d_tried[2 * j + 1];
+    }
 }
 struct IsOpen {
     const unsigned char* state;
@@ -1730,14 +1889,14 @@ __device__ bool joint_same(const JointMove& x, const JointMove& y) {  // joint_s
     }
     return true;
 }
-// Sort keys of a joint move.  (k1, k2), compared as unsigned words in that
-// order, is a monotone projection of the comparator's leading fields: unequal
-// keys decide a comparison the same way the comparator does, and only equal
-// keys need the comparator itself.  A signed field enters as its value
-// clamped to [-2^53, 2^53) with one value for each side beyond, 55 bits; a
-// word that would need a field after a clamped one stops there (zero).
+// Sort keys of a joint move.  (k1, k2, k3, k4), compared as unsigned words
+// in that order, is a monotone projection of the comparator's leading
+// fields: unequal keys decide a comparison the same way the comparator does,
+// and only equal keys need the comparator itself.  A signed field enters as
+// its value clamped to [-2^53, 2^53) with one value for each side beyond, 55
+// bits; the words after a clamped field are zero.
 struct MoveKey {
-    u64 k1, k2;
+    u64 k1, k2, k3, k4;
 };
 constexpr long long kKeyLimit = 1LL << 53;
 __device__ __forceinline__ u64 field_key(long long v, bool descending, bool& clamped) {
@@ -1755,7 +1914,10 @@ struct NetOrder {  // JointNetOrder (complementary_moves.cuh:5-14)
         for (int j = 0; j < x.size; ++j) if (x.vertices[j] != y.vertices[j]) return x.vertices[j] < y.vertices[j];
         return x.id < y.id;
     }
-    // k1 = (a + 1, net ascending), k2 = (gain descending, size).
+    // k1 = (a + 1, net ascending), k2 = (gain descending, size), then the
+    // 32-bit fields vertex 0 + 1, ..., vertex size-1 + 1, id + 2^31, the
+    // first four of them in k3 and k4 (zero-padded): a move of up to three
+    // vertices is then fully keyed.
     __device__ static MoveKey key(const JointMove& x) {
         bool net_clamped, gain_clamped;
         const u64 net = field_key(x.net, false, net_clamped);
@@ -1763,6 +1925,16 @@ struct NetOrder {  // JointNetOrder (complementary_moves.cuh:5-14)
         MoveKey r;
         r.k1 = (static_cast<u64>(x.a + 1) << 55) | net;
         r.k2 = net_clamped ? 0 : (gain << 8) | (gain_clamped ? 0 : static_cast<u64>(x.size));
+        u64 f[4] = {0, 0, 0, 0};
+        if (!net_clamped && !gain_clamped) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                f[j] = j < x.size ? static_cast<u64>(static_cast<u32>(x.vertices[j] + 1))
+                     : j == x.size ? static_cast<u64>(static_cast<u32>(x.id) ^ 0x80000000u)
+                                   : 0;
+        }
+        r.k3 = (f[0] << 32) | f[1];
+        r.k4 = (f[2] << 32) | f[3];
         return r;
     }
 };
@@ -1780,6 +1952,8 @@ struct MoveOrder {  // JointOrder (exchange.cuh:29-36)
         MoveKey r;
         r.k1 = (static_cast<u64>(x.size == 0) << 63) | (static_cast<u64>(x.a + 1) << 55) | gain;
         r.k2 = gain_clamped ? 0 : static_cast<u64>(static_cast<long long>(x.id) + 2147483649LL);
+        r.k3 = 0;
+        r.k4 = 0;
         return r;
     }
 };
@@ -1794,6 +1968,8 @@ __device__ __forceinline__ bool move_before(const MoveKey& kb, const MoveKey& ka
                                             Cmp cmp) {
     if (kb.k1 != ka.k1) return kb.k1 < ka.k1;
     if (kb.k2 != ka.k2) return kb.k2 < ka.k2;
+    if (kb.k3 != ka.k3) return kb.k3 < ka.k3;
+    if (kb.k4 != ka.k4) return kb.k4 < ka.k4;
     return cmp(moves[b], moves[a]);
 }
 
@@ -2694,7 +2870,14 @@ bool LevelRefiner<T>::repair() {
                 // Small sets of open donors finish all their attempts in one block.
                 auto finish_in_block = [&](int first_attempt) {
                     auto go = [&](auto d) {
-                        launch(k_attempts<T, decltype(d)::value>, 1, kAttemptThreads, 0, s(), static_cast<const u32*>(open),
+                        // Sized for kAttemptCap donors (the count is on the
+                        // device); the limit is set on every call, as it
+                        // belongs to the kernel on whichever device is current.
+                        constexpr size_t smem = attempt_smem<T>(kAttemptCap);
+                        GP_CUDA(cudaFuncSetAttribute(k_attempts<T, decltype(d)::value>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     static_cast<int>(smem)));
+                        launch(k_attempts<T, decltype(d)::value>, 1, kAttemptThreads, smem, s(), static_cast<const u32*>(open),
                                static_cast<const u32*>(open_count), first_attempt, static_cast<const u32*>(active),
                                static_cast<const T*>(A), static_cast<const int*>(g.off), static_cast<const int*>(g.nbr),
                                static_cast<const u32*>(g.ew), static_cast<const int*>(labels), g.vw, k,
