@@ -2039,14 +2039,16 @@ __global__ void __launch_bounds__(1024) k_bitonic_local(int size, int count, con
             bitonic_step_smem(seg, base, count, kk, jj, moves, s_key, s_idx, cmp);
     for (int i = threadIdx.x; i < seg; i += blockDim.x) idx[base + i] = s_idx[i];
 }
-// A whole sort of up to kBitonicSegment moves in one block: keys, the full
-// network in shared memory (the same steps as k_bitonic_local over one
-// segment) and the gather of the sorted moves.
+// A whole sort of up to kBitonicSegment moves in one block: the full network
+// over indices in shared memory (the same compare-exchange steps as
+// k_bitonic_local over one segment) and the gather of the sorted moves.
+// The keys stay in place, indexed by move, so an exchange writes two
+// indices and no keys.
 template <class Cmp>
 __global__ void __launch_bounds__(1024) k_sort_moves_block(int size, int count, const JointMove* in, JointMove* out,
                                                           Cmp cmp) {
     extern __shared__ __align__(16) unsigned char bitonic_smem[];
-    MoveKey* s_key = reinterpret_cast<MoveKey*>(bitonic_smem);
+    MoveKey* s_key = reinterpret_cast<MoveKey*>(bitonic_smem);  // by move
     int* s_idx = reinterpret_cast<int*>(s_key + size);
     for (int i = threadIdx.x; i < size; i += blockDim.x) {
         s_idx[i] = i;
@@ -2054,7 +2056,22 @@ __global__ void __launch_bounds__(1024) k_sort_moves_block(int size, int count, 
     }
     __syncthreads();
     for (int kk = 2; kk <= size; kk <<= 1)
-        for (int jj = kk >> 1; jj; jj >>= 1) bitonic_step_smem(size, 0, count, kk, jj, in, s_key, s_idx, cmp);
+        for (int jj = kk >> 1; jj; jj >>= 1) {
+            for (int p = threadIdx.x; p < size / 2; p += blockDim.x) {
+                const int i = (p / jj) * 2 * jj + p % jj;
+                const int x = i + jj;
+                const int a = s_idx[i], b = s_idx[x];
+                bool greater;
+                if (a >= count) greater = b < count;
+                else if (b >= count) greater = false;
+                else greater = move_before(s_key[b], s_key[a], in, b, a, cmp);
+                if (greater == ((i & kk) == 0)) {
+                    s_idx[i] = b;
+                    s_idx[x] = a;
+                }
+            }
+            __syncthreads();
+        }
     for (int i = threadIdx.x; i < count; i += blockDim.x) out[i] = in[s_idx[i]];
 }
 __global__ void k_iota(int n, int* idx) {
