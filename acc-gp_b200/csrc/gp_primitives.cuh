@@ -110,7 +110,23 @@ __global__ void k_scan_small(i64 count, T* values, T* total) {
     if (threadIdx.x == 0 && total) *total = carry;
 }
 
-template <class T, class In>
+// Up to this many tiles, the writing pass of a scan or selection takes each
+// tile's start from the raw tile sums (every block adds up the sums before
+// it) instead of a separate launch that scans them.
+constexpr int kDirectScanTiles = 256;
+
+// sums[0] + ... + sums[tiles - 1], by the whole block; every thread gets it.
+template <class T>
+__device__ __forceinline__ T sum_before(const T* sums, int tiles, T* smem /* >= 9 */) {
+    T local = 0;
+    for (int t = threadIdx.x; t < tiles; t += kScanThreads) local += sums[t];
+    T total;
+    block_exclusive_scan<T>(local, total, smem);
+    return total;
+}
+
+// Direct: `offsets` holds the tile sums, not their exclusive scan.
+template <class T, class In, bool Direct = false>
 __global__ void k_scan_tiles(i64 n, In in, const T* offsets, T* out, T* total) {
     __shared__ T smem[9];
     const i64 base = static_cast<i64>(blockIdx.x) * kScanTile;
@@ -123,8 +139,10 @@ __global__ void k_scan_tiles(i64 n, In in, const T* offsets, T* out, T* total) {
         v[j] = i < n ? in(i) : T(0);
         local += v[j];
     }
+    T start = T(0);
+    if (offsets) start = Direct ? sum_before(offsets, static_cast<int>(blockIdx.x), smem) : offsets[blockIdx.x];
     T tile_total;
-    T run = block_exclusive_scan<T>(local, tile_total, smem) + (offsets ? offsets[blockIdx.x] : T(0));
+    T run = block_exclusive_scan<T>(local, tile_total, smem) + start;
 #pragma unroll
     for (int j = 0; j < kScanItems; ++j) {
         const i64 i = base + static_cast<i64>(threadIdx.x) * kScanItems + j;
@@ -156,6 +174,10 @@ void exclusive_scan(Arena& arena, cudaStream_t s, i64 n, In in, T* out, T* total
     ArenaScope scope(arena);
     T* sums = arena.alloc<T>(static_cast<size_t>(tiles));
     launch(k_tile_sums<T, In>, tiles, kScanThreads, 0, s, n, in, sums);
+    if (tiles <= kDirectScanTiles) {
+        launch(k_scan_tiles<T, In, true>, tiles, kScanThreads, 0, s, n, in, static_cast<const T*>(sums), out, total);
+        return;
+    }
     launch(k_scan_small<T>, 1, kScanThreads, 0, s, tiles, sums, static_cast<T*>(nullptr));
     launch(k_scan_tiles<T, In>, tiles, kScanThreads, 0, s, n, in, sums, out, total);
 }
@@ -177,7 +199,7 @@ __global__ void k_select_count(i64 n, Pred pred, u32* counts) {
     if (threadIdx.x == 0) counts[blockIdx.x] = total;
 }
 
-template <class Pred, class Out>
+template <class Pred, class Out, bool Direct = false>
 __global__ void k_select_write(i64 n, Pred pred, const u32* offsets, Out out, u32* count) {
     __shared__ u32 smem[9];
     const i64 base = static_cast<i64>(blockIdx.x) * kScanTile;
@@ -189,8 +211,10 @@ __global__ void k_select_write(i64 n, Pred pred, const u32* offsets, Out out, u3
         f[j] = i < n && pred(i);
         local += f[j];
     }
+    u32 start = 0;
+    if (offsets) start = Direct ? sum_before(offsets, static_cast<int>(blockIdx.x), smem) : offsets[blockIdx.x];
     u32 total;
-    u32 run = block_exclusive_scan<u32>(local, total, smem) + (offsets ? offsets[blockIdx.x] : 0u);
+    u32 run = block_exclusive_scan<u32>(local, total, smem) + start;
 #pragma unroll
     for (int j = 0; j < kScanItems; ++j) {
         const i64 i = base + static_cast<i64>(threadIdx.x) * kScanItems + j;
@@ -220,6 +244,11 @@ void select_if(Arena& arena, cudaStream_t s, i64 n, Pred pred, Out out, u32* cou
     ArenaScope scope(arena);
     u32* counts = arena.alloc<u32>(static_cast<size_t>(tiles));
     launch(k_select_count<Pred>, tiles, kScanThreads, 0, s, n, pred, counts);
+    if (tiles <= kDirectScanTiles) {
+        launch(k_select_write<Pred, Out, true>, tiles, kScanThreads, 0, s, n, pred, static_cast<const u32*>(counts), out,
+               count);
+        return;
+    }
     launch(k_scan_small<u32>, 1, kScanThreads, 0, s, tiles, counts, static_cast<u32*>(nullptr));
     launch(k_select_write<Pred, Out>, tiles, kScanThreads, 0, s, n, pred, counts, out, count);
 }
