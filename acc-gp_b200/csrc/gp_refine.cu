@@ -2953,15 +2953,18 @@ bool LevelRefiner<T>::repair() {
                         break;
                     }
                 }
-                // Movers = placed donors, in repair order.
-                select_if(A_, s(), acount, IsPlaced{state}, WriteActiveVertex{active, movers}, donor_count);
-                GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                // Movers = placed donors, in repair order, applied with their
+                // count left on the device (counters[9], whose upper half
+                // stays zero): one read-back brings the count and the
+                // batch's counters together.  An empty batch changes nothing
+                // on the device.
+                select_if(A_, s(), acount, IsPlaced{state}, WriteActiveVertex{active, movers},
+                          reinterpret_cast<u32*>(counters + 9));
+                apply(movers, counters + 9, acount, false, samples != nullptr);
+                GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 8 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
                 GP_CUDA(cudaStreamSynchronize(s()));
-                placed = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+                placed = static_cast<i64>(ctx.host_scalars[7] & 0xffffffffULL);
                 if (placed) {
-                    apply(movers, nullptr, placed, false, samples != nullptr);
-                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 6 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
-                    GP_CUDA(cudaStreamSynchronize(s()));
                     delta = settled_delta(ctx.host_scalars);
                     max_load_host = ctx.host_scalars[1];
                     stats.accepted += static_cast<u64>(placed);
@@ -3019,14 +3022,16 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
         using Cmp = decltype(cmp);
         int size = 1;
         while (size < count) size <<= 1;
-        // (Shared-memory limits are set on every call that needs more than
-        // the default: they belong to the kernel, on whichever device is
-        // current.)
+        // (Shared-memory limits are set to one value for every size, on every
+        // call that needs more than the default: the limit belongs to the
+        // kernel for the whole process, on whichever device is current, and
+        // concurrent worker contexts must not lower it under each other's
+        // launches.)
         if (size <= kBitonicSegment) {
             const size_t smem = kBitonicEntryBytes * size;
             if (smem > 48 * 1024)
                 GP_CUDA(cudaFuncSetAttribute(k_sort_moves_block<Cmp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
+                                             static_cast<int>(kBitonicEntryBytes * kBitonicSegment)));
             launch(k_sort_moves_block<Cmp>, 1, 1024, smem, s(), size, count, static_cast<const JointMove*>(in), out,
                    cmp);
             return;
@@ -3105,13 +3110,16 @@ void LevelRefiner<T>::exchange(u64& best_cut) {
                static_cast<const u64*>(events), static_cast<const u64*>(loads), C, stops);
         launch(k_accept, blocks_for(active, kThreads), kThreads, 0, s(), active, static_cast<const JointMove*>(act_sorted),
                static_cast<const int*>(stops), flags);
-        select_if(A_, s(), n, Flagged{flags}, WriteIndex{movers}, cnt);
-        const i64 count = read_count();
+        // The accepted moves applied with their count left on the device
+        // (as the repair does): one read-back for the count and the
+        // batch's counters; an empty batch changes nothing.
+        select_if(A_, s(), n, Flagged{flags}, WriteIndex{movers}, reinterpret_cast<u32*>(counters + 9));
+        apply(movers, counters + 9, n, false, false);
+        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 8 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
+        GP_CUDA(cudaStreamSynchronize(s()));
+        const i64 count = static_cast<i64>(ctx.host_scalars[7] & 0xffffffffULL);
         if (!count) { if (++empty >= 2) break; continue; }
         empty = 0;
-        apply(movers, nullptr, count, false, false);
-        GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 2, 6 * sizeof(u64), cudaMemcpyDeviceToHost, s()));
-        GP_CUDA(cudaStreamSynchronize(s()));
         const long long delta = settled_delta(ctx.host_scalars);
         max_load_host = ctx.host_scalars[1];
         account(delta);
@@ -3167,8 +3175,10 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     flags = A_.alloc<int>(n);
     cand = A_.alloc<int>(n);
     movers = A_.alloc<int>(n);
-    counters = A_.alloc<u64>(9);  // [8]: k_commit's finished-block count, zero between launches
-    GP_CUDA(cudaMemsetAsync(counters + 8, 0, sizeof(u64), s()));
+    // [8]: k_commit's finished-block count, zero between launches; [9]: the
+    // repair's placed-donor count (a 32-bit count in a zeroed word).
+    counters = A_.alloc<u64>(10);
+    GP_CUDA(cudaMemsetAsync(counters + 8, 0, 2 * sizeof(u64), s()));
     corr_acc = A_.alloc<long long>(g.heavy_count + 1);
     if (g.chunks) {
         chunk_work = A_.alloc<int>(g.chunks);
