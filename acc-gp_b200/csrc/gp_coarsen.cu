@@ -682,6 +682,38 @@ __global__ void k_key_target(i64 count, const u32* items, const int* targets, u6
     if (i < count) keys[i] = static_cast<u64>(targets[items[i]]);
 }
 
+// order_by_target for at most one sort tile of items, in one block: each of
+// the three stable stages builds its keys from the current order and sorts
+// them in shared memory, the same passes the separate launches make.
+__global__ void __launch_bounds__(kSortThreads) k_order_small(int count, u32* items, const u32* ties,
+                                                             const u64* key_values, u64 mask, int key_bits,
+                                                             const int* targets, int target_bits) {
+    __shared__ SortTileSmem sm;
+    u64 k[kSortItems];
+    u32 v[kSortItems];
+    bool valid[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const i64 i = sort_index(0, j);
+        valid[j] = i < count;
+        v[j] = valid[j] ? items[i] : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) k[j] = valid[j] ? static_cast<u64>(~ties[v[j]]) : 0;
+    tile_sort_passes<true>(sm, k, v, valid, 0, 32);
+    if (key_bits > 0) {
+#pragma unroll
+        for (int j = 0; j < kSortItems; ++j) k[j] = valid[j] ? mask - (key_values[v[j]] & mask) : 0;
+        tile_sort_passes<true>(sm, k, v, valid, 0, key_bits);
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) k[j] = valid[j] ? static_cast<u64>(targets[v[j]]) : 0;
+    tile_sort_passes<true>(sm, k, v, valid, 0, target_bits);
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j)
+        if (valid[j]) items[sort_index(0, j)] = v[j];
+}
+
 // Segment heads of an ordered list grouped by target.
 __global__ void k_segment_heads(i64 count, const u32* items, const int* targets, const u64* prefix, u64* segment_base,
                                 int* segment_first) {
@@ -863,19 +895,37 @@ __global__ void k_row_base(i64 n, const int* off, const int* map, int* cursor, i
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (v < n) base[v] = atomicAdd(cursor + map[v], off[v + 1] - off[v]);
 }
+// W lanes per fine row (8 for short rows, 32 when rows are long, so that a
+// level of few dense rows still has enough memory requests in flight), four
+// entries per lane at a time.
+template <int W>
 __global__ void k_scatter(i64 n, const int* off, const int* nbr, const u32* ew, const int* map, const int* base,
                           int* raw_t, u32* raw_w) {
-    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
-    const int lane = threadIdx.x & 7;
+    constexpr int U = 4;
+    const i64 v = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+    const int lane = threadIdx.x % W;
     if (v >= n) return;
     const int begin = off[v], end = off[v + 1];
     if (end - begin > kHeavyRow) return;
     const int c = map[v];
     const int out = base[v] - begin;
-    for (int e = begin + lane; e < end; e += 8) {
-        const int t = map[nbr[e]];
-        raw_t[out + e] = t == c ? INT_MAX : t;
-        raw_w[out + e] = edge_w(ew, e);
+    for (int e0 = begin + lane; e0 < end; e0 += U * W) {
+        int u[U], t[U];
+        u32 w[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) u[j] = e0 + j * W < end ? nbr[e0 + j * W] : 0;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const bool in = e0 + j * W < end;
+            t[j] = in ? map[u[j]] : 0;
+            w[j] = in ? edge_w(ew, e0 + j * W) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (e0 + j * W < end) {
+                raw_t[out + e0 + j * W] = t[j] == c ? INT_MAX : t[j];
+                raw_w[out + e0 + j * W] = w[j];
+            }
     }
 }
 __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int* raw_t, u32* raw_w) {
@@ -889,9 +939,9 @@ __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int*
     }
 }
 
-// Row classes: 0 <= 128 raw entries, 1 <= 512, 2 <= 4096, 3 <= 8192, 4 larger;
-// sc[5] counts the records of class 4.
-constexpr int kRowClasses = 7;  // raw row sizes: <=128, <=512, <=1024, <=2048, <=4096, <=8192, larger
+// Row classes by raw size: 0 <= 128 entries, 1 <= 512, 2 <= 1024, 3 <= 2048,
+// 4 <= 4096, 5 <= 8192, 6 larger; sc[kRowClasses] counts the records of class 6.
+constexpr int kRowClasses = 7;
 __global__ void k_row_classes(i64 nc, const int* raw, int* lists, i64 stride, u64* sc) {
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int r = c < nc ? raw[c] : 0;
@@ -1265,17 +1315,32 @@ __global__ void k_large_counts(i64 count, const int* rows, const int* rec_off, c
     ucount[rows[j]] = static_cast<int>(last - first);
 }
 
-// contraction_copy_rows (contraction_rows.cuh:140-154); heavy coarse rows by chunks.
+// contraction_copy_rows (contraction_rows.cuh:140-154); heavy coarse rows by
+// chunks.  W lanes per row as in k_scatter.
+template <int W>
 __global__ void k_copy_rows(i64 nc, const int* raw_off, const int* raw_t, const u32* raw_w, const int* off, int* nbr,
                             u32* ew) {
-    const i64 c = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
-    const int lane = threadIdx.x & 7;
+    constexpr int U = 4;
+    const i64 c = (static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x) / W;
+    const int lane = threadIdx.x % W;
     if (c >= nc) return;
     const int begin = off[c], end = off[c + 1], raw = raw_off[c];
     if (end - begin > kHeavyRow) return;
-    for (int e = begin + lane; e < end; e += 8) {
-        nbr[e] = raw_t[raw + e - begin];
-        ew[e] = raw_w[raw + e - begin];
+    for (int e0 = begin + lane; e0 < end; e0 += U * W) {
+        int t[U];
+        u32 w[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const bool in = e0 + j * W < end;
+            t[j] = in ? raw_t[raw + e0 + j * W - begin] : 0;
+            w[j] = in ? raw_w[raw + e0 + j * W - begin] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (e0 + j * W < end) {
+                nbr[e0 + j * W] = t[j];
+                ew[e0 + j * W] = w[j];
+            }
     }
 }
 __global__ void k_copy_chunks(DGraph g, const int* raw_off, const int* raw_t, const u32* raw_w) {
@@ -1344,9 +1409,16 @@ struct AggregateOut {
 constexpr int kThreads = 256;
 
 // Orders `items` (vertex ids, `count` of them, ascending on entry) by
-// (target asc, key desc, tie desc): three stable LSD stages.
+// (target asc, key desc, tie desc): three stable LSD stages (one block for at
+// most one sort tile).
 void order_by_target(Context& ctx, i64 count, u32*& items, u32*& items_alt, const int* targets, const u64* key_values,
                      int key_bits, const u32* ties, int target_bits) {
+    if (count <= kSortTile) {
+        const u64 mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
+        launch(k_order_small, 1, kSortThreads, 0, ctx.stream, static_cast<int>(count), items, ties, key_values, mask,
+               key_bits, targets, target_bits);
+        return;
+    }
     Arena& A = ctx.scratch;
     ArenaScope scope(A);
     u64* keys = A.alloc<u64>(static_cast<size_t>(count));
@@ -1692,8 +1764,14 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
         ArenaScope bs(A);
         int* base = A.alloc<int>(n);
         launch(k_row_base, vb, kThreads, 0, s, n, fine.off, agg.map, cursor, base);
-        launch(k_scatter, blocks_for(n * 8, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map,
-               static_cast<const int*>(base), raw_t, raw_w);
+        // A warp per row when the light rows (at most kHeavyRow entries; the
+        // heavier ones go by chunks) average more than 64 entries.
+        if (fine.m - fine.heavy_entries > 64 * (n - fine.heavy_count))
+            launch(k_scatter<32>, blocks_for(n * 32, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map,
+                   static_cast<const int*>(base), raw_t, raw_w);
+        else
+            launch(k_scatter<8>, blocks_for(n * 8, kThreads), kThreads, 0, s, n, fine.off, fine.nbr, fine.ew, agg.map,
+                   static_cast<const int*>(base), raw_t, raw_w);
         if (fine.chunks)
             launch(k_scatter_chunks, static_cast<int>(fine.chunks), 256, 0, s, fine, agg.map,
                    static_cast<const int*>(base), raw_t, raw_w);
@@ -1713,15 +1791,14 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     if (count[1])
         launch(k_sort_rows_warp<true>, blocks_for(count[1] * 32, kThreads), kThreads, 0, s, count[1], lists + nc,
                raw_off, raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
-    if (count[2])
-        launch(k_sort_rows_block<4>, static_cast<int>(count[2]), 256, 0, s, lists + 2 * nc, raw_off, raw_t, raw_w,
+    auto sort_block = [&](auto items, int cls) {
+        constexpr int I = decltype(items)::value;
+        launch(k_sort_rows_block<I>, static_cast<int>(count[cls]), 256, 0, s, lists + cls * nc, raw_off, raw_t, raw_w,
                ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
-    if (count[3])
-        launch(k_sort_rows_block<8>, static_cast<int>(count[3]), 256, 0, s, lists + 3 * nc, raw_off, raw_t, raw_w,
-               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
-    if (count[4])
-        launch(k_sort_rows_block<16>, static_cast<int>(count[4]), 256, 0, s, lists + 4 * nc, raw_off, raw_t, raw_w,
-               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
+    };
+    if (count[2]) sort_block(std::integral_constant<int, 4>{}, 2);
+    if (count[3]) sort_block(std::integral_constant<int, 8>{}, 3);
+    if (count[4]) sort_block(std::integral_constant<int, 16>{}, 4);
     if (count[5]) {
         // Set on every call (one fixed value): the attribute belongs to the
         // kernel, on whichever device is current.
@@ -1772,8 +1849,12 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     coarse.nbr = ctx.persist.alloc<int>(coarse.m);
     coarse.ew = ctx.persist.alloc<u32>(coarse.m);
     build_chunks(ctx, coarse);
-    launch(k_copy_rows, blocks_for(nc * 8, kThreads), kThreads, 0, s, nc, raw_off, raw_t, raw_w, coarse.off,
-           coarse.nbr, coarse.ew);
+    if (coarse.m - coarse.heavy_entries > 64 * (nc - coarse.heavy_count))
+        launch(k_copy_rows<32>, blocks_for(nc * 32, kThreads), kThreads, 0, s, nc, raw_off, raw_t, raw_w, coarse.off,
+               coarse.nbr, coarse.ew);
+    else
+        launch(k_copy_rows<8>, blocks_for(nc * 8, kThreads), kThreads, 0, s, nc, raw_off, raw_t, raw_w, coarse.off,
+               coarse.nbr, coarse.ew);
     if (coarse.chunks)
         launch(k_copy_chunks, static_cast<int>(coarse.chunks), 256, 0, s, coarse, static_cast<const int*>(raw_off),
                static_cast<const int*>(raw_t), static_cast<const u32*>(raw_w));

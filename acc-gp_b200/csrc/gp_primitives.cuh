@@ -432,21 +432,12 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_downsweep(i64 count, con
     }
 }
 
-// Whole sort of at most one tile by one block: every pass reorders the items
-// in shared memory; the result is written back in place.
+// The LSD passes over bits [begin_bit, end_bit) of one tile held in
+// registers in the sort_index layout: every pass reorders the items through
+// shared memory.
 template <bool WithValues>
-__global__ void __launch_bounds__(kSortThreads) k_radix_tile_sort(int count, u64* keys, u32* vals, int begin_bit, int end_bit) {
-    __shared__ SortTileSmem sm;
-    u64 k[kSortItems];
-    u32 v[kSortItems];
-    bool valid[kSortItems];
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const i64 i = sort_index(0, j);
-        valid[j] = i < count;
-        k[j] = valid[j] ? keys[i] : 0;
-        if (WithValues) v[j] = valid[j] ? vals[i] : 0;
-    }
+__device__ __forceinline__ void tile_sort_passes(SortTileSmem& sm, u64 (&k)[kSortItems], u32 (&v)[kSortItems],
+                                                 const bool (&valid)[kSortItems], int begin_bit, int end_bit) {
     for (int shift = begin_bit; shift < end_bit; shift += kRadixBits) {
         u32 pos[kSortItems];
         int digit[kSortItems];
@@ -467,6 +458,24 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_tile_sort(int count, u64
         }
         __syncthreads();
     }
+}
+
+// Whole sort of at most one tile by one block; the result is written back in
+// place.
+template <bool WithValues>
+__global__ void __launch_bounds__(kSortThreads) k_radix_tile_sort(int count, u64* keys, u32* vals, int begin_bit, int end_bit) {
+    __shared__ SortTileSmem sm;
+    u64 k[kSortItems];
+    u32 v[kSortItems];
+    bool valid[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const i64 i = sort_index(0, j);
+        valid[j] = i < count;
+        k[j] = valid[j] ? keys[i] : 0;
+        if (WithValues) v[j] = valid[j] ? vals[i] : 0;
+    }
+    tile_sort_passes<WithValues>(sm, k, v, valid, begin_bit, end_bit);
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         if (!valid[j]) continue;
