@@ -2298,13 +2298,26 @@ __global__ void k_combine(int count, const JointMove* archive, const int* off, c
         out[i] = y;
         out[count + i] = empty_move();
     }
+    // First position whose move does not come before (x.a, net) (after it,
+    // with upper).  The warp probes 32 evenly spaced positions at once, so
+    // each round trip narrows the range 32-fold; the answer is the binary
+    // search's (the predicate holds on a prefix of the sorted fragments).
     auto bound = [&](long long net, bool upper) {
-        int l = 0, h = count;
+        int l = 0, h = count;  // the answer lies in [l, h]
         while (l < h) {
-            const int mid = (l + h) / 2;
-            const JointMove& y = archive[mid];
-            if (y.a < x.a || (y.a == x.a && (y.net < net || (upper && y.net == net)))) l = mid + 1;
-            else h = mid;
+            const int p = l + static_cast<int>((static_cast<long long>(h - l) * lane) / 32);
+            bool before = false;
+            if (p < h) {
+                const JointMove& y = archive[p];
+                before = y.a < x.a || (y.a == x.a && (y.net < net || (upper && y.net == net)));
+            }
+            const unsigned yes = __ballot_sync(0xffffffffu, before);
+            if (!yes) return l;  // position l already does not come before
+            const int last = 31 - __clz(yes);
+            const int lp = __shfl_sync(0xffffffffu, p, last);
+            const int np = last < 31 ? __shfl_sync(0xffffffffu, p, last + 1) : h;
+            l = lp + 1;
+            h = np > l ? np : l;
         }
         return l;
     };
@@ -2342,16 +2355,25 @@ __global__ void k_combine(int count, const JointMove* archive, const int* off, c
         for (int u = 0; u < x.size; ++u) {
             const int v = x.vertices[u];
             const int lv = labels[v];
-            for (int e = off[v] + lane; e < off[v + 1]; e += 32) {
-                const int w = nbr[e];
-                unsigned hit = 0;
+            const int end = off[v + 1];
+            // Four entries per lane in flight.
+            for (int e0 = off[v] + lane; e0 < end; e0 += 4 * 32) {
+                int w4[4];
 #pragma unroll
-                for (int q = 0; q < 32; ++q) hit |= w == yv[q] ? 1u << (q >> 3) : 0u;
-                if (!hit) continue;
-                const long long contrib = (lv == labels[w] ? 2LL : -2LL) * edge_w(ew, e);
+                for (int j = 0; j < 4; ++j) w4[j] = e0 + 32 * j < end ? nbr[e0 + 32 * j] : -1;
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (hit & (1u << c)) correction[c] += contrib;
+                for (int j = 0; j < 4; ++j) {
+                    const int w = w4[j];
+                    if (w < 0) continue;
+                    unsigned hit = 0;
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) hit |= w == yv[q] ? 1u << (q >> 3) : 0u;
+                    if (!hit) continue;
+                    const long long contrib = (lv == labels[w] ? 2LL : -2LL) * edge_w(ew, e0 + 32 * j);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (hit & (1u << c)) correction[c] += contrib;
+                }
             }
         }
     }
