@@ -328,7 +328,28 @@ struct LpParams {
     int* movers;
     u64* counters;  // 0 candidates, 1 movers, 2 delta (signed), 3 max load
     int heavy_min;  // rows longer than this go through the chunk kernels
+    u64* proposal;  // per vertex, the round's proposal packed for the filter (below)
 };
+
+// A vertex's proposal of the round in one word, written by the proposal
+// kernels for every vertex they visit and read by the priority filter for
+// each neighbour, one 8-byte gather instead of the target, gain and label
+// gathers: bits 0-7 the label, 8-15 the target, bit 16 set for a proposer,
+// bit 17 set when the gain does not fit the 46-bit field in bits 18-63 (the
+// filter then reads the gain array).  0: not proposing.  Vertices the
+// proposals do not visit (outside the frontier) keep the 0 written at the
+// start of the level, as their targets stay -1.
+constexpr u64 kProposer = 1ULL << 16, kGainApart = 1ULL << 17;
+constexpr long long kPackedGainLimit = 1LL << 45;
+__device__ __forceinline__ u64 pack_proposal(int label, int target, long long gain) {
+    if (target < 0) return 0;
+    const u64 head = static_cast<u64>(label & 0xff) | (static_cast<u64>(target & 0xff) << 8) | kProposer;
+    if (gain < -kPackedGainLimit || gain >= kPackedGainLimit) return head | kGainApart;
+    return head | (static_cast<u64>(gain) << 18);
+}
+__device__ __forceinline__ long long packed_gain(u64 w, const long long* gains, int u) {
+    return (w & kGainApart) ? gains[u] : static_cast<long long>(w) >> 18;
+}
 
 // incremental_lp_proposal (incremental.cuh:166-198).  A warp takes 32
 // consecutive vertices: each lane reads its vertex's lock, label, own-part
@@ -372,7 +393,10 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
             }
             // A gain is read only where the target is set, so only
             // proposers write one.
-            if (!act) q.targets[v] = -1;
+            if (!act) {
+                q.targets[v] = -1;
+                q.proposal[v] = 0;
+            }
         }
         s_propose[threadIdx.x] = 0;
         __syncwarp();
@@ -430,8 +454,9 @@ __global__ void __launch_bounds__(kThreads) k_proposals(LpParams q, const C* A, 
             if (owner >= 0 && sub == 0) {
                 const bool propose = target >= 0 && (best >= ocur || ocur - best < static_cast<u64>(q.filter * static_cast<double>(ocur)));
                 q.targets[vv] = propose ? target : -1;
-                if (propose)
-                    q.gains[vv] = best >= ocur ? static_cast<long long>(best - ocur) : -static_cast<long long>(ocur - best);
+                const long long gain = best >= ocur ? static_cast<long long>(best - ocur) : -static_cast<long long>(ocur - best);
+                if (propose) q.gains[vv] = gain;
+                q.proposal[vv] = pack_proposal(osrc, propose ? target : -1, gain);
                 s_propose[(threadIdx.x & ~31) + owner] = propose;
             }
         }
@@ -510,6 +535,7 @@ __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q, const int
             if (q.locks[v]) {
                 q.locks[v] = 0;
                 q.targets[v] = -1;
+                q.proposal[v] = 0;
             } else {
                 const int src = q.labels[v];
                 RowRegs<D> r;
@@ -540,8 +566,10 @@ __global__ void __launch_bounds__(kThreads) k_proposals_od(LpParams q, const int
                 propose = target >= 0 &&
                           (best >= current || current - best < static_cast<u64>(q.filter * static_cast<double>(current)));
                 q.targets[v] = propose ? target : -1;
-                if (propose)
-                    q.gains[v] = best >= current ? static_cast<long long>(best - current) : -static_cast<long long>(current - best);
+                const long long gain =
+                    best >= current ? static_cast<long long>(best - current) : -static_cast<long long>(current - best);
+                if (propose) q.gains[v] = gain;
+                q.proposal[v] = pack_proposal(src, propose ? target : -1, gain);
             }
         }
         block_append(static_cast<int>(v), propose, q.cand, q.counters + 0);
@@ -557,22 +585,22 @@ __device__ __forceinline__ long long filter_entries(const LpParams& q, int v, in
     constexpr int U = 4;
     long long corr = 0;
     for (int e0 = first; e0 < end; e0 += U * stride) {
-        int u[U], tu[U], lu[U];
-        long long gu[U];
+        int u[U];
+        u64 w[U];
 #pragma unroll
         for (int j = 0; j < U; ++j) u[j] = e0 + j * stride < end ? q.nbr[e0 + j * stride] : v;
 #pragma unroll
-        for (int j = 0; j < U; ++j) {
-            const bool real = u[j] != v;
-            tu[j] = real ? q.targets[u[j]] : -1;
-            lu[j] = real ? q.labels[u[j]] : 0;
-            gu[j] = real ? q.gains[u[j]] : 0;
-        }
+        for (int j = 0; j < U; ++j) w[j] = u[j] != v ? q.proposal[u[j]] : 0;
 #pragma unroll
-        for (int j = 0; j < U; ++j)
-            if (tu[j] >= 0 && (gu[j] > gain || (gu[j] == gain && u[j] < v)))
+        for (int j = 0; j < U; ++j) {
+            if (!(w[j] & kProposer)) continue;
+            const long long gu = packed_gain(w[j], q.gains, u[j]);
+            if (gu > gain || (gu == gain && u[j] < v)) {
+                const int tu = static_cast<int>((w[j] >> 8) & 0xffu), lu = static_cast<int>(w[j] & 0xffu);
                 corr += static_cast<long long>(edge_w(q.ew, e0 + j * stride)) *
-                        ((tu[j] == t) - (tu[j] == s) - (lu[j] == t) + (lu[j] == s));
+                        ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+            }
+        }
     }
     return corr;
 }
@@ -2575,6 +2603,7 @@ private:
     T* totals = nullptr;
     int* targets = nullptr;
     long long* gains = nullptr;
+    u64* proposal = nullptr;  // packed proposals for the filter (pack_proposal)
     unsigned char* locks = nullptr;
     int* flags = nullptr;
     int* cand = nullptr;
@@ -2789,8 +2818,8 @@ private:
 template <class T>
 void LevelRefiner<T>::enqueue_lp_round(double filter) {
     GP_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(u64), s()));  // [0..1] here, [2..7] for apply
-    LpParams q{n,     k,      C,     filter, g.off, g.nbr, g.ew,   g.vw,     labels, loads,
-               prices, targets, gains, locks, flags, cand,  movers, counters, g.heavy_min};
+    LpParams q{n,     k,      C,     filter, g.off, g.nbr, g.ew,   g.vw,     labels,     loads,
+               prices, targets, gains, locks, flags, cand,  movers, counters, g.heavy_min, proposal};
     proposals(q);
     if (on_demand)
         with_row_size([&](auto d) { launch(k_filter_od<decltype(d)::value>, grid_for(n, kThreads), kThreads, 0, s(), q); });
@@ -3193,6 +3222,8 @@ LevelResult LevelRefiner<T>::run(bool has_known, u64 known) {
     }
     targets = A_.alloc<int>(n);
     gains = A_.alloc<long long>(n);
+    proposal = A_.alloc<u64>(n);
+    GP_CUDA(cudaMemsetAsync(proposal, 0, sizeof(u64) * n, s()));
     locks = A_.alloc<unsigned char>(n);
     flags = A_.alloc<int>(n);
     cand = A_.alloc<int>(n);
