@@ -232,6 +232,7 @@ struct RoundParams {
     const int* clusters;
     const u64* cw;
     const unsigned char* roles;
+    const u64* recv;  // per cluster: its weight, or all ones when its role excludes it (k_roles)
     u64 capacity;
     u32 tie_salt;
     bool filter_roles;  // receivers only, with admissibility
@@ -243,12 +244,18 @@ struct RoundParams {
 };
 
 // residual_freeze_roles (singleton_growth.cuh:27-40); also resets proposals.
+// Also writes recv[v], the cluster weight with the role folded in (all ones
+// for a mover, which no capacity admits), so that considering a neighbour
+// cluster is one gather instead of the role and weight gathers.
 __global__ void k_roles(i64 n, const int* clusters, const u32* vw, const u64* cw, u32 salt, u32 threshold,
-                        bool all_singletons, unsigned char* roles, int* proposals) {
+                        bool all_singletons, unsigned char* roles, u64* recv, int* proposals) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (v >= n) return;
-    roles[v] = clusters[v] == v && cw[v] == static_cast<u64>(vw[v]) &&
-               (all_singletons || mix32(static_cast<u32>(v) ^ salt) < threshold);
+    const u64 weight = cw[v];
+    const bool role = clusters[v] == v && weight == static_cast<u64>(vw[v]) &&
+                      (all_singletons || mix32(static_cast<u32>(v) ^ salt) < threshold);
+    roles[v] = role;
+    recv[v] = role ? ~0ULL : weight;
     proposals[v] = kInvalid;
 }
 
@@ -293,8 +300,7 @@ __device__ __forceinline__ void reduce_summary(Summary& s) {
 __device__ __forceinline__ void consider(const RoundParams& p, Summary& s, int v, int src, int c, u64 conn) {
     if (c == src) { s.current = conn; return; }
     if (p.filter_roles) {
-        if (p.roles[c]) return;
-        const u64 base = p.cw[c];
+        const u64 base = p.recv[c];  // all ones (above any capacity) for a mover cluster
         if (!(base != 0 && base <= p.capacity && p.cw[src] <= p.capacity - base)) return;
     }
     const u64 tie = (static_cast<u64>(mix32(static_cast<u32>(v) ^ mix32(static_cast<u32>(c)) ^ p.tie_salt)) << 32) |
@@ -302,18 +308,17 @@ __device__ __forceinline__ void consider(const RoundParams& p, Summary& s, int v
     add_candidate(s, conn, tie);
 }
 
-// consider() split in two so that callers can issue the role and weight
-// gathers of several clusters before using any of them.
-__device__ __forceinline__ void gather_cluster(const RoundParams& p, int src, int c, unsigned char& role, u64& base) {
+// consider() split in two so that callers can issue the receiver gathers of
+// several clusters before using any of them.
+__device__ __forceinline__ void gather_cluster(const RoundParams& p, int src, int c, u64& base) {
     const bool other = p.filter_roles && c >= 0 && c != src;
-    role = other ? p.roles[c] : 0;
-    base = other ? p.cw[c] : 0;
+    base = other ? p.recv[c] : 0;
 }
 __device__ __forceinline__ void consider_gathered(const RoundParams& p, Summary& s, int v, int src, u64 own, int c,
-                                                  u64 conn, unsigned char role, u64 base) {
+                                                  u64 conn, u64 base) {
     if (c < 0) return;
     if (c == src) { s.current = conn; return; }
-    if (p.filter_roles && (role || !(base != 0 && base <= p.capacity && own <= p.capacity - base))) return;
+    if (p.filter_roles && !(base != 0 && base <= p.capacity && own <= p.capacity - base)) return;
     const u64 tie = (static_cast<u64>(mix32(static_cast<u32>(v) ^ mix32(static_cast<u32>(c)) ^ p.tie_salt)) << 32) |
                     (0xffffffffULL - static_cast<u32>(c));
     add_candidate(s, conn, tie);
@@ -424,7 +429,6 @@ __device__ __forceinline__ void consider_slots(const RoundParams& p, Summary& s,
     for (Slot s0 = first; s0 < size; s0 += 4 * stride) {
         int c[4];
         u64 conn[4], base[4];
-        unsigned char role[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const Slot sl = s0 + j * stride;
@@ -433,9 +437,9 @@ __device__ __forceinline__ void consider_slots(const RoundParams& p, Summary& s,
             if (sl < size) T.read(sl, c[j], conn[j]);
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) gather_cluster(p, src, c[j], role[j], base[j]);
+        for (int j = 0; j < 4; ++j) gather_cluster(p, src, c[j], base[j]);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) consider_gathered(p, s, v, src, own, c[j], conn[j], role[j], base[j]);
+        for (int j = 0; j < 4; ++j) consider_gathered(p, s, v, src, own, c[j], conn[j], base[j]);
     }
 }
 
@@ -589,12 +593,11 @@ __global__ void __launch_bounds__(256) k_affinity_heavy_summary(const int* heavy
     const u64 own = p.filter_roles ? p.cw[src] : 0;
 #pragma unroll
     for (int j0 = 0; j0 < kPerThread; j0 += 4) {
-        unsigned char role[4];
         u64 cwt[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) gather_cluster(p, src, c[j0 + q], role[q], cwt[q]);
+        for (int q = 0; q < 4; ++q) gather_cluster(p, src, c[j0 + q], cwt[q]);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) consider_gathered(p, sm, v, src, own, c[j0 + q], conn[j0 + q], role[q], cwt[q]);
+        for (int q = 0; q < 4; ++q) consider_gathered(p, sm, v, src, own, c[j0 + q], conn[j0 + q], cwt[q]);
     }
 #pragma unroll
     for (int j = 0; j < kPerThread; ++j)
@@ -1460,6 +1463,7 @@ private:
     int* clusters = nullptr;
     u64* cw = nullptr;
     unsigned char* roles = nullptr;
+    u64* recv = nullptr;  // receiver weights (k_roles)
     int* proposals = nullptr;
     u64* gains = nullptr;
     u64* regret = nullptr;
@@ -1520,8 +1524,8 @@ void Aggregator::form_proposals(u64 capacity, int round, bool filter_roles, u32 
     const u32 tie_salt = seed ^ (static_cast<u32>(level) * 0xc2b2ae35U) ^ (static_cast<u32>(round) * 0x165667b1U) ^ 0xd3a2646cU;
     const i64 n = g.n;
     launch(k_roles, blocks_for(n, kThreads), kThreads, 0, ctx.stream, n, clusters, g.vw, cw, role_salt, threshold,
-                                                                         !filter_roles, roles, proposals);
-    RoundParams p{g.off, g.nbr, g.ew, g.vw, clusters, cw, roles, capacity, tie_salt, filter_roles,
+           !filter_roles, roles, recv, proposals);
+    RoundParams p{g.off, g.nbr, g.ew, g.vw, clusters, cw, roles, recv, capacity, tie_salt, filter_roles,
                   filter_roles && need_regret, proposals, gains, regret, ties};
     if (list_size[0])
         launch(k_affinity_low, blocks_for(list_size[0] * 8, kThreads), kThreads, 0, ctx.stream, list_size[0], lists[0], p);
@@ -1547,6 +1551,7 @@ AggregateOut Aggregator::run() {
     clusters = A.alloc<int>(n);
     cw = A.alloc<u64>(n);
     roles = A.alloc<unsigned char>(n);
+    recv = A.alloc<u64>(n);
     proposals = A.alloc<int>(n);
     gains = A.alloc<u64>(n);
     regret = A.alloc<u64>(n);
