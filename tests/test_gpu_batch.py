@@ -84,15 +84,15 @@ def test_server_footprint_budget_still_completes(gp, ctx):
 def test_batch_mixed_part_counts_equal_single_calls(gp, ctx):
     """Concurrent workers launch the same kernels with different shared-memory
     sizes (the part-matching table grows with k, the large-row tables with
-    the row class); every result must still equal the graph partitioned
-    alone."""
+    the row class, the exchange's one-block move sort with the number of
+    moves); every result must still equal the graph partitioned alone."""
     jobs = []
-    for i in range(24):
-        k = (8, 128, 32, 64)[i % 4]
-        g = gp.rmat(12 + i % 3, 12, 0.57, 0.19, 0.19, 100 + i) if i % 2 else gp.grid2d(90 + i, 70)
+    for i in range(48):
+        k = (8, 128, 32, 64, 16, 4)[i % 6]
+        g = gp.rmat(12 + i % 4, 12, 0.57, 0.19, 0.19, 100 + i) if i % 2 else gp.grid2d(90 + 3 * i, 70)
         jobs.append((g, k, 1.03, i % 5))
     alone = [ctx.partition(g, k, eps, seed)[0] for g, k, eps, seed in jobs]
-    for labels_batched, expect in zip(ctx.partition_batch(jobs, concurrency=12), alone):
+    for labels_batched, expect in zip(ctx.partition_batch(jobs, concurrency=16), alone):
         np.testing.assert_array_equal(labels_batched[0], expect)
 
 
