@@ -2722,7 +2722,11 @@ private:
                    reinterpret_cast<long long*>(counters + 2), sample ? samples : static_cast<Sample*>(nullptr), gate,
                    threshold, work_counter(k_update_chunks<T>));
         }
-        launch(k_commit, grid_for(host_count, kThreads), kThreads, sizeof(long long) * k, s(), host_count, list, live,
+        // At most four blocks per SM: each block also aggregates its load
+        // changes and reports to the finished-block counter, so a grid sized
+        // by an upper bound of the movers would mostly pay that.
+        launch(k_commit, std::min(grid_for(host_count, kThreads), 148 * 4), kThreads, sizeof(long long) * k, s(),
+               host_count, list, live,
                labels, targets, g.vw, k, loads, lp ? locks : static_cast<unsigned char*>(nullptr), flags,
                static_cast<const u32*>(rposition), rlabels, state, counters + 3,
                reinterpret_cast<unsigned int*>(counters + 8));
