@@ -280,7 +280,11 @@ def run_ours(args):
     if world == 1 and not args.no_forms:
         # The survey's batched (B) and serving (S) forms, measured on the same
         # GPU after the timed region; they do not enter `value`.
-        line["batch"] = batch_form(gp, ctx, 512, 32)
+        # The batched form runs on a context of its own, closed before the
+        # serving form, so that its 32 worker contexts (streams, arenas) are
+        # released and the server meets the GPU as a serving process would.
+        with gp.Context(0) as batch_ctx:
+            line["batch"] = batch_form(gp, batch_ctx, 512, 32)
         line["serving"] = serving_form(gp, rate=30.0, requests=300, workers=8, pool_graphs=16, budget_gb=120.0,
                                        saturation_requests=120)
     if rank == 0:
