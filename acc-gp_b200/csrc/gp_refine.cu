@@ -1541,66 +1541,89 @@ __global__ void __launch_bounds__(kThreads) k_choose(i64 count, const u32* activ
     block_atomic_add(requesters, asked);
 }
 
-struct WantsPart {
-    const int* want;
-    __device__ bool operator()(i64 i) const { return want[i] >= 0; }
-};
 struct WriteIdx {
     u32* out;
     __device__ void operator()(u32 slot, i64 i) const { out[slot] = static_cast<u32>(i); }
 };
-__global__ void k_want_keys(i64 count, const u32* reqs, const int* want, u64* keys) {
-    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (j < count) keys[j] = static_cast<u64>(want[reqs[j]]);
-}
-struct ReqWeight {
-    const u32* reqs;
-    const u32* active;
-    const u32* vw;
-    __device__ u64 operator()(i64 j) const { return vw[active[reqs[j]]]; }
-};
-__global__ void k_req_heads(i64 count, const u64* keys, const u64* prefix, u64* base) {
-    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (j < count && (j == 0 || keys[j - 1] != keys[j])) base[keys[j]] = prefix[j];
-}
-// reserve_receiver_prefixes' ticket rule (rebalance_graph.cuh:127-153) in
-// (part, repair order) order: a donor is admitted when its whole weighted
-// range [begin, begin+w) lies inside the part's immutable room.
-// The weight requested per part is summed per warp (requests arrive sorted
-// by part, so a warp holds one or two parts) and per block in shared memory
-// before one global atomic per part and block.
-__global__ void k_admit(i64 count, const u32* reqs, const u64* keys, const u32* active, const u64* prefix,
-                        const u64* base, const u32* vw, const u64* slack, const u64* requests, u64* added,
-                        u64* tried, unsigned char* state, int* targets, int* flags, int k) {
-    __shared__ u64 block_added[kMaxParts];
-    for (int p = threadIdx.x; p < k; p += blockDim.x) block_added[p] = 0;
+// reserve_receiver_prefixes' ticket rule (rebalance_graph.cuh:127-153): a
+// donor asking for part t is admitted when its weighted range [begin,
+// begin + w) lies inside the part's immutable room, begin being the weight
+// already requested for t plus the weight asked for t by the donors before
+// it in repair order (the active donors' order).  Every asked weight is
+// added to the part's requests, admitted or not.  Without sorting the
+// requests by part: each tile of kAdmitTile donors sums the weight asked per
+// part (k_part_requests), an exclusive scan over the part-major array of
+// tile sums gives every tile its start per part, and k_admit_tiles finishes
+// the order inside the tile (earlier warps, then earlier lanes).
+constexpr int kAdmitTile = kThreads;
+__global__ void k_part_requests(i64 count, const int* want, const u32* active, const u32* vw, int k, int tiles,
+                                u64* tile_sums) {
+    __shared__ u64 s_sum[kMaxParts];
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_sum[p] = 0;
     __syncthreads();
-    const i64 j = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const bool valid = j < count;
-    const int t = valid ? static_cast<int>(keys[j]) : -1;
-    u64 w = 0;
-    if (valid) {
-        const u32 i = reqs[j];
-        const int v = static_cast<int>(active[i]);
-        w = vw[v];
+    const i64 i = static_cast<i64>(blockIdx.x) * kAdmitTile + threadIdx.x;
+    const int t = i < count ? want[i] : -1;
+    const u64 w = t >= 0 ? vw[active[i]] : 0;
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    u64 sum = 0;
+    for (unsigned rest = peers; rest; rest &= rest - 1) sum += __shfl_sync(peers, w, __ffs(rest) - 1);
+    if (t >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(reinterpret_cast<unsigned long long*>(s_sum + t), sum);
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        tile_sums[static_cast<i64>(p) * tiles + blockIdx.x] = s_sum[p];
+}
+// `offsets`: the exclusive scan of tile_sums (part-major), so the weight
+// asked for part t by the tiles before this one is offsets[t * tiles + tile]
+// - offsets[t * tiles].
+__global__ void k_admit_tiles(i64 count, const int* want, const u32* active, const u32* vw, const u64* offsets,
+                              int tiles, const u64* slack, const u64* requests, u64* tried, unsigned char* state,
+                              int* targets, int* flags, int k) {
+    constexpr int kWarps = kAdmitTile / 32;
+    __shared__ u64 s_warp[kMaxParts][kWarps];  // per part, the weight each warp asks (then its start)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int x = threadIdx.x; x < k * kWarps; x += blockDim.x) s_warp[x / kWarps][x % kWarps] = 0;
+    __syncthreads();
+    const i64 i = static_cast<i64>(blockIdx.x) * kAdmitTile + threadIdx.x;
+    const int t = i < count ? want[i] : -1;
+    const int v = t >= 0 ? static_cast<int>(active[i]) : 0;
+    const u64 w = t >= 0 ? vw[v] : 0;
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    u64 before = 0, sum = 0;
+    for (unsigned rest = peers; rest; rest &= rest - 1) {
+        const int l = __ffs(rest) - 1;
+        const u64 o = __shfl_sync(peers, w, l);
+        sum += o;
+        if (l < lane) before += o;
+    }
+    if (t >= 0 && lane == __ffs(peers) - 1) s_warp[t][warp] = sum;
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        u64 run = offsets[static_cast<i64>(p) * tiles + blockIdx.x] - offsets[static_cast<i64>(p) * tiles];
+        for (int w2 = 0; w2 < kWarps; ++w2) {
+            const u64 x = s_warp[p][w2];
+            s_warp[p][w2] = run;
+            run += x;
+        }
+    }
+    __syncthreads();
+    if (t >= 0) {
         tried[2 * i + (t >> 6)] |= 1ULL << (t & 63);
-        const u64 begin = requests[t] + prefix[j] - base[t];
+        const u64 begin = requests[t] + s_warp[t][warp] + before;
         if (begin <= slack[t] && w <= slack[t] - begin) {
             targets[v] = t;
             flags[v] = 1;
             state[i] = 1;
         }
     }
-    const unsigned peers = __match_any_sync(0xffffffffu, t);
-    u64 sum = 0;
-    for (unsigned rest = peers; rest; rest &= rest - 1) sum += __shfl_sync(peers, w, __ffs(rest) - 1);
-    if (t >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(block_added + t, sum);
-    __syncthreads();
-    for (int p = threadIdx.x; p < k; p += blockDim.x)
-        if (block_added[p]) atomicAdd(added + p, block_added[p]);
 }
-__global__ void k_merge_requests(int k, u64* requests, u64* added) {
-    for (int p = threadIdx.x; p < k; p += blockDim.x) { requests[p] += added[p]; added[p] = 0; }
+// Every weight asked this attempt joins its part's requests: per part, the
+// scan's span over that part's tiles (the last part ends at the scan total).
+__global__ void k_merge_tiles(int k, int tiles, const u64* offsets, const u64* total, u64* requests) {
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        const u64 first = offsets[static_cast<i64>(p) * tiles];
+        const u64 end = p + 1 < k ? offsets[static_cast<i64>(p + 1) * tiles] : *total;
+        requests[p] += end - first;
+    }
 }
 // The remaining attempts of a receiver reservation by one block, for a small
 // set of open donors: the choice of k_choose and the ticket rule of k_admit,
@@ -2871,11 +2894,8 @@ bool LevelRefiner<T>::repair() {
     ArenaScope scope(A_);
     u64* slack = A_.alloc<u64>(k);
     u64* requests = A_.alloc<u64>(k);
-    u64* added = A_.alloc<u64>(k);
     u64* cdf = A_.alloc<u64>(k + 1);
     u64* part_base = A_.alloc<u64>(k);
-    u64* base_t = A_.alloc<u64>(k);
-    GP_CUDA(cudaMemsetAsync(added, 0, sizeof(u64) * k, s()));
     u32* donors = A_.alloc<u32>(n);
     u32* donor_count = reinterpret_cast<u32*>(counters + 4);
     unsigned char* active_flag = A_.alloc<unsigned char>(n);
@@ -2932,11 +2952,10 @@ bool LevelRefiner<T>::repair() {
                 int* want = A_.alloc<int>(acount);
                 GP_CUDA(cudaMemsetAsync(tried, 0, sizeof(u64) * 2 * acount, s()));
                 GP_CUDA(cudaMemsetAsync(state, 0, acount, s()));
-                u32* reqs = A_.alloc<u32>(acount);
-                u32* reqs_alt = A_.alloc<u32>(acount);
-                u64* rkeys = A_.alloc<u64>(acount);
-                u64* rkeys_alt = A_.alloc<u64>(acount);
-                u64* rprefix = A_.alloc<u64>(acount);
+                const int tiles = blocks_for(acount, kAdmitTile);
+                u64* tile_sums = A_.alloc<u64>(static_cast<size_t>(k) * tiles);
+                u64* tile_offsets = A_.alloc<u64>(static_cast<size_t>(k) * tiles);
+                u64* tile_total = A_.alloc<u64>(1);
                 u32* open = A_.alloc<u32>(acount);
                 u32* open_count = reinterpret_cast<u32*>(counters + 5);
                 // Small sets of open donors finish all their attempts in one block.
@@ -2985,22 +3004,22 @@ bool LevelRefiner<T>::repair() {
                                    acount, active, attempt, static_cast<const T*>(A), labels, g.vw, k, targets, slack,
                                    requests, tried, state, want, counters + 5);
                         });
-                    select_if(A_, s(), acount, WantsPart{want}, WriteIdx{reqs}, donor_count);
-                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 4, sizeof(u64), cudaMemcpyDeviceToHost, s()));
+                    // Admission of this attempt's requests (a no-op when none
+                    // asked), then one read-back of the number that asked.
+                    launch(k_part_requests, tiles, kAdmitTile, 0, s(), acount, static_cast<const int*>(want),
+                           static_cast<const u32*>(active), static_cast<const u32*>(g.vw), k, tiles, tile_sums);
+                    exclusive_scan<u64>(A_, s(), static_cast<i64>(k) * tiles, LoadOf<u64>{tile_sums}, tile_offsets,
+                                        tile_total);
+                    launch(k_admit_tiles, tiles, kAdmitTile, 0, s(), acount, static_cast<const int*>(want),
+                           static_cast<const u32*>(active), static_cast<const u32*>(g.vw),
+                           static_cast<const u64*>(tile_offsets), tiles, static_cast<const u64*>(slack),
+                           static_cast<const u64*>(requests), tried, state, targets, flags, k);
+                    launch(k_merge_tiles, 1, 128, 0, s(), k, tiles, static_cast<const u64*>(tile_offsets),
+                           static_cast<const u64*>(tile_total), requests);
+                    GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 5, sizeof(u64), cudaMemcpyDeviceToHost, s()));
                     GP_CUDA(cudaStreamSynchronize(s()));
-                    const i64 rcount = static_cast<i64>(ctx.host_scalars[0] & 0xffffffffULL);
+                    const i64 rcount = static_cast<i64>(ctx.host_scalars[0]);
                     if (!rcount) break;
-                    u32* r = reqs;
-                    u32* ra = reqs_alt;
-                    u64* kk = rkeys;
-                    u64* ka = rkeys_alt;
-                    launch(k_want_keys, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, want, kk);
-                    radix_sort_pairs(A_, s(), rcount, kk, r, ka, ra, 0, 8);
-                    exclusive_scan<u64>(A_, s(), rcount, ReqWeight{r, active, g.vw}, rprefix, static_cast<u64*>(nullptr));
-                    launch(k_req_heads, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, kk, rprefix, base_t);
-                    launch(k_admit, blocks_for(rcount, kThreads), kThreads, 0, s(), rcount, r, kk, active, rprefix, base_t,
-                           g.vw, slack, requests, added, tried, state, targets, flags, k);
-                    launch(k_merge_requests, 1, 128, 0, s(), k, requests, added);
                     // At most rcount donors remain open.
                     if (rcount <= kAttemptCap && attempt + 1 < k) {
                         select_if(A_, s(), acount, IsOpen{state}, WriteIdx{open}, open_count);
