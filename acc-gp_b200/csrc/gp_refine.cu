@@ -1575,9 +1575,14 @@ __global__ void k_part_requests(i64 count, const int* want, const u32* active, c
 // `offsets`: the exclusive scan of tile_sums (part-major), so the weight
 // asked for part t by the tiles before this one is offsets[t * tiles + tile]
 // - offsets[t * tiles].
+// The last block to finish (a finished-block counter, zero between
+// launches) then adds every weight asked this attempt to its part's
+// requests: per part, the scan's span over that part's tiles (the last part
+// ends at the scan total).
 __global__ void k_admit_tiles(i64 count, const int* want, const u32* active, const u32* vw, const u64* offsets,
-                              int tiles, const u64* slack, const u64* requests, u64* tried, unsigned char* state,
-                              int* targets, int* flags, int k) {
+                              const u64* total, int tiles, const u64* slack, u64* requests, u64* tried,
+                              unsigned char* state, int* targets, int* flags, int k, unsigned int* blocks_done) {
+    __shared__ bool last;
     constexpr int kWarps = kAdmitTile / 32;
     __shared__ u64 s_warp[kMaxParts][kWarps];  // per part, the weight each warp asks (then its start)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1615,15 +1620,19 @@ __global__ void k_admit_tiles(i64 count, const int* want, const u32* active, con
             state[i] = 1;
         }
     }
-}
-// Every weight asked this attempt joins its part's requests: per part, the
-// scan's span over that part's tiles (the last part ends at the scan total).
-__global__ void k_merge_tiles(int k, int tiles, const u64* offsets, const u64* total, u64* requests) {
+    __syncthreads();  // every read of `requests` in this block is done
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         const u64 first = offsets[static_cast<i64>(p) * tiles];
         const u64 end = p + 1 < k ? offsets[static_cast<i64>(p + 1) * tiles] : *total;
         requests[p] += end - first;
     }
+    if (threadIdx.x == 0) *blocks_done = 0;
 }
 // The remaining attempts of a receiver reservation by one block, for a small
 // set of open donors: the choice of k_choose and the ticket rule of k_admit,
@@ -3012,10 +3021,9 @@ bool LevelRefiner<T>::repair() {
                                         tile_total);
                     launch(k_admit_tiles, tiles, kAdmitTile, 0, s(), acount, static_cast<const int*>(want),
                            static_cast<const u32*>(active), static_cast<const u32*>(g.vw),
-                           static_cast<const u64*>(tile_offsets), tiles, static_cast<const u64*>(slack),
-                           static_cast<const u64*>(requests), tried, state, targets, flags, k);
-                    launch(k_merge_tiles, 1, 128, 0, s(), k, tiles, static_cast<const u64*>(tile_offsets),
-                           static_cast<const u64*>(tile_total), requests);
+                           static_cast<const u64*>(tile_offsets), static_cast<const u64*>(tile_total), tiles,
+                           static_cast<const u64*>(slack), requests, tried, state, targets, flags, k,
+                           reinterpret_cast<unsigned int*>(counters + 8));
                     GP_CUDA(cudaMemcpyAsync(ctx.host_scalars, counters + 5, sizeof(u64), cudaMemcpyDeviceToHost, s()));
                     GP_CUDA(cudaStreamSynchronize(s()));
                     const i64 rcount = static_cast<i64>(ctx.host_scalars[0]);
