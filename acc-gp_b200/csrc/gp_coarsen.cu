@@ -28,7 +28,7 @@ constexpr int kLargeDegree = kHeavyRow;   // rows above use a chunked global tab
 constexpr int kMediumHash = 512;          // SCLP_MEDIUM_HASH_SIZE
 constexpr int kLargeHash = 2 * kHeavyRow; // shared-memory table of the large class
 constexpr int kSegment = 4096;            // table slots summarised per block
-constexpr int kBlockSortRow = 4096;       // contraction: one 256-thread block sorts rows up to this
+constexpr int kBlockSortRow = 4096;       // contraction: one block sorts rows up to this in shared memory
 constexpr int kBigSortRow = 8192;         // one 1024-thread block (dynamic shared memory) up to this
 constexpr int kBigSortThreads = 1024;
 constexpr int kMediumWarps = 4;
@@ -1168,17 +1168,17 @@ __device__ __forceinline__ void sort_row_in_smem(int* keys, u32* vals, u32 (*war
     }
 }
 
-// Rows of 513..4096 raw entries: stable LSD radix sort by target in shared
+// Rows of 513..2048 raw entries: stable LSD radix sort by target in shared
 // memory (8-bit digits over the bits of nc; dropped intra-cluster entries
 // take the key nc and sort last), then one thread per run of equal keys sums
 // it and writes the unique run back at the row's start.  One instantiation
-// per row class (Items = 4, 8, 16 per thread: rows up to 1024, 2048, 4096),
-// each launched on its own list, so the short classes run with their own
-// register count and shared memory and more blocks fit on an SM.
+// per row class (Items = 4 or 8 per thread: rows up to 1024 or 2048), each
+// launched on its own list, so the shorter class runs with its own register
+// count and shared memory and more blocks fit on an SM.
 template <int Items>
 __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const int* raw_off, int* raw_t, u32* raw_w,
                                                          int* ucount, int nc, int bits) {
-    static_assert(Items * 256 <= kBlockSortRow, "row class above the block sort");
+    static_assert(Items * 256 <= 2048, "row class of the 256-thread block sort");
     __shared__ int keys[Items * 256];
     __shared__ u32 vals[Items * 256];
     __shared__ u32 warp_count[8][kRadix];
@@ -1210,21 +1210,31 @@ __global__ void __launch_bounds__(256) k_sort_rows_block(const int* rows, const 
     if (threadIdx.x == 0) ucount[c] = total;
 }
 
-// Rows of 4097..8192 raw entries: the same in-place sort by one block of
-// 1024 threads, 8 items each, in dynamic shared memory.
-__global__ void __launch_bounds__(kBigSortThreads) k_sort_rows_big(const int* rows, const int* raw_off, int* raw_t,
-                                                                   u32* raw_w, int* ucount, int nc, int bits) {
+// Rows of 2049..4096 (Threads 512) and 4097..8192 (Threads 1024) raw
+// entries: the same in-place sort by one block of Threads threads, 8 items
+// each, in dynamic shared memory.  Eight items per thread keep the register
+// count at 64, so two 512-thread blocks fit on an SM where the 256-thread,
+// 16-item block needed 128 registers and fit two of 256.
+template <int Threads>
+constexpr size_t big_sort_smem() {
+    return sizeof(int) * Threads * 8 * 2 + sizeof(u32) * (Threads / 32) * kRadix + sizeof(u32) * (kRadix + 33) +
+           sizeof(int) * 33;
+}
+template <int Threads>
+__global__ void __launch_bounds__(Threads, 1024 / Threads) k_sort_rows_big(const int* rows, const int* raw_off,
+                                                                          int* raw_t, u32* raw_w, int* ucount, int nc,
+                                                                          int bits) {
+    constexpr int kRow = Threads * 8;
     extern __shared__ __align__(16) unsigned char big_smem[];
     int* keys = reinterpret_cast<int*>(big_smem);
-    u32* vals = reinterpret_cast<u32*>(keys + kBigSortRow);
-    u32 (*warp_count)[kRadix] = reinterpret_cast<u32 (*)[kRadix]>(vals + kBigSortRow);
-    u32* local_base = reinterpret_cast<u32*>(warp_count + kBigSortThreads / 32);
+    u32* vals = reinterpret_cast<u32*>(keys + kRow);
+    u32 (*warp_count)[kRadix] = reinterpret_cast<u32 (*)[kRadix]>(vals + kRow);
+    u32* local_base = reinterpret_cast<u32*>(warp_count + Threads / 32);
     u32* scan_u = local_base + kRadix;
     int* scan_i = reinterpret_cast<int*>(scan_u + 33);
     const int c = rows[blockIdx.x];
     const int begin = raw_off[c], degree = raw_off[c + 1] - begin;
-    sort_row_in_smem<kBigSortRow / kBigSortThreads>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin,
-                                                    degree, nc, bits);
+    sort_row_in_smem<8>(keys, vals, warp_count, local_base, scan_u, raw_t, raw_w, begin, degree, nc, bits);
     const int per = (degree + blockDim.x - 1) / blockDim.x;
     int local = 0;
     for (int q = 0; q < per; ++q) {
@@ -1245,8 +1255,6 @@ __global__ void __launch_bounds__(kBigSortThreads) k_sort_rows_big(const int* ro
     }
     if (threadIdx.x == 0) ucount[c] = total;
 }
-constexpr size_t kBigSortSmem = sizeof(int) * kBigSortRow * 2 + sizeof(u32) * (kBigSortThreads / 32) * kRadix +
-                                sizeof(u32) * (kRadix + 33) + sizeof(int) * 33;
 
 // Rows above 8192 raw entries: records (row rank, target) -> global radix
 // sort.  Flat over records; the row of a record is found by binary search.
@@ -1803,15 +1811,18 @@ DGraph contract(Context& ctx, const DGraph& fine, AggregateOut& agg, Workspace& 
     };
     if (count[2]) sort_block(std::integral_constant<int, 4>{}, 2);
     if (count[3]) sort_block(std::integral_constant<int, 8>{}, 3);
-    if (count[4]) sort_block(std::integral_constant<int, 16>{}, 4);
-    if (count[5]) {
-        // Set on every call (one fixed value): the attribute belongs to the
-        // kernel, on whichever device is current.
-        GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kBigSortSmem)));
-        launch(k_sort_rows_big, static_cast<int>(count[5]), kBigSortThreads, kBigSortSmem, s, lists + 5 * nc, raw_off,
-               raw_t, raw_w, ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
-    }
+    auto sort_big = [&](auto threads, int cls) {
+        constexpr int T = decltype(threads)::value;
+        constexpr size_t smem = big_sort_smem<T>();
+        // Set on every call (one fixed value per instantiation): the
+        // attribute belongs to the kernel, on whichever device is current.
+        GP_CUDA(cudaFuncSetAttribute(k_sort_rows_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        launch(k_sort_rows_big<T>, static_cast<int>(count[cls]), T, smem, s, lists + cls * nc, raw_off, raw_t, raw_w,
+               ucount, static_cast<int>(nc), bit_length(static_cast<u64>(nc)));
+    };
+    if (count[4]) sort_big(std::integral_constant<int, 512>{}, 4);
+    if (count[5]) sort_big(std::integral_constant<int, kBigSortThreads>{}, 5);
     if (count[6]) {
         ArenaScope ls(A);
         const int* large = lists + 6 * nc;
