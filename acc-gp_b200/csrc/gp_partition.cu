@@ -839,7 +839,8 @@ gp_status gp_autotune(gp_context* ctx, const gp_csr* graph, int32_t k, double ep
         } restore{ctx, ctx->mapping};
         const double default_ms = time_setting(true);
         double best_ms = default_ms;
-        struct Knob { int Mapping::*field; std::vector<int> values; };
+        using Field = int Mapping::*;
+        struct Knob { Field field; std::vector<int> values; };
         const Knob knobs[] = {
             {&Mapping::medium_degree, {64, 128, 256}},
             {&Mapping::large_narrow, {512, 1024, 2048}},
