@@ -931,14 +931,26 @@ __global__ void k_scatter(i64 n, const int* off, const int* nbr, const u32* ew, 
             }
     }
 }
+// A block per chunk; every thread's entries (kChunk / blockDim of them) have
+// their neighbour and map gathers in flight together.
 __global__ void k_scatter_chunks(DGraph g, const int* map, const int* base, int* raw_t, u32* raw_w) {
+    constexpr int U = 8;
     const int ch = blockIdx.x, v = g.chunk_row[ch];
     const int c = map[v];
     const int out = base[v] - g.off[v];
-    for (int e = g.chunk_begin[ch] + threadIdx.x; e < chunk_end(g, ch, v); e += blockDim.x) {
-        const int t = map[g.nbr[e]];
-        raw_t[out + e] = t == c ? INT_MAX : t;
-        raw_w[out + e] = edge_w(g.ew, e);
+    const int end = chunk_end(g, ch, v), stride = static_cast<int>(blockDim.x);
+    for (int e0 = g.chunk_begin[ch] + static_cast<int>(threadIdx.x); e0 < end; e0 += U * stride) {
+        int u[U], t[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) u[j] = e0 + j * stride < end ? g.nbr[e0 + j * stride] : 0;
+#pragma unroll
+        for (int j = 0; j < U; ++j) t[j] = e0 + j * stride < end ? map[u[j]] : 0;
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (e0 + j * stride < end) {
+                raw_t[out + e0 + j * stride] = t[j] == c ? INT_MAX : t[j];
+                raw_w[out + e0 + j * stride] = edge_w(g.ew, e0 + j * stride);
+            }
     }
 }
 
@@ -1355,11 +1367,25 @@ __global__ void k_copy_rows(i64 nc, const int* raw_off, const int* raw_t, const 
     }
 }
 __global__ void k_copy_chunks(DGraph g, const int* raw_off, const int* raw_t, const u32* raw_w) {
+    constexpr int U = 8;
     const int ch = blockIdx.x, c = g.chunk_row[ch];
     const int shift = raw_off[c] - g.off[c];
-    for (int e = g.chunk_begin[ch] + threadIdx.x; e < chunk_end(g, ch, c); e += blockDim.x) {
-        g.nbr[e] = raw_t[shift + e];
-        g.ew[e] = raw_w[shift + e];
+    const int end = chunk_end(g, ch, c), stride = static_cast<int>(blockDim.x);
+    for (int e0 = g.chunk_begin[ch] + static_cast<int>(threadIdx.x); e0 < end; e0 += U * stride) {
+        int t[U];
+        u32 w[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const bool in = e0 + j * stride < end;
+            t[j] = in ? raw_t[shift + e0 + j * stride] : 0;
+            w[j] = in ? raw_w[shift + e0 + j * stride] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (e0 + j * stride < end) {
+                g.nbr[e0 + j * stride] = t[j];
+                g.ew[e0 + j * stride] = w[j];
+            }
     }
 }
 
