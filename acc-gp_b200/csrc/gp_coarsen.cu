@@ -1272,14 +1272,27 @@ __global__ void __launch_bounds__(Threads, 1024 / Threads) k_sort_rows_big(const
 // sort.  Flat over records; the row of a record is found by binary search.
 // With vals == nullptr the record's weight rides in the low 32 bits of its
 // key word (key << 32 | weight), so the sort moves one 8-byte word per record.
+// Every large row has more records than a block has threads, so the records
+// of one block pass span at most two rows: one thread finds the row of the
+// pass's first record by binary search and the others step past at most
+// one boundary.
 __global__ void k_large_records(i64 records, i64 count, const int* rows, const int* raw_off, const int* rec_off,
                                 const int* raw_t, const u32* raw_w, int tbits, u64* keys, u32* vals) {
+    __shared__ int s_row;
     const u64 sentinel = (1ULL << tbits) - 1;
-    for (i64 r = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; r < records;
-         r += static_cast<i64>(gridDim.x) * blockDim.x) {
-        int lo = 0, hi = static_cast<int>(count);  // last j with rec_off[j] <= r
-        while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (rec_off[mid] <= r) lo = mid; else hi = mid; }
-        const int j = lo;
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < records;
+         base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = static_cast<int>(count);  // last j with rec_off[j] <= base
+            while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (rec_off[mid] <= base) lo = mid; else hi = mid; }
+            s_row = lo;
+        }
+        __syncthreads();
+        const i64 r = base + threadIdx.x;
+        int j = s_row;
+        __syncthreads();  // s_row is rewritten by the next pass
+        if (r >= records) continue;
+        if (j + 1 < count && rec_off[j + 1] <= r) ++j;
         const int pos = raw_off[rows[j]] + static_cast<int>(r - rec_off[j]);
         const int t = raw_t[pos];
         const u64 key = (static_cast<u64>(j) << tbits) | (t == INT_MAX ? sentinel : static_cast<u64>(t));
