@@ -1969,7 +1969,9 @@ Hierarchy coarsen(Context& ctx, const DGraph& input, const CoarsenOptions& o) {
         ws.row_bounds = ctx.persist.alloc<u64>(current.n);
         ctx.clear_scalars(7);
         const int meta_grid = static_cast<int>(std::min<i64>(blocks_for(current.n * 8, kThreads), 148 * 16));
-        if (current.m / current.n < 8)
+        // 8 lanes per row unless the light rows (the heavier ones go by
+        // chunks) average more than 64 entries.
+        if (current.m - current.heavy_entries <= 64 * (current.n - current.heavy_count))
             launch(k_level0_meta<8>, meta_grid, kThreads, 0, s, current.n, current.off, current.nbr, current.ew,
                    current.vw, ws.row_bounds, ctx.dev_scalars);
         else
