@@ -278,7 +278,7 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline(gp, m)
         line["cpu_parts"] = cpu_parts(gp, g, labels, stats[-1].initial_seconds)
     if world == 1 and not args.no_forms:
-        # The survey's batched (B) and serving (S) forms, measured on the same
+        # The batched (B) and serving (S) forms of the workload set, measured on the same
         # GPU after the timed region; they do not enter `value`.
         # The batched form runs on a context of its own, closed before the
         # serving form, so that its 32 worker contexts (streams, arenas) are
@@ -639,7 +639,7 @@ def serving_form(gp, rate, requests, workers, pool_graphs, budget_gb, saturation
             "kept_hierarchy": kept_hierarchy(gp, max(pool, key=lambda g: g.m)),
             "pool_vertices": [int(g.n) for g in pool], "sample_identical_to_alone": same,
             "workload": "serving_poisson: resident R-MAT pool (n 1e4..4e6, weighted), k uniform 2..128, "
-                        "eps in {1.01, 1.03, 1.05}; the survey's 200 req/s exceeds one B200, so the latency "
+                        "eps in {1.01, 1.03, 1.05}; the configuration's 200 req/s exceeds one B200, so the latency "
                         "phase offers a rate below saturation and saturation is measured separately"}
 
 
