@@ -110,10 +110,11 @@ __global__ void k_scan_small(i64 count, T* values, T* total) {
     if (threadIdx.x == 0 && total) *total = carry;
 }
 
-// Up to this many tiles, the writing pass of a scan or selection takes each
-// tile's start from the raw tile sums (every block adds up the sums before
-// it) instead of a separate launch that scans them.
-constexpr int kDirectScanTiles = 256;
+// Up to this many tiles (4 Mi items), the writing pass of a scan or
+// selection takes each tile's start from the raw tile sums (every block adds
+// up the sums before it, at most eight per thread) instead of a separate
+// launch that scans them.
+constexpr int kDirectScanTiles = 2048;
 
 // sums[0] + ... + sums[tiles - 1], by the whole block; every thread gets it.
 template <class T>
