@@ -9,6 +9,7 @@ and the final cut.  Needs a CUDA GPU (the reference is GPU code).
     python tests/golden/make_golden.py [--out DIR] [--cases a,b,...] [--baseline]
     python tests/golden/make_golden.py --refine [--out DIR]
     python tests/golden/make_golden.py --digests-only --cases rmat22_k64,m3_k128
+    python tests/golden/make_golden.py --oracle-labels --cases rmat22_k64,m3_k128
 
 --refine runs the reference's single-level refinement (oracle/_ref/
 gpart_ref_refine: its run_incremental_refinement on a one-level resident
@@ -18,6 +19,9 @@ RefineStats fields the reference reports for that run (-1 where it reports
 none).  --digests-only records hierarchy
 digests and the METIS digest without the final-label checks (for the
 headline-size cases, whose full arrays are too large to keep).
+--oracle-labels needs no GPU: it adds the serial oracle's final-label digest
+and cut to existing case files, for the label-identity check of the
+headline-size cases.
 
 --baseline additionally times the unmodified reference CLI on R-MAT scale 22
 (k=64, seeds 0-2) and writes baseline_rmat22.json.
@@ -203,6 +207,26 @@ def baseline(out_dir):
         json.dump(dict(graph=dict(n=g.n, m=g.m), k=64, eps=1.03, runs=rows), f, indent=1)
 
 
+def oracle_labels(out_dir, names):
+    """Adds to each named case file the SHA-256 of the serial oracle's final
+    labels and its cut, so a GPU test can require identical labels on graphs
+    whose full label arrays are too large to keep (the headline cases).  Runs
+    on the CPU only; R-MAT scale 22 takes a few minutes on one core."""
+    import oracle  # CPU restatement of the reference's rules
+    for name in names:
+        path = os.path.join(out_dir, f"{name}.json")
+        with open(path) as f:
+            record = json.load(f)
+        spec = CASES[name]
+        graph = build_case(gp, spec)
+        labels, cut = oracle.partition(graph, spec["k"], spec["eps"], spec["seed"])
+        record["oracle_final_labels"] = digest(labels)
+        record["oracle_final_cut"] = int(cut)
+        with open(path, "w") as f:
+            json.dump(record, f, indent=1)
+        print(name, "oracle cut", cut, flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
@@ -211,8 +235,13 @@ def main():
     ap.add_argument("--keep-arrays", action="store_true", help="also save full small-level arrays (npz)")
     ap.add_argument("--refine", action="store_true", help="refinement goldens (refine_cases.json)")
     ap.add_argument("--arrays-dir", default="", help="--refine: also save each refined labelling here (.npy)")
+    ap.add_argument("--oracle-labels", action="store_true",
+                    help="add the CPU oracle's final-label digest and cut to existing case files (no GPU)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    if args.oracle_labels:
+        oracle_labels(args.out, [c for c in args.cases.split(",") if c])
+        return
     if args.refine:
         names = [c for c in args.cases.split(",") if c] or list(REFINE_CASES)
         if args.arrays_dir:

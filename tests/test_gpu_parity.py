@@ -77,7 +77,8 @@ def test_headline_hierarchy_bit_exact_with_reference(name, gp, ctx, cases):
     """R-MAT scale 22 at k=64 and the 256^3 weighted mesh at k=128: every
     level's CSR, weights, map and metadata, and the METIS labels, equal the
     reference build's (SHA-256 digests); the cut is within 1% of the
-    reference run's and the capacity holds."""
+    reference run's and the capacity holds; the final labels and cut equal
+    the serial oracle's (digest recorded by make_golden.py --oracle-labels)."""
     CASES, build = cases
     spec, fx = CASES[name], golden(name)
     g = build(gp, spec)
@@ -97,6 +98,9 @@ def test_headline_hierarchy_bit_exact_with_reference(name, gp, ctx, cases):
     verdict = gp.verify(g, labels, spec["k"], spec["eps"])
     assert verdict["capacity_ok"] and verdict["cut"] == st.edge_cut
     assert st.edge_cut <= 1.01 * fx["reference_final_cut"]
+    if "oracle_final_labels" in fx:
+        assert st.edge_cut == fx["oracle_final_cut"]
+        assert digest(labels) == fx["oracle_final_labels"]
 
 
 def test_reference_failure_reproduced(gp, ctx, cases):
